@@ -1,0 +1,46 @@
+"""``torch.autograd.Function`` over the CB-SpMV C ABI (a test harness).
+
+Y = A(vals) X where ``vals`` are the matrix's input nonzero values (the
+caller's COO order) and X is (n,) or (n, k).  Backward:
+
+* dL/dX    = A^T dL/dY, on the plan's transposed CB layout (build the plan
+  with ``want_transpose=1``);
+* dL/dvals = for each input nonzero k, dL/dY[row_k, :] . X[col_k, :], computed
+  per stored value slot (``grad_vals``) and gathered back to input order
+  through ``input_slots`` -- every input is summed into exactly one slot, so
+  the slot's gradient is the input's gradient.
+"""
+from __future__ import annotations
+
+import torch
+
+
+class CBSpMVFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, vals, x, plan):
+        plan.set_values(vals.detach().contiguous())
+        y = plan.spmv(x.detach().contiguous())
+        ctx.plan = plan
+        ctx.save_for_backward(x)
+        return y
+
+    @staticmethod
+    def backward(ctx, gy):
+        plan = ctx.plan
+        (x,) = ctx.saved_tensors
+        gy = gy.contiguous()
+        gx = gvals = None
+        if ctx.needs_input_grad[1]:
+            gx = plan.spmv_t(gy)
+        if ctx.needs_input_grad[0]:
+            slots = getattr(plan, "_slots_dev", None)
+            if slots is None or slots.device != gy.device:
+                slots = torch.from_numpy(plan.input_slots()).to(gy.device)
+                plan._slots_dev = slots
+            gvals = plan.grad_vals(gy, x.contiguous())[slots]
+        return gvals, gx, None
+
+
+def cbspmv_apply(plan, vals, x):
+    """Differentiable Y = A(vals) X through the plan."""
+    return CBSpMVFunction.apply(vals, x, plan)

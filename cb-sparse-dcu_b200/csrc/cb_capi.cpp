@@ -1,0 +1,534 @@
+// C ABI of include/cbspmv.h.  Plans own the host structure (for export and
+// parity), the device layout, and the device buffers.  Every entry point
+// returns a status and records a message; none exits or throws.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <chrono>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "cb_builder.hpp"
+#include "cb_kernels.hpp"
+#include "cb_layout.hpp"
+#include "cbspmv.h"
+
+namespace {
+
+thread_local std::string g_error;
+std::atomic<int64_t> g_launches{0};
+
+cbspmv_status fail(cbspmv_status code, const std::string &msg) {
+    g_error = msg;
+    return code;
+}
+
+cbspmv_status cuda_fail(cudaError_t e, const char *what) {
+    cudaGetLastError();  // clear a sticky-free error so later calls can run
+    return fail(CBSPMV_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CB_CUDA(call, what)                              \
+    do {                                                 \
+        cudaError_t e_ = (call);                         \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+template <class T>
+cudaError_t upload_vec(const std::vector<T> &v, T **dst, cudaStream_t s) {
+    *dst = nullptr;
+    if (v.empty()) return cudaSuccess;
+    cudaError_t e = cudaMalloc((void **)dst, v.size() * sizeof(T));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyAsync(*dst, v.data(), v.size() * sizeof(T),
+                           cudaMemcpyHostToDevice, s);
+}
+
+struct DevSide {
+    cb::DeviceLayout lay;
+    cb::DevLayout d;
+    void *tiles = nullptr, *blocks = nullptr;
+    uint8_t *payload = nullptr;
+    int32_t *block_cols = nullptr;
+    void *partials = nullptr;
+    int32_t *counters = nullptr;
+    int partial_nrhs = 0;
+    int64_t *vsrc_ptr = nullptr;
+    int32_t *vsrc = nullptr;
+    uint64_t *val_off = nullptr;
+    int32_t *val_row = nullptr, *val_col = nullptr;
+
+    void release() {
+        void *ps[] = {tiles, blocks, payload, block_cols, partials, counters,
+                      vsrc_ptr, vsrc, val_off, val_row, val_col};
+        for (void *p : ps)
+            if (p) cudaFree(p);
+        tiles = blocks = partials = nullptr;
+        payload = nullptr;
+        block_cols = counters = vsrc = val_row = val_col = nullptr;
+        vsrc_ptr = nullptr;
+        val_off = nullptr;
+        partial_nrhs = 0;
+        d = cb::DevLayout();
+    }
+};
+
+}  // namespace
+
+struct cbspmv_plan {
+    cbspmv_opts opts;
+    cb::HostCB host, host_t;
+    DevSide A, AT;
+    bool has_t = false;
+    bool uploaded = false;
+    int device = -1;
+    // staging for the host-buffer entry points
+    void *hx = nullptr, *hy = nullptr;
+    size_t hx_bytes = 0, hy_bytes = 0;
+    ~cbspmv_plan() {
+        A.release();
+        AT.release();
+        if (hx) cudaFree(hx);
+        if (hy) cudaFree(hy);
+    }
+};
+
+namespace {
+
+size_t vsize(const cbspmv_plan *p) {
+    return p->opts.value_type == CBSPMV_F32 ? 4 : 8;
+}
+
+cbspmv_status upload_side(DevSide &s, cudaStream_t st) {
+    const cb::DeviceLayout &L = s.lay;
+    CB_CUDA(upload_vec(L.tiles, (cb::TileDesc **)&s.tiles, st), "upload tiles");
+    CB_CUDA(upload_vec(L.blocks, (cb::BlockDesc **)&s.blocks, st), "upload blocks");
+    CB_CUDA(upload_vec(L.payload, &s.payload, st), "upload payload");
+    CB_CUDA(upload_vec(L.block_cols, &s.block_cols, st), "upload gather list");
+    CB_CUDA(upload_vec(L.vsrc_ptr, &s.vsrc_ptr, st), "upload value sources");
+    CB_CUDA(upload_vec(L.vsrc, &s.vsrc, st), "upload value sources");
+    CB_CUDA(upload_vec(L.val_off, &s.val_off, st), "upload value offsets");
+    CB_CUDA(upload_vec(L.val_row, &s.val_row, st), "upload value rows");
+    CB_CUDA(upload_vec(L.val_col, &s.val_col, st), "upload value columns");
+    if (L.gb_m > 0) {
+        CB_CUDA(cudaMalloc((void **)&s.counters, L.gb_m * sizeof(int32_t)),
+                "allocate row counters");
+        CB_CUDA(cudaMemsetAsync(s.counters, 0, L.gb_m * sizeof(int32_t), st),
+                "clear row counters");
+    }
+    s.d.tiles = s.tiles;
+    s.d.blocks = s.blocks;
+    s.d.payload = s.payload;
+    s.d.block_cols = s.block_cols;
+    s.d.ntiles = (int64_t)L.tiles.size();
+    s.d.bs = L.bs;
+    s.d.f32 = L.f32;
+    s.d.gather = L.gather;
+    s.d.m = L.m;
+    s.d.n = L.n;
+    s.d.counters = s.counters;
+    return CBSPMV_OK;
+}
+
+// Partial slots sized for nrhs right-hand sides.
+cbspmv_status ensure_partials(DevSide &s, int nrhs, size_t vsz) {
+    if (s.lay.slots == 0 || s.partial_nrhs >= nrhs) return CBSPMV_OK;
+    if (s.partials) cudaFree(s.partials);
+    s.partials = nullptr;
+    const size_t bytes = (size_t)s.lay.slots * nrhs * s.lay.bs * vsz;
+    CB_CUDA(cudaMalloc(&s.partials, bytes), "allocate split-row partials");
+    s.partial_nrhs = nrhs;
+    s.d.partials = s.partials;
+    return CBSPMV_OK;
+}
+
+cbspmv_status run_side(cbspmv_plan *p, DevSide &s, const void *x, void *y,
+                       int nrhs, int64_t ldx, int64_t ldy, cudaStream_t st) {
+    if (!p->uploaded) return fail(CBSPMV_ERR_STATE, "plan not uploaded");
+    if (nrhs < 1) return fail(CBSPMV_ERR_INVALID, "nrhs must be >= 1");
+    if (ldx == 0) ldx = nrhs;
+    if (ldy == 0) ldy = nrhs;
+    if (ldx < nrhs || ldy < nrhs)
+        return fail(CBSPMV_ERR_INVALID, "leading dimension smaller than nrhs");
+    if ((s.lay.m > 0 && !y) || (s.lay.n > 0 && !x && s.lay.nvals > 0))
+        return fail(CBSPMV_ERR_INVALID, "null x or y");
+    cbspmv_status rc = ensure_partials(s, nrhs, vsize(p));
+    if (rc) return rc;
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev != p->device)
+        return fail(CBSPMV_ERR_STATE, "plan was uploaded to another device");
+    CB_CUDA(cb::launch_spmv(s.d, x, y, nrhs, ldx, ldy, st), "spmv launch");
+    if (s.d.ntiles > 0) g_launches++;
+    return CBSPMV_OK;
+}
+
+cb::BuildOpts to_build(const cbspmv_opts &o) {
+    cb::BuildOpts b;
+    b.bs = o.block_size;
+    b.row_owned = o.row_owned;
+    b.waves = o.waves_per_block;
+    b.dense_sixteenths = o.dense_sixteenths;
+    b.force_coo64 = o.force_coo64;
+    return b;
+}
+
+}  // namespace
+
+extern "C" {
+
+void cbspmv_default_opts(cbspmv_opts *o) {
+    if (!o) return;
+    o->block_size = 16;
+    o->row_owned = 1;
+    o->waves_per_block = 4;
+    o->dense_sixteenths = 15;
+    o->force_coo64 = 0;
+    o->value_type = CBSPMV_F64;
+    o->want_transpose = 0;
+    o->tile_entries = 0;
+}
+
+cbspmv_status cbspmv_coo2block_gather(const cbspmv_coo *coo,
+                                      const cbspmv_opts *opts,
+                                      cbspmv_plan **out) {
+    if (!coo || !out) return fail(CBSPMV_ERR_INVALID, "null argument");
+    *out = nullptr;
+    cbspmv_opts o;
+    cbspmv_default_opts(&o);
+    if (opts) o = *opts;
+    if (o.value_type != CBSPMV_F64 && o.value_type != CBSPMV_F32)
+        return fail(CBSPMV_ERR_INVALID, "value_type must be CBSPMV_F64 or CBSPMV_F32");
+    cbspmv_plan *p = new (std::nothrow) cbspmv_plan;
+    if (!p) return fail(CBSPMV_ERR_ALLOC, "out of host memory");
+    p->opts = o;
+    try {
+        int code = 0;
+        std::string err = cb::build_cb(to_build(o), coo->m, coo->n, coo->nnz,
+                                       coo->row, coo->col, coo->val, p->host, &code);
+        if (!err.empty()) {
+            delete p;
+            return fail(code, err);
+        }
+        err = cb::build_layout(p->host, o.value_type == CBSPMV_F32, o.tile_entries,
+                               p->A.lay, &code);
+        if (!err.empty()) {
+            delete p;
+            return fail(code, err);
+        }
+        if (o.want_transpose) {
+            // A^T as a row-sorted COO: a stable counting sort by column keeps
+            // each column's entries in row order.
+            const int64_t nnz = coo->nnz, n = coo->n;
+            std::vector<int64_t> cnt(n + 1, 0);
+            for (int64_t i = 0; i < nnz; ++i) cnt[coo->col[i] + 1]++;
+            for (int64_t c = 0; c < n; ++c) cnt[c + 1] += cnt[c];
+            std::vector<int32_t> tr(nnz), tc(nnz), perm(nnz);
+            std::vector<double> tv(nnz);
+            for (int64_t i = 0; i < nnz; ++i) {
+                const int64_t d = cnt[coo->col[i]]++;
+                tr[d] = coo->col[i];
+                tc[d] = coo->row[i];
+                tv[d] = coo->val[i];
+                perm[d] = (int32_t)i;
+            }
+            err = cb::build_cb(to_build(o), coo->n, coo->m, nnz, tr.data(), tc.data(),
+                               tv.data(), p->host_t, &code);
+            if (err.empty())
+                err = cb::build_layout(p->host_t, o.value_type == CBSPMV_F32,
+                                       o.tile_entries, p->AT.lay, &code);
+            if (!err.empty()) {
+                delete p;
+                return fail(code, "transpose: " + err);
+            }
+            // value sources of A^T refer to the caller's nonzero order
+            for (int32_t &s : p->AT.lay.vsrc) s = perm[s];
+            std::vector<int64_t> slot(nnz);
+            for (int64_t i = 0; i < nnz; ++i) slot[perm[i]] = p->AT.lay.input_slot[i];
+            p->AT.lay.input_slot.swap(slot);
+            p->has_t = true;
+        }
+    } catch (const std::bad_alloc &) {
+        delete p;
+        return fail(CBSPMV_ERR_ALLOC, "out of host memory while building");
+    }
+    *out = p;
+    return CBSPMV_OK;
+}
+
+cbspmv_status cbspmv_upload(cbspmv_plan *p, void *stream) {
+    if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
+    if (p->uploaded) return CBSPMV_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    CB_CUDA(cudaGetDevice(&p->device), "cudaGetDevice");
+    cbspmv_status rc = upload_side(p->A, st);
+    if (!rc && p->has_t) rc = upload_side(p->AT, st);
+    if (rc) {
+        p->A.release();
+        p->AT.release();
+        return rc;
+    }
+    CB_CUDA(cudaStreamSynchronize(st), "upload");
+    p->uploaded = true;
+    return CBSPMV_OK;
+}
+
+cbspmv_status cbspmv_spmv(cbspmv_plan *p, const void *x, void *y, int nrhs,
+                          int64_t ldx, int64_t ldy, void *stream) {
+    if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
+    return run_side(p, p->A, x, y, nrhs, ldx, ldy, (cudaStream_t)stream);
+}
+
+cbspmv_status cbspmv_spmv_t(cbspmv_plan *p, const void *g, void *gx, int nrhs,
+                            int64_t ldg, int64_t ldgx, void *stream) {
+    if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
+    if (!p->has_t) return fail(CBSPMV_ERR_STATE, "plan built without want_transpose");
+    return run_side(p, p->AT, g, gx, nrhs, ldg, ldgx, (cudaStream_t)stream);
+}
+
+cbspmv_status cbspmv_spmv_host(cbspmv_plan *p, const void *x_host, void *y_host,
+                               int nrhs, void *stream) {
+    if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
+    if (nrhs < 1) return fail(CBSPMV_ERR_INVALID, "nrhs must be >= 1");
+    cbspmv_status rc = cbspmv_upload(p, stream);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t xb = (size_t)p->host.n * nrhs * vsize(p);
+    const size_t yb = (size_t)p->host.m * nrhs * vsize(p);
+    if (xb > p->hx_bytes) {
+        if (p->hx) cudaFree(p->hx);
+        p->hx = nullptr;
+        p->hx_bytes = 0;
+        CB_CUDA(cudaMalloc(&p->hx, xb), "allocate x");
+        p->hx_bytes = xb;
+    }
+    if (yb > p->hy_bytes) {
+        if (p->hy) cudaFree(p->hy);
+        p->hy = nullptr;
+        p->hy_bytes = 0;
+        CB_CUDA(cudaMalloc(&p->hy, yb), "allocate y");
+        p->hy_bytes = yb;
+    }
+    if (xb) CB_CUDA(cudaMemcpyAsync(p->hx, x_host, xb, cudaMemcpyHostToDevice, st), "copy x");
+    rc = run_side(p, p->A, p->hx, p->hy, nrhs, nrhs, nrhs, st);
+    if (rc) return rc;
+    if (yb) CB_CUDA(cudaMemcpyAsync(y_host, p->hy, yb, cudaMemcpyDeviceToHost, st), "copy y");
+    CB_CUDA(cudaStreamSynchronize(st), "spmv_host");
+    return CBSPMV_OK;
+}
+
+cbspmv_status cbspmv_cb_spmv(cbspmv_plan *p, const double *x, double *y,
+                             cbspmv_metrics *metrics) {
+    if (!p || !x || !y) return fail(CBSPMV_ERR_INVALID, "null argument");
+    if (p->opts.value_type != CBSPMV_F64)
+        return fail(CBSPMV_ERR_STATE, "cbspmv_cb_spmv takes double values");
+    if (metrics) *metrics = cbspmv_metrics{0.0, 0.0};
+    if (p->host.nnz == 0) {  // cb-spmv-dcu.hpp:1091-1098
+        for (int64_t i = 0; i < p->host.m; ++i) y[i] = 0.0;
+        return CBSPMV_OK;
+    }
+    cbspmv_status rc = cbspmv_spmv_host(p, x, y, 1, nullptr);
+    if (rc) return rc;
+    // 100 warm-up and 1000 timed launches (cb-spmv-dcu.hpp:1631-1656)
+    for (int i = 0; i < 100; ++i) {
+        rc = run_side(p, p->A, p->hx, p->hy, 1, 1, 1, nullptr);
+        if (rc) return rc;
+    }
+    cudaEvent_t a, b;
+    CB_CUDA(cudaEventCreate(&a), "event");
+    CB_CUDA(cudaEventCreate(&b), "event");
+    cudaEventRecord(a, nullptr);
+    for (int i = 0; i < 1000 && !rc; ++i) rc = run_side(p, p->A, p->hx, p->hy, 1, 1, 1, nullptr);
+    cudaEventRecord(b, nullptr);
+    cudaError_t e = cudaEventSynchronize(b);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "timing");
+    if (metrics) {
+        metrics->runtime_ms = ms / 1000.0;
+        if (metrics->runtime_ms > 0)
+            metrics->gflops = 2.0 * (double)p->host.nnz * 1.0e-6 / metrics->runtime_ms;
+    }
+    return CBSPMV_OK;
+}
+
+cbspmv_status cbspmv_grad_vals(cbspmv_plan *p, const void *g, const void *x,
+                               void *gvals, int nrhs, int64_t ldg, int64_t ldx,
+                               void *stream) {
+    if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
+    if (!p->uploaded) return fail(CBSPMV_ERR_STATE, "plan not uploaded");
+    if (nrhs < 1) return fail(CBSPMV_ERR_INVALID, "nrhs must be >= 1");
+    if (ldg == 0) ldg = nrhs;
+    if (ldx == 0) ldx = nrhs;
+    if (ldg < nrhs || ldx < nrhs)
+        return fail(CBSPMV_ERR_INVALID, "leading dimension smaller than nrhs");
+    DevSide &s = p->A;
+    CB_CUDA(cb::launch_grad_vals(s.lay.f32, s.lay.nvals, s.val_row, s.val_col, g,
+                                 ldg, x, ldx, nrhs, gvals, (cudaStream_t)stream),
+            "grad_vals launch");
+    if (s.lay.nvals) g_launches++;
+    return CBSPMV_OK;
+}
+
+int64_t cbspmv_num_values(const cbspmv_plan *p) { return p ? p->A.lay.nvals : -1; }
+
+cbspmv_status cbspmv_set_values(cbspmv_plan *p, const void *input_values,
+                                void *stream) {
+    if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
+    if (!p->uploaded) return fail(CBSPMV_ERR_STATE, "plan not uploaded");
+    cudaStream_t st = (cudaStream_t)stream;
+    DevSide *sides[2] = {&p->A, p->has_t ? &p->AT : nullptr};
+    for (DevSide *s : sides) {
+        if (!s) continue;
+        CB_CUDA(cb::launch_set_values(s->lay.f32, s->lay.nvals, s->vsrc_ptr, s->vsrc,
+                                      s->val_off, input_values, s->payload, st),
+                "set_values launch");
+        if (s->lay.nvals) g_launches++;
+    }
+    return CBSPMV_OK;
+}
+
+cbspmv_status cbspmv_value_coords(const cbspmv_plan *p, int32_t *row, int32_t *col,
+                                  int64_t *first_input) {
+    if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
+    const cb::DeviceLayout &L = p->A.lay;
+    if (row) std::memcpy(row, L.val_row.data(), L.nvals * 4);
+    if (col) std::memcpy(col, L.val_col.data(), L.nvals * 4);
+    if (first_input)
+        for (int64_t v = 0; v < L.nvals; ++v)
+            first_input[v] = L.vsrc_ptr[v + 1] > L.vsrc_ptr[v] ? L.vsrc[L.vsrc_ptr[v]] : -1;
+    return CBSPMV_OK;
+}
+
+cbspmv_status cbspmv_input_slots(const cbspmv_plan *p, int64_t *slot) {
+    if (!p || !slot) return fail(CBSPMV_ERR_INVALID, "null argument");
+    std::memcpy(slot, p->A.lay.input_slot.data(), p->host.nnz * sizeof(int64_t));
+    return CBSPMV_OK;
+}
+
+cbspmv_status cbspmv_info_get(const cbspmv_plan *p, cbspmv_info *info) {
+    if (!p || !info) return fail(CBSPMV_ERR_INVALID, "null argument");
+    const cb::HostCB &g = p->host;
+    cbspmv_info I;
+    std::memset(&I, 0, sizeof(I));
+    I.m = g.m;
+    I.n = g.n;
+    I.nnz = g.nnz;
+    I.gb_m = g.gb_m;
+    I.gb_n = g.gb_n;
+    I.gb_nnzb = g.nnzb;
+    I.gather_flag = g.gather_flag;
+    I.direct_coo_columns = g.direct;
+    I.compact_coo_indices = g.compact;
+    I.load_balanced = g.balanced;
+    I.unit_values = g.unit_values;
+    I.super_sparse_blocks = g.super_sparse;
+    I.analyzed_blocks = g.analyzed;
+    I.super_sparse_ratio = g.ratio;
+    I.load_stddev_before = g.sd_before;
+    I.load_stddev_after = g.sd_after;
+    for (int64_t i = 0; i < g.nnzb; ++i) {
+        if (g.nnz_blk[i] <= 0) continue;
+        const int t = g.type_blk[i] & cb::kTypeMask;
+        I.coo_blocks += t == cb::kCOO;
+        I.csr_blocks += t == cb::kCSR;
+        I.dense_blocks += t == cb::kDENSE;
+        I.uniform_blocks += (g.type_blk[i] & cb::kUniform) != 0;
+    }
+    I.segments = (int64_t)g.seg_rows.size();
+    I.patterns = g.pat_row_ptr.empty() ? 0 : (int64_t)g.pat_row_ptr.size() - 1;
+    I.stored_values = p->A.lay.nvals;
+    I.tiles = (int64_t)p->A.lay.tiles.size();
+    I.split_rows = p->A.lay.split_rows;
+    I.device_bytes = (int64_t)(p->A.lay.tiles.size() * sizeof(cb::TileDesc) +
+                               p->A.lay.blocks.size() * sizeof(cb::BlockDesc) +
+                               p->A.lay.payload.size() + p->A.lay.block_cols.size() * 4);
+    I.algorithmic_bytes = p->A.lay.alg_bytes;
+    I.scratch_bytes = (int64_t)(p->A.lay.slots * p->A.lay.bs * vsize(p) +
+                                p->A.lay.gb_m * 4);
+    *info = I;
+    return CBSPMV_OK;
+}
+
+namespace {
+// Raw device-layout arrays, for host-side checks of the layout:
+// dev_tiles (u32, 8 per tile), dev_blocks (u32, 4 per block), dev_payload
+// (bytes), dev_values (stored values as double, device order).
+int64_t export_device(const cb::DeviceLayout &L, const std::string &k, void *out) {
+    auto raw = [&](const void *src, size_t bytes, size_t unit) -> int64_t {
+        if (out && bytes) std::memcpy(out, src, bytes);
+        return (int64_t)(bytes / unit);
+    };
+    if (k == "dev_tiles")
+        return raw(L.tiles.data(), L.tiles.size() * sizeof(cb::TileDesc), 4);
+    if (k == "dev_blocks")
+        return raw(L.blocks.data(), L.blocks.size() * sizeof(cb::BlockDesc), 4);
+    if (k == "dev_payload") return raw(L.payload.data(), L.payload.size(), 1);
+    if (k == "dev_values") {
+        if (out)
+            for (int64_t v = 0; v < L.nvals; ++v) {
+                double x;
+                if (L.f32) {
+                    float f;
+                    std::memcpy(&f, L.payload.data() + L.val_off[v], 4);
+                    x = f;
+                } else {
+                    std::memcpy(&x, L.payload.data() + L.val_off[v], 8);
+                }
+                ((double *)out)[v] = x;
+            }
+        return L.nvals;
+    }
+    return -1;
+}
+}  // namespace
+
+int64_t cbspmv_export(const cbspmv_plan *p, const char *name, void *out) {
+    if (!p || !name) return -1;
+    const std::string k(name);
+    if (k.rfind("dev_", 0) == 0) return export_device(p->A.lay, k, out);
+    return cb::export_array(p->host, k, out);
+}
+
+int64_t cbspmv_export_t(const cbspmv_plan *p, const char *name, void *out) {
+    if (!p || !name || !p->has_t) return -1;
+    const std::string k(name);
+    if (k.rfind("dev_", 0) == 0) return export_device(p->AT.lay, k, out);
+    return cb::export_array(p->host_t, k, out);
+}
+
+void cbspmv_export_scalars(const cbspmv_plan *p, int transpose, int64_t *out12,
+                           double *out3) {
+    const cb::HostCB &g = transpose ? p->host_t : p->host;
+    const int64_t s[12] = {g.m, g.n, g.nnz, g.gb_m, g.gb_n, g.nnzb,
+                           g.gather_flag, g.direct, g.compact, g.super_sparse,
+                           g.analyzed, g.balanced};
+    std::memcpy(out12, s, sizeof(s));
+    out3[0] = g.ratio;
+    out3[1] = g.sd_before;
+    out3[2] = g.sd_after;
+}
+
+cbspmv_status cbspmv_destroy(cbspmv_plan *p) {
+    delete p;
+    return CBSPMV_OK;
+}
+
+size_t cbspmv_last_error(char *buf, size_t len) {
+    if (buf && len) {
+        const size_t n = std::min(len - 1, g_error.size());
+        std::memcpy(buf, g_error.data(), n);
+        buf[n] = 0;
+    }
+    return g_error.size();
+}
+
+int64_t cbspmv_launch_count(void) { return g_launches.load(); }
+
+}  // extern "C"

@@ -1,0 +1,341 @@
+// sm_100a kernels of the CB-SpMV: the tile kernel (the reference's `comp` and
+// `gather` kernels, cb-spmv-dcu.hpp:159-1084, folded into one: the layout
+// resolves COO columns at build time and stages gathered x columns per
+// CSR/DENSE block), plus value refresh and value-gradient kernels.
+//
+// Mapping (32-lane warps, one warp per tile, 8 warps per CTA):
+//   phase 1  products of all COO entries of the tile, lane-strided with
+//            independent loads (idx, value, x[col]) -> shared memory; x tiles
+//            of the CSR/DENSE blocks (bs values each, through the gather list
+//            when the matrix was gathered) -> shared memory.
+//   phase 2  per COO block: a segmented scan over its row runs (entries are
+//            sorted by row inside a block, coo2block.h:219-227), two blocks of
+//            <= 16 entries per warp, 32-entry passes otherwise; the number of
+//            scan steps is the block's log2(longest run), stored in its
+//            descriptor.  CSR: 32/bs lanes per row (the reference's
+//            LANES_PER_ROW, macros.h:84, re-derived for 32 lanes).  DENSE:
+//            2 lanes per row for bs=16, 1 for bs=32.  Run tails add into two
+//            per-warp row accumulators (one per half-warp), never colliding.
+//   phase 3  the tile's bs row sums go to y, or for a block row split over
+//            several tiles to a partial slot; the last tile to arrive on the
+//            row's counter adds all partials in tile order and stores y.  No
+//            tile waits on another (the reference spins on a row epoch,
+//            cb-spmv-dcu.hpp:238-282).
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <type_traits>
+
+#include "cb_kernels.hpp"
+
+namespace cb {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kWarps = 8;
+constexpr int kTileEntries = 512;  // == cb_layout.hpp kTileEntries
+constexpr uint32_t kColMask = (1u << 27) - 1;
+
+__host__ __device__ constexpr int max_xt(int bs) { return bs == 16 ? 16 : 8; }
+__host__ __device__ constexpr uint32_t a16(uint32_t x) { return (x + 15u) & ~15u; }
+
+template <typename T, int BS>
+struct WarpSmem {
+    T prod[kTileEntries];
+    T xt[max_xt(BS) * BS];
+    T acc[2][BS];
+    uint8_t rowb[kTileEntries];
+};
+
+template <typename T>
+__device__ __forceinline__ T ldg(const T *p) {
+    return __ldg(p);
+}
+
+// One tile per warp; nrhs right-hand sides handled one after another
+// (x column j at x[col * ldx + j]).
+template <typename T, int BS>
+__global__ void __launch_bounds__(kWarps * 32)
+    cb_spmv_tile_kernel(const uint4 *__restrict__ tiles, int64_t ntiles,
+                        const uint4 *__restrict__ blocks,
+                        const uint8_t *__restrict__ payload,
+                        const int32_t *__restrict__ block_cols, int gather,
+                        const T *__restrict__ x, T *__restrict__ y, int64_t m,
+                        int nrhs, int64_t ldx, int64_t ldy,
+                        T *__restrict__ partials, int32_t *__restrict__ counters) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int64_t tile = (int64_t)blockIdx.x * kWarps + wib;
+    if (tile >= ntiles) return;
+    WarpSmem<T, BS> &S = reinterpret_cast<WarpSmem<T, BS> *>(smem_raw)[wib];
+
+    const uint4 ta = __ldg(&tiles[2 * tile]);      // begin, row, counts, pay16
+    const uint4 tb = __ldg(&tiles[2 * tile + 1]);  // E, slot, first, ntiles
+    const int nb = ta.z & 0xff;
+    const int ncoo = (ta.z >> 8) & 0xff;
+    const int nxt = (ta.z >> 16) & 0xff;
+    const int E = (int)tb.x;
+    const uint8_t *base = payload + (size_t)ta.w * 16;
+    uint4 bd = make_uint4(0, 0, 0, 0);
+    if (lane < nb) bd = __ldg(&blocks[ta.x + lane]);
+    const uint32_t *cidx = reinterpret_cast<const uint32_t *>(base);
+    const T *cval = reinterpret_cast<const T *>(base + a16(4u * E));
+    const int64_t row0 = (int64_t)ta.y * BS;
+
+    for (int j = 0; j < nrhs; ++j) {
+        const T *xj = x + j;
+        // ---- phase 1a: COO products
+#pragma unroll 4
+        for (int e = lane; e < E; e += 32) {
+            const uint32_t w = __ldg(&cidx[e]);
+            const T v = __ldg(&cval[e]);
+            const T p = v * ldg(&xj[(int64_t)(w & kColMask) * ldx]);
+            S.prod[e] = p;
+            S.rowb[e] = (uint8_t)(w >> 27);
+        }
+        // ---- phase 1b: x tiles of CSR/DENSE blocks
+        for (int t0 = 0; t0 < nxt * BS; t0 += 32) {
+            const int t = t0 + lane;
+            const int jb = min(t / BS, nxt - 1);
+            const uint32_t xb = __shfl_sync(kFull, bd.z, ncoo + jb);
+            const uint32_t mb = __shfl_sync(kFull, bd.y, ncoo + jb);
+            const int c = t % BS;
+            const int valid = (mb >> 14) & 63;
+            if (t < nxt * BS) {
+                T xv = T(0);
+                if (c < valid) {
+                    const int64_t col = gather ? (int64_t)__ldg(&block_cols[xb + c])
+                                               : (int64_t)(xb + c);
+                    xv = ldg(&xj[col * ldx]);
+                }
+                S.xt[t] = xv;
+            }
+        }
+        for (int t = lane; t < 2 * BS; t += 32) (&S.acc[0][0])[t] = T(0);
+        __syncwarp();
+
+        // ---- phase 2a: COO blocks
+        int i = 0;
+        while (i < ncoo) {
+            const uint32_t m0 = __shfl_sync(kFull, bd.y, i);
+            const uint32_t m1 = __shfl_sync(kFull, bd.y, min(i + 1, 31));
+            const int k0 = (m0 >> 3) & 2047;
+            const int k1 = (i + 1 < ncoo) ? (int)((m1 >> 3) & 2047) : 1 << 20;
+            if (k0 <= 16 && k1 <= 16) {
+                const int h = lane >> 4, hl = lane & 15;
+                const uint32_t off = __shfl_sync(kFull, bd.x, i + h);
+                const int k = h ? k1 : k0;
+                const int steps = max((int)((m0 >> 20) & 7), (int)((m1 >> 20) & 7));
+                const bool act = hl < k;
+                T p = act ? S.prod[off + hl] : T(0);
+                int r = act ? (int)S.rowb[off + hl] : 64 + hl;
+                for (int s = 0; s < steps; ++s) {
+                    const int d = 1 << s;
+                    const T pu = __shfl_up_sync(kFull, p, d, 16);
+                    const int ru = __shfl_up_sync(kFull, r, d, 16);
+                    if (hl >= d && ru == r) p += pu;
+                }
+                const int rn = __shfl_down_sync(kFull, r, 1, 16);
+                if (act && (hl == k - 1 || rn != r)) S.acc[h][r] += p;
+                __syncwarp();
+                i += 2;
+            } else {
+                const uint32_t off = __shfl_sync(kFull, bd.x, i);
+                const int steps = (m0 >> 20) & 7;
+                for (int b = 0; b < k0; b += 32) {
+                    const int q = b + lane;
+                    const bool act = q < k0;
+                    T p = act ? S.prod[off + q] : T(0);
+                    int r = act ? (int)S.rowb[off + q] : 64 + lane;
+                    for (int s = 0; s < steps; ++s) {
+                        const int d = 1 << s;
+                        const T pu = __shfl_up_sync(kFull, p, d);
+                        const int ru = __shfl_up_sync(kFull, r, d);
+                        if (lane >= d && ru == r) p += pu;
+                    }
+                    const int rn = __shfl_down_sync(kFull, r, 1);
+                    if (act && (q == k0 - 1 || lane == 31 || rn != r))
+                        S.acc[0][r] += p;
+                    __syncwarp();
+                }
+                i += 1;
+            }
+        }
+
+        // ---- phase 2b: CSR and DENSE blocks
+        for (int jb = 0; jb < nxt; ++jb) {
+            const uint32_t off = __shfl_sync(kFull, bd.x, ncoo + jb);
+            const uint32_t mb = __shfl_sync(kFull, bd.y, ncoo + jb);
+            const int k = (mb >> 3) & 2047;
+            const uint8_t *pb = base + off;
+            const T *xt = &S.xt[jb * BS];
+            if ((mb & 3) == 1) {
+                using IdxT = typename std::conditional<BS == 16, uint8_t, uint16_t>::type;
+                const IdxT *rp = reinterpret_cast<const IdxT *>(pb);
+                const IdxT *ci = rp + BS + 1;
+                const T *vv = reinterpret_cast<const T *>(
+                    pb + a16((uint32_t)((BS + 1 + k) * sizeof(IdxT))));
+                constexpr int L = 32 / BS;
+                const int row = lane / L, sub = lane % L;
+                const int kb = __ldg(&rp[row]), ke = __ldg(&rp[row + 1]);
+                T sum = T(0);
+                for (int q = kb + sub; q < ke; q += L)
+                    sum += __ldg(&vv[q]) * xt[__ldg(&ci[q])];
+                if (L == 2) sum += __shfl_xor_sync(kFull, sum, 1);
+                if (sub == 0) S.acc[0][row] += sum;
+            } else {
+                const T *vv = reinterpret_cast<const T *>(pb);
+                T sum = T(0);
+                if (BS == 16) {
+                    const int row = lane >> 1, c0 = (lane & 1) * 8;
+#pragma unroll
+                    for (int c = 0; c < 8; ++c)
+                        sum += __ldg(&vv[row * 16 + c0 + c]) * xt[c0 + c];
+                    sum += __shfl_xor_sync(kFull, sum, 1);
+                    if ((lane & 1) == 0) S.acc[0][row] += sum;
+                } else {
+#pragma unroll 8
+                    for (int c = 0; c < BS; ++c)
+                        sum += __ldg(&vv[lane * BS + c]) * xt[c];
+                    S.acc[0][lane] += sum;
+                }
+            }
+            __syncwarp();
+        }
+
+        // ---- phase 3: output
+        T s = T(0);
+        if (lane < BS) s = S.acc[0][lane] + S.acc[1][lane];
+        const int64_t grow = row0 + lane;
+        if (tb.y == 0xffffffffu) {
+            if (lane < BS && grow < m) y[grow * ldy + j] = s;
+        } else {
+            T *part = partials + ((size_t)tb.y * nrhs + j) * BS;
+            if (lane < BS) part[lane] = s;
+            __threadfence();
+            __syncwarp();
+            int last = 0;
+            if (lane == 0) {
+                const int old = atomicAdd(&counters[ta.y], 1);
+                last = old == (int)(tb.w * nrhs) - 1;
+            }
+            last = __shfl_sync(kFull, last, 0);
+            if (last) {
+                __threadfence();
+                if (lane < BS) {
+                    for (int jj = 0; jj < nrhs; ++jj) {
+                        T tot = T(0);
+                        for (uint32_t t = 0; t < tb.w; ++t)
+                            tot += __ldcg(&partials[((size_t)(tb.z + t) * nrhs + jj) * BS + lane]);
+                        if (grow < m) y[grow * ldy + jj] = tot;
+                    }
+                }
+                if (lane == 0) atomicExch(&counters[ta.y], 0);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+template <typename T>
+__global__ void cb_set_values_kernel(int64_t nvals, const int64_t *__restrict__ ptr,
+                                     const int32_t *__restrict__ src,
+                                     const uint64_t *__restrict__ off,
+                                     const T *__restrict__ in,
+                                     uint8_t *__restrict__ payload) {
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nvals) return;
+    T s = T(0);
+    for (int64_t z = ptr[v]; z < ptr[v + 1]; ++z) s += in[src[z]];
+    *reinterpret_cast<T *>(payload + off[v]) = s;
+}
+
+template <typename T>
+__global__ void cb_grad_vals_kernel(int64_t nvals, const int32_t *__restrict__ vrow,
+                                    const int32_t *__restrict__ vcol,
+                                    const T *__restrict__ g, int64_t ldg,
+                                    const T *__restrict__ x, int64_t ldx, int nrhs,
+                                    T *__restrict__ out) {
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nvals) return;
+    const int32_t r = vrow[v], c = vcol[v];
+    T s = T(0);
+    if (r >= 0 && c >= 0)
+        for (int j = 0; j < nrhs; ++j)
+            s += __ldg(&g[(int64_t)r * ldg + j]) * __ldg(&x[(int64_t)c * ldx + j]);
+    out[v] = s;
+}
+
+template <typename T, int BS>
+cudaError_t launch_tiles(const DevLayout &d, const void *x, void *y, int nrhs,
+                         int64_t ldx, int64_t ldy, cudaStream_t stream) {
+    const size_t smem = sizeof(WarpSmem<T, BS>) * kWarps;
+    static bool configured = false;  // per instantiation, per process
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(cb_spmv_tile_kernel<T, BS>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    const int64_t grid = (d.ntiles + kWarps - 1) / kWarps;
+    if (grid == 0) return cudaSuccess;
+    cb_spmv_tile_kernel<T, BS><<<(unsigned)grid, kWarps * 32, smem, stream>>>(
+        static_cast<const uint4 *>(d.tiles), d.ntiles,
+        static_cast<const uint4 *>(d.blocks), d.payload, d.block_cols, d.gather,
+        static_cast<const T *>(x), static_cast<T *>(y), d.m, nrhs, ldx, ldy,
+        static_cast<T *>(d.partials), d.counters);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t spmv_smem_bytes(int bs, int f32) {
+    if (bs == 16)
+        return kWarps * (f32 ? sizeof(WarpSmem<float, 16>) : sizeof(WarpSmem<double, 16>));
+    return kWarps * (f32 ? sizeof(WarpSmem<float, 32>) : sizeof(WarpSmem<double, 32>));
+}
+
+cudaError_t launch_spmv(const DevLayout &d, const void *x, void *y, int nrhs,
+                        int64_t ldx, int64_t ldy, cudaStream_t stream) {
+    if (d.bs == 16)
+        return d.f32 ? launch_tiles<float, 16>(d, x, y, nrhs, ldx, ldy, stream)
+                     : launch_tiles<double, 16>(d, x, y, nrhs, ldx, ldy, stream);
+    return d.f32 ? launch_tiles<float, 32>(d, x, y, nrhs, ldx, ldy, stream)
+                 : launch_tiles<double, 32>(d, x, y, nrhs, ldx, ldy, stream);
+}
+
+cudaError_t launch_set_values(int f32, int64_t nvals, const int64_t *vsrc_ptr,
+                              const int32_t *vsrc, const uint64_t *val_off,
+                              const void *in, uint8_t *payload,
+                              cudaStream_t stream) {
+    if (nvals == 0) return cudaSuccess;
+    const unsigned grid = (unsigned)((nvals + 255) / 256);
+    if (f32)
+        cb_set_values_kernel<float><<<grid, 256, 0, stream>>>(
+            nvals, vsrc_ptr, vsrc, val_off, static_cast<const float *>(in), payload);
+    else
+        cb_set_values_kernel<double><<<grid, 256, 0, stream>>>(
+            nvals, vsrc_ptr, vsrc, val_off, static_cast<const double *>(in), payload);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grad_vals(int f32, int64_t nvals, const int32_t *vrow,
+                             const int32_t *vcol, const void *g, int64_t ldg,
+                             const void *x, int64_t ldx, int nrhs, void *gvals,
+                             cudaStream_t stream) {
+    if (nvals == 0) return cudaSuccess;
+    const unsigned grid = (unsigned)((nvals + 255) / 256);
+    if (f32)
+        cb_grad_vals_kernel<float><<<grid, 256, 0, stream>>>(
+            nvals, vrow, vcol, static_cast<const float *>(g), ldg,
+            static_cast<const float *>(x), ldx, nrhs, static_cast<float *>(gvals));
+    else
+        cb_grad_vals_kernel<double><<<grid, 256, 0, stream>>>(
+            nvals, vrow, vcol, static_cast<const double *>(g), ldg,
+            static_cast<const double *>(x), ldx, nrhs, static_cast<double *>(gvals));
+    return cudaGetLastError();
+}
+
+}  // namespace cb

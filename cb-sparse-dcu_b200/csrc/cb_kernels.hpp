@@ -1,0 +1,43 @@
+// Launchers of the sm_100a kernels (cb_kernels.cu), callable from host C++.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace cb {
+
+// Device-resident pieces of one DeviceLayout (cb_layout.hpp).
+struct DevLayout {
+    const void *tiles = nullptr;      // TileDesc[ntiles]
+    const void *blocks = nullptr;     // BlockDesc[nblocks]
+    const uint8_t *payload = nullptr;
+    const int32_t *block_cols = nullptr;
+    int64_t ntiles = 0;
+    int bs = 16, f32 = 0, gather = 0;
+    int64_t m = 0, n = 0;
+    void *partials = nullptr;         // slots * bs values (scratch)
+    int32_t *counters = nullptr;      // gb_m arrival counters (scratch)
+};
+
+// y = A x; x: n rows, y: m rows, row-major with leading dims for nrhs > 1.
+cudaError_t launch_spmv(const DevLayout &d, const void *x, void *y, int nrhs,
+                        int64_t ldx, int64_t ldy, cudaStream_t stream);
+
+// payload value v = sum of in[vsrc[z]] for z in [vsrc_ptr[v], vsrc_ptr[v+1])
+cudaError_t launch_set_values(int f32, int64_t nvals, const int64_t *vsrc_ptr,
+                              const int32_t *vsrc, const uint64_t *val_off,
+                              const void *in, uint8_t *payload,
+                              cudaStream_t stream);
+
+// gvals[v] = sum_j g[row_v * ldg + j] * x[col_v * ldx + j] (0 when the slot
+// has no row or column)
+cudaError_t launch_grad_vals(int f32, int64_t nvals, const int32_t *vrow,
+                             const int32_t *vcol, const void *g, int64_t ldg,
+                             const void *x, int64_t ldx, int nrhs, void *gvals,
+                             cudaStream_t stream);
+
+// Dynamic shared memory of the SpMV kernel per CTA.
+size_t spmv_smem_bytes(int bs, int f32);
+
+}  // namespace cb

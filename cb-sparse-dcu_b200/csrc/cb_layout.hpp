@@ -1,0 +1,86 @@
+// Device layout of a built CB structure: what the sm_100a kernels read.
+//
+// The reference packs one buffer with per-block pointers (cb-spmv-dcu.hpp:
+// 1130-1348).  Here the unit of work is a TILE: up to kTileBlocks consecutive
+// blocks of ONE block row (and at most kTileEntries COO entries), processed by
+// one warp.  A tile's payload is contiguous and 16-byte aligned:
+//
+//   [COO section]  u32 idx[E] | pad16 | T val[E] | pad16
+//                  idx = (row_in_block << 27) | original column (resolved
+//                  through the gather list at build time, so the kernel does
+//                  no dependent lookup for COO entries)
+//   [per CSR block] IdxT row_ptr[bs+1] | IdxT col[k] | pad16 | T val[k] | pad16
+//                  (IdxT = u8 for bs=16, u16 for bs=32; col is block-local
+//                  in the block's column space: gathered when gather_flag)
+//   [per DENSE block] T val[bs*bs] row-major | pad16
+//
+// Block rows longer than one tile are split; each of their tiles writes bs
+// partial sums to a scratch slot and the last tile to arrive (a per-block-row
+// counter) adds the partials in tile order and stores y.  Rows of empty block
+// rows are covered by tiles with no blocks, which store zeros.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "cb_builder.hpp"
+
+namespace cb {
+
+constexpr int kTileBlocks = 32;
+constexpr int kTileEntries = 512;
+constexpr int kColBits = 27;  // COO idx: column in bits 0..26
+constexpr int64_t kMaxCols = int64_t(1) << kColBits;
+
+// 8 x u32 per tile
+struct TileDesc {
+    uint32_t block_begin;  // first block (device order)
+    uint32_t block_row;
+    uint32_t counts;       // nblocks | ncoo_blocks << 8 | nxt << 16
+    uint32_t payload16;    // payload offset in 16-byte units
+    uint32_t coo_entries;  // E
+    uint32_t slot;         // partial slot, 0xffffffff when the row is whole
+    uint32_t first_slot;   // first slot of this block row
+    uint32_t row_tiles;    // tiles of this block row
+};
+
+// 4 x u32 per block (device order: within a tile COO blocks first)
+struct BlockDesc {
+    uint32_t off;    // COO: first entry in the tile; else byte offset in tile
+    uint32_t meta;   // type | uniform<<2 | nnz<<3 | valid_cols<<14 | steps<<20
+    uint32_t xbase;  // gather: index of first gathered column in block_cols;
+                     // otherwise first column (gb_col * bs)
+    uint32_t gb_col;
+};
+
+inline uint32_t meta_type(uint32_t m) { return m & 3u; }
+inline uint32_t meta_nnz(uint32_t m) { return (m >> 3) & 2047u; }
+
+struct DeviceLayout {
+    int bs = 16;
+    int f32 = 0;  // value type of the payload
+    int gather = 0;
+    int64_t m = 0, n = 0, gb_m = 0;
+    std::vector<TileDesc> tiles;
+    std::vector<BlockDesc> blocks;
+    std::vector<uint8_t> payload;
+    std::vector<int32_t> block_cols;  // only when gather and CSR/DENSE exist
+    int64_t slots = 0;                // partial slots (tiles of split rows)
+    int64_t split_rows = 0;
+    int max_row_tiles = 0;
+    // stored values in device order
+    int64_t nvals = 0;
+    std::vector<uint64_t> val_off;   // byte offset of each value in payload
+    std::vector<int32_t> val_row, val_col;
+    std::vector<int64_t> vsrc_ptr;   // input nonzeros of each value, in the
+    std::vector<int32_t> vsrc;       // builder's summation order
+    std::vector<int64_t> input_slot; // per input nonzero: its value
+    // algorithmic bytes of one launch (nrhs = 1), padding excluded
+    int64_t alg_bytes = 0;
+};
+
+// Returns "" or an error; *code receives a cbspmv_status.
+std::string build_layout(const HostCB &g, int f32, int tile_entries,
+                         DeviceLayout &L, int *code);
+
+}  // namespace cb

@@ -1,0 +1,194 @@
+/* cbspmv.h -- C ABI of the B200-native CB-SpMV (cache-friendly block SpMV).
+ *
+ * The reference (xing-cong/CB-Sparse-DCU, cb-spmv-dcu/src/) is a header-only
+ * C++/HIP library whose operator surface is two calls:
+ *
+ *   void coo2block_gather(const int *row, const int *col, const ValType *val,
+ *                         GLOBAL_BLOCK &gb);                 coo2block.h:628
+ *   PROGRAM_METRICS cb_spmv(const GLOBAL_BLOCK &gb, const ValType *x,
+ *                           ValType *y);                      cb-spmv-dcu.hpp:1088
+ *
+ * This header keeps that surface (cbspmv_coo2block_gather, cbspmv_cb_spmv) and
+ * splits the second call into upload / execute / free so the packed matrix
+ * stays resident in HBM across solves.  Conventions:
+ *   - every function returns a cbspmv_status; 0 is success.  No call exits
+ *     the process (the reference's CHECK_HIP does, macros.h:17-31);
+ *   - cbspmv_last_error() gives the message of the calling thread's last
+ *     failure;
+ *   - pointers are plain host or device addresses; streams are cudaStream_t
+ *     passed as void* (0 = the legacy default stream);
+ *   - a plan is immutable after upload; one plan may be executed on one
+ *     stream at a time (its split-row scratch is shared by its launches).
+ */
+#ifndef CBSPMV_H
+#define CBSPMV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int cbspmv_status;
+enum {
+    CBSPMV_OK = 0,
+    CBSPMV_ERR_INVALID = 1,     /* bad argument, size or option           */
+    CBSPMV_ERR_UNSORTED = 2,    /* COO rows not in non-decreasing order   */
+    CBSPMV_ERR_BOUNDS = 3,      /* COO index outside [0,m) x [0,n)        */
+    CBSPMV_ERR_ALLOC = 4,       /* host or device allocation failed       */
+    CBSPMV_ERR_CUDA = 5,        /* a CUDA runtime call failed             */
+    CBSPMV_ERR_STATE = 6,       /* plan not uploaded / wrong value type   */
+    CBSPMV_ERR_UNSUPPORTED = 7  /* size beyond a documented limit         */
+};
+
+enum { CBSPMV_F64 = 0, CBSPMV_F32 = 1 };
+
+/* Build options.  The first five mirror the reference's compile-time macros
+ * (macros.h:38-97; its Makefile:4-7 sets the defaults used here). */
+typedef struct cbspmv_opts {
+    int block_size;       /* CB_BLOCK_SIZE: 16 (default) or 32              */
+    int row_owned;        /* CB_ROW_OWNED: 1 (default) row-owned segments;
+                             0 builds the reference's balance permutation  */
+    int waves_per_block;  /* CB_WAVES_PER_BLOCK: blocks per segment, 4      */
+    int dense_sixteenths; /* CB_DENSE_SIXTEENTHS: dense if nnz >= bs*bs*k/16
+                             (default 15)                                   */
+    int force_coo64;      /* CB_FORCE_COO64: 0                              */
+    int value_type;       /* CBSPMV_F64 (default) or CBSPMV_F32 values      */
+    int want_transpose;   /* also build the CB layout of A^T for adjoints   */
+    int tile_entries;     /* device tile size in stored entries (0 = auto)  */
+} cbspmv_opts;
+
+/* Host COO, 0-based, rows in non-decreasing order (the order the reference's
+ * reader produces, io/mmio_highlevel.h:392-398); duplicates are allowed and
+ * summed as the reference's builder sums them (coo2block.h:249-255). */
+typedef struct cbspmv_coo {
+    int32_t m, n;
+    int64_t nnz;
+    const int32_t *row;
+    const int32_t *col;
+    const double *val;
+} cbspmv_coo;
+
+/* PROGRAM_METRICS (format.h:185-188): mean kernel time and GFLOP/s. */
+typedef struct cbspmv_metrics {
+    double runtime_ms;
+    double gflops;
+} cbspmv_metrics;
+
+/* Sizes of the built structure (GLOBAL_BLOCK counters, format.h:62-104) and
+ * of the device layout. */
+typedef struct cbspmv_info {
+    int64_t m, n, nnz, gb_m, gb_n, gb_nnzb;
+    int32_t gather_flag, direct_coo_columns, compact_coo_indices;
+    int32_t load_balanced, unit_values;
+    int64_t super_sparse_blocks, analyzed_blocks;
+    double super_sparse_ratio, load_stddev_before, load_stddev_after;
+    int64_t coo_blocks, csr_blocks, dense_blocks, uniform_blocks;
+    int64_t segments, patterns, stored_values;
+    int64_t tiles, split_rows, device_bytes, algorithmic_bytes;
+    int64_t scratch_bytes;
+} cbspmv_info;
+
+typedef struct cbspmv_plan cbspmv_plan;
+
+/* ---- reference surface ------------------------------------------------ */
+
+/* Builds the CB structure on the host.  Replaces coo2block_gather
+ * (coo2block.h:628-670) and produces the same GLOBAL_BLOCK content bit for
+ * bit (block order, formats, index encodings, gather lists, segments,
+ * balance permutation, row patterns).  opts may be NULL for the defaults. */
+cbspmv_status cbspmv_coo2block_gather(const cbspmv_coo *coo,
+                                      const cbspmv_opts *opts,
+                                      cbspmv_plan **out);
+
+/* Replaces cb_spmv (cb-spmv-dcu.hpp:1088-1667): host x (n values) and host y
+ * (m values, overwritten), value type double.  Uploads the plan if needed,
+ * runs one checked launch, 100 warm-up and 1000 timed launches as the
+ * reference does (:1625-1656) and returns their mean time and 2*nnz/t. */
+cbspmv_status cbspmv_cb_spmv(cbspmv_plan *plan, const double *x, double *y,
+                             cbspmv_metrics *metrics);
+
+/* ---- split surface ---------------------------------------------------- */
+
+void cbspmv_default_opts(cbspmv_opts *opts);
+
+/* Copies the packed device layout to the current CUDA device. */
+cbspmv_status cbspmv_upload(cbspmv_plan *plan, void *stream);
+
+/* y = A x on the device, asynchronously on `stream`.  x and y are device
+ * arrays of the plan's value type: x has n rows, y has m rows.  With
+ * nrhs > 1 they are row-major n x nrhs / m x nrhs with leading dimensions
+ * ldx, ldy >= nrhs (pass 0 for nrhs).  y is overwritten. */
+cbspmv_status cbspmv_spmv(cbspmv_plan *plan, const void *x, void *y, int nrhs,
+                          int64_t ldx, int64_t ldy, void *stream);
+
+/* The same through host buffers: copies x to the device, runs, copies y
+ * back, and synchronizes `stream`.  Device buffers are kept in the plan. */
+cbspmv_status cbspmv_spmv_host(cbspmv_plan *plan, const void *x_host,
+                               void *y_host, int nrhs, void *stream);
+
+/* Adjoint: gx = A^T g (g: m rows, gx: n rows, same conventions).  Needs the
+ * plan built with want_transpose. */
+cbspmv_status cbspmv_spmv_t(cbspmv_plan *plan, const void *g, void *gx,
+                            int nrhs, int64_t ldg, int64_t ldgx, void *stream);
+
+/* Gradient of <g, A x> with respect to the plan's stored value slots, in
+ * packed order: gvals[k] = sum_j g[row_k, j] * x[col_k, j] (device arrays
+ * of the plan's value type; gvals has cbspmv_num_values entries). */
+cbspmv_status cbspmv_grad_vals(cbspmv_plan *plan, const void *g,
+                               const void *x, void *gvals, int nrhs,
+                               int64_t ldg, int64_t ldx, void *stream);
+
+/* Stored values: the plan's packed value slots, in device (tile) order.
+ * Dense blocks store all bs*bs values, so there can be more slots than input
+ * nonzeros; COO blocks merge duplicates (coo2block.h:249-255), so there can
+ * be fewer.  cbspmv_set_values takes NEW INPUT values (nnz of them, in the
+ * caller's COO order, plan value type, device memory) and re-packs every slot
+ * of A -- and of A^T when built -- as the sum of its input nonzeros, in the
+ * builder's summation order. */
+int64_t cbspmv_num_values(const cbspmv_plan *plan);
+cbspmv_status cbspmv_set_values(cbspmv_plan *plan, const void *input_values,
+                                void *stream);
+/* For each stored slot: its row and column (-1 for dense padding outside
+ * the matrix) and its first input nonzero (-1 if none).  Host arrays of
+ * cbspmv_num_values entries; any pointer may be NULL. */
+cbspmv_status cbspmv_value_coords(const cbspmv_plan *plan, int32_t *row,
+                                  int32_t *col, int64_t *first_input);
+/* For each input nonzero (caller's order): the slot it is summed into. */
+cbspmv_status cbspmv_input_slots(const cbspmv_plan *plan, int64_t *slot);
+
+cbspmv_status cbspmv_info_get(const cbspmv_plan *plan, cbspmv_info *info);
+
+/* Copies one named GLOBAL_BLOCK array (the dump names of the oracle:
+ * gb_row_idx, nnz_per_blk, type_per_blk, block_cols, segment_*, pattern_*,
+ * bidx_*, pay_u32, pay_f64, pay_*_off, ...) into out (may be NULL) and
+ * returns its length, or -1 for an unknown name.  The names dev_tiles,
+ * dev_blocks (uint32 words), dev_payload (bytes) and dev_values (double, one
+ * per stored slot) give the device layout itself. */
+int64_t cbspmv_export(const cbspmv_plan *plan, const char *name, void *out);
+
+/* The same for the CB structure of A^T (plans built with want_transpose). */
+int64_t cbspmv_export_t(const cbspmv_plan *plan, const char *name, void *out);
+
+/* GLOBAL_BLOCK scalars of A (transpose = 0) or A^T: out12 = m, n, nnz, gb_m,
+ * gb_n, gb_nnzb, gather_flag, direct_coo_columns, compact_coo_indices,
+ * super_sparse_blocks, analyzed_blocks, load_balanced; out3 =
+ * super_sparse_ratio, load_stddev_before, load_stddev_after. */
+void cbspmv_export_scalars(const cbspmv_plan *plan, int transpose,
+                           int64_t *out12, double *out3);
+
+cbspmv_status cbspmv_destroy(cbspmv_plan *plan);
+
+/* Message of the calling thread's last error ("" if none); returns its full
+ * length. */
+size_t cbspmv_last_error(char *buf, size_t len);
+
+/* Number of kernels this library launched in the calling process. */
+int64_t cbspmv_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CBSPMV_H */

@@ -1,0 +1,137 @@
+"""GPU parity of the CB-SpMV kernels against the oracle, through the C ABI.
+
+Tolerance (per row i, right-hand side j):
+    |y_ij - y_ref_ij| <= tol * sum_k |a_ik x_kj|
+with y_ref the oracle's long-double restatement of the reference's CPU SpMV
+(cb-spmv-dcu/src/utils.h:98-111); tol = 1e-12 for FP64, 1e-5 for FP32 (FP32
+values, FP32 accumulation, error measured against the FP64 oracle).  A plain
+relative error is ill-defined where y ~ 0 (N(0,1) values), so the bound is
+scaled by each row's absolute sum.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TOL = {False: 1e-12, True: 1e-5}
+
+
+def _cases():
+    from cbspmv import gen
+    rng = np.random.default_rng(7)
+    out = [
+        ("rand-small", gen.random_small(rng, 50, 40, 300)),
+        ("rand-dups", gen.random_small(rng, 300, 300, 3000, dup=True)),
+        ("rand-mid", gen.random_small(rng, 1000, 800, 20000)),
+        ("rand-wide", gen.random_small(rng, 400, 70000, 30000)),
+        ("rand-dense", gen.random_small(rng, 100, 100, 9000)),
+        ("dense-dups", gen.random_small(rng, 64, 64, 40000, dup=True)),
+        ("ragged", gen.random_small(rng, 37, 41, 1500, dup=True)),
+        ("unit", gen.random_small(rng, 500, 500, 8000, unit=True)),
+        ("lap64", gen.laplacian_2d(64, 64)),
+        ("st6", gen.stencil_27pt(6)),
+        ("pl8192", gen.power_law(8192, kmax=8192, band=512, seed=11)),
+    ]
+    m, n = 200, 300
+    cols = np.array([3, 7, 40, 41, 42, 100, 250])
+    out.append(("uniform", gen.Coo(m, n, np.repeat(np.arange(m), 7).astype(np.int32),
+                                   np.tile(cols, m).astype(np.int32),
+                                   np.ones(7 * m))))
+    return out
+
+
+CASES = _cases()
+
+
+def _check(y, yref, absrow, f32, what):
+    err = np.abs(np.asarray(y, np.float64) - yref)
+    bound = TOL[f32] * absrow + (1e-300 if not f32 else 1e-30)
+    worst = float(np.max(err / bound)) if err.size else 0.0
+    assert worst <= 1.0, f"{what}: error {worst:.3g} x tolerance"
+    return worst
+
+
+@pytest.mark.parametrize("name,coo", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("bs", [16, 32])
+@pytest.mark.parametrize("f32", [False, True])
+@pytest.mark.parametrize("tile_entries", [0, 64])
+def test_spmv_matches_oracle(cuda, name, coo, bs, f32, tile_entries):
+    import torch
+    import cbspmv
+    import cbdump as cd
+    from cbspmv import gen
+    dt = torch.float32 if f32 else torch.float64
+    plan = cbspmv.Plan(coo, block_size=bs, value_type=int(f32),
+                       tile_entries=tile_entries)
+    x = gen.uniform_x(coo.n, 5)
+    if f32:
+        x = x.astype(np.float32).astype(np.float64)  # same x for both
+    yref, ab = cd.oracle_spmm_ld(coo, x[None, :])
+    xd = torch.from_numpy(x).to(cuda, dt)
+    y = torch.full((coo.m,), float("nan"), dtype=dt, device=cuda)
+    plan.spmv(xd, y)
+    torch.cuda.synchronize()
+    y1 = y.cpu().numpy()
+    _check(y1, yref[0], ab[0], f32, f"{name} bs{bs} f32={f32}")
+    # repeated launches reuse the split-row counters: results stay bitwise equal
+    for _ in range(3):
+        plan.spmv(xd, y)
+    torch.cuda.synchronize()
+    assert np.array_equal(y.cpu().numpy().view(np.uint8), y1.view(np.uint8))
+
+
+@pytest.mark.parametrize("nrhs", [2, 5])
+@pytest.mark.parametrize("f32", [False, True])
+def test_multi_rhs(cuda, nrhs, f32):
+    import torch
+    import cbspmv
+    import cbdump as cd
+    from cbspmv import gen
+    coo = gen.power_law(4096, kmax=4096, band=256, seed=3, mean=24)
+    dt = torch.float32 if f32 else torch.float64
+    plan = cbspmv.Plan(coo, value_type=int(f32), tile_entries=128)
+    X = gen.uniform_x(coo.n, 9, nrhs=nrhs)  # (nrhs, n)
+    if f32:
+        X = X.astype(np.float32).astype(np.float64)
+    yref, ab = cd.oracle_spmm_ld(coo, X)
+    Y = plan.spmv(torch.from_numpy(np.ascontiguousarray(X.T)).to(cuda, dt))
+    torch.cuda.synchronize()
+    _check(Y.cpu().numpy().T, yref, ab, f32, f"nrhs={nrhs}")
+
+
+def test_host_entry_points(cuda):
+    """cb_spmv (the reference's one-call surface) and spmv_host."""
+    import cbspmv
+    import cbdump as cd
+    from cbspmv import gen
+    coo = gen.laplacian_2d(128, 128)
+    plan = cbspmv.Plan(coo)
+    x = gen.uniform_x(coo.n, 0)
+    yref, ab = cd.oracle_spmm_ld(coo, x[None, :])
+    y, met = plan.cb_spmv(x)
+    _check(y, yref[0], ab[0], False, "cb_spmv")
+    assert met["runtime"] > 0 and met["gflops"] > 0
+    y2 = plan.spmv_host(x)
+    assert np.array_equal(y, y2)
+
+
+def test_empty_and_degenerate(cuda):
+    import torch
+    import cbspmv
+    from cbspmv import gen
+    # no nonzeros: y must be all zeros (cb-spmv-dcu.hpp:1091-1098)
+    e = gen.Coo(33, 17, np.zeros(0, np.int32), np.zeros(0, np.int32), np.zeros(0))
+    p = cbspmv.Plan(e)
+    y = p.spmv(torch.ones(17, dtype=torch.float64, device=cuda),
+               torch.full((33,), 5.0, dtype=torch.float64, device=cuda))
+    assert torch.count_nonzero(y).item() == 0
+    yh, _ = p.cb_spmv(np.ones(17))
+    assert not yh.any()
+    # a single nonzero in a corner, empty rows around it
+    c = gen.Coo(1000, 1000, np.array([999], np.int32), np.array([0], np.int32),
+                np.array([2.5]))
+    p = cbspmv.Plan(c)
+    x = torch.arange(1000, dtype=torch.float64, device=cuda) + 1
+    y = p.spmv(x, torch.full((1000,), 7.0, dtype=torch.float64, device=cuda))
+    yy = y.cpu().numpy()
+    assert yy[999] == 2.5 and not yy[:999].any()
