@@ -13,12 +13,13 @@ current stream.
 from __future__ import annotations
 
 import ctypes
+import os
 import pathlib
 
 import numpy as np
 
 _HERE = pathlib.Path(__file__).resolve().parent
-LIB_PATH = _HERE / "libcbspmv.so"
+LIB_PATH = pathlib.Path(os.environ.get("CBSPMV_LIB", _HERE / "libcbspmv.so"))
 
 F64, F32 = 0, 1
 STATUS = {0: "OK", 1: "INVALID", 2: "UNSORTED", 3: "BOUNDS", 4: "ALLOC",

@@ -113,12 +113,11 @@ cbspmv_status upload_side(DevSide &s, cudaStream_t st) {
     CB_CUDA(upload_vec(L.val_off, &s.val_off, st), "upload value offsets");
     CB_CUDA(upload_vec(L.val_row, &s.val_row, st), "upload value rows");
     CB_CUDA(upload_vec(L.val_col, &s.val_col, st), "upload value columns");
-    if (L.gb_m > 0) {
-        CB_CUDA(cudaMalloc((void **)&s.counters, L.gb_m * sizeof(int32_t)),
-                "allocate row counters");
-        CB_CUDA(cudaMemsetAsync(s.counters, 0, L.gb_m * sizeof(int32_t), st),
-                "clear row counters");
-    }
+    // scratch: 2 scheduler counters, then one arrival counter per block row
+    CB_CUDA(cudaMalloc((void **)&s.counters, (L.gb_m + 2) * sizeof(int32_t)),
+            "allocate counters");
+    CB_CUDA(cudaMemsetAsync(s.counters, 0, (L.gb_m + 2) * sizeof(int32_t), st),
+            "clear counters");
     s.d.tiles = s.tiles;
     s.d.blocks = s.blocks;
     s.d.payload = s.payload;
@@ -129,7 +128,8 @@ cbspmv_status upload_side(DevSide &s, cudaStream_t st) {
     s.d.gather = L.gather;
     s.d.m = L.m;
     s.d.n = L.n;
-    s.d.counters = s.counters;
+    s.d.sched = reinterpret_cast<uint32_t *>(s.counters);
+    s.d.counters = s.counters + 2;
     return CBSPMV_OK;
 }
 
@@ -451,7 +451,7 @@ cbspmv_status cbspmv_info_get(const cbspmv_plan *p, cbspmv_info *info) {
                                p->A.lay.payload.size() + p->A.lay.block_cols.size() * 4);
     I.algorithmic_bytes = p->A.lay.alg_bytes;
     I.scratch_bytes = (int64_t)(p->A.lay.slots * p->A.lay.bs * vsize(p) +
-                                p->A.lay.gb_m * 4);
+                                (p->A.lay.gb_m + 2) * 4);
     *info = I;
     return CBSPMV_OK;
 }

@@ -23,7 +23,9 @@
 //            cb-spmv-dcu.hpp:238-282).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <type_traits>
 
 #include "cb_kernels.hpp"
@@ -33,18 +35,18 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWarps = 8;
-constexpr int kTileEntries = 512;  // == cb_layout.hpp kTileEntries
 constexpr uint32_t kColMask = (1u << 27) - 1;
 
 __host__ __device__ constexpr int max_xt(int bs) { return bs == 16 ? 16 : 8; }
 __host__ __device__ constexpr uint32_t a16(uint32_t x) { return (x + 15u) & ~15u; }
 
+// Per-warp shared memory.  acc holds one private row accumulator per lane
+// (lane l owns acc[l * (BS + 1) + r]; the +1 pad spreads a column over the
+// banks), so entries accumulate without atomics and in a fixed order.
 template <typename T, int BS>
 struct WarpSmem {
-    T prod[kTileEntries];
-    T xt[max_xt(BS) * BS];
-    T acc[2][BS];
-    uint8_t rowb[kTileEntries];
+    T xt[max_xt(BS) * BS];      // x tiles of the tile's CSR/DENSE blocks
+    T acc[32 * (BS + 1)];
 };
 
 template <typename T>
@@ -52,189 +54,218 @@ __device__ __forceinline__ T ldg(const T *p) {
     return __ldg(p);
 }
 
-// One tile per warp; nrhs right-hand sides handled one after another
-// (x column j at x[col * ldx + j]).
+// Sums the 32 lane-private accumulators of row r = lane % BS, clearing them
+// for the next tile.  Lanes >= BS (BS = 16) sum the upper 16 lanes' copies and
+// hand their half over by shuffle.  Result valid in lanes < BS.
 template <typename T, int BS>
-__global__ void __launch_bounds__(kWarps * 32)
+__device__ __forceinline__ T reduce_rows(T *acc, int lane) {
+    T s = T(0);
+    if (BS == 16) {
+        const int r = lane & 15, l0 = (lane >> 4) * 16;
+#pragma unroll
+        for (int l = 0; l < 16; ++l) {
+            T *p = &acc[(l0 + l) * (BS + 1) + r];
+            s += *p;
+            *p = T(0);
+        }
+        s += __shfl_down_sync(kFull, s, 16);
+    } else {
+#pragma unroll 8
+        for (int l = 0; l < 32; ++l) {
+            T *p = &acc[l * (BS + 1) + lane];
+            s += *p;
+            *p = T(0);
+        }
+    }
+    return s;
+}
+
+// Persistent warps fetch tiles from a global counter (sched[0]); the warp
+// whose exit completes sched[1] == number of warps resets both for the next
+// launch, so no launch waits on another and no host reset is needed.
+// kChunk COO entries per lane have their loads in flight together; nrhs
+// right-hand sides are handled one after another (x column j at
+// x[col * ldx + j]).
+template <typename T, int BS, int kChunk>
+__global__ void __launch_bounds__(kWarps * 32, 4)
     cb_spmv_tile_kernel(const uint4 *__restrict__ tiles, int64_t ntiles,
                         const uint4 *__restrict__ blocks,
                         const uint8_t *__restrict__ payload,
                         const int32_t *__restrict__ block_cols, int gather,
                         const T *__restrict__ x, T *__restrict__ y, int64_t m,
                         int nrhs, int64_t ldx, int64_t ldy,
-                        T *__restrict__ partials, int32_t *__restrict__ counters) {
+                        T *__restrict__ partials, int32_t *__restrict__ counters,
+                        uint32_t *__restrict__ sched) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    const int64_t tile = (int64_t)blockIdx.x * kWarps + wib;
-    if (tile >= ntiles) return;
     WarpSmem<T, BS> &S = reinterpret_cast<WarpSmem<T, BS> *>(smem_raw)[wib];
+    T *myacc = &S.acc[lane * (BS + 1)];
+    for (int t = lane; t < 32 * (BS + 1); t += 32) S.acc[t] = T(0);
+    __syncwarp();
 
-    const uint4 ta = __ldg(&tiles[2 * tile]);      // begin, row, counts, pay16
-    const uint4 tb = __ldg(&tiles[2 * tile + 1]);  // E, slot, first, ntiles
-    const int nb = ta.z & 0xff;
-    const int ncoo = (ta.z >> 8) & 0xff;
-    const int nxt = (ta.z >> 16) & 0xff;
-    const int E = (int)tb.x;
-    const uint8_t *base = payload + (size_t)ta.w * 16;
-    uint4 bd = make_uint4(0, 0, 0, 0);
-    if (lane < nb) bd = __ldg(&blocks[ta.x + lane]);
-    const uint32_t *cidx = reinterpret_cast<const uint32_t *>(base);
-    const T *cval = reinterpret_cast<const T *>(base + a16(4u * E));
-    const int64_t row0 = (int64_t)ta.y * BS;
-
-    for (int j = 0; j < nrhs; ++j) {
-        const T *xj = x + j;
-        // ---- phase 1a: COO products
-#pragma unroll 4
-        for (int e = lane; e < E; e += 32) {
-            const uint32_t w = __ldg(&cidx[e]);
-            const T v = __ldg(&cval[e]);
-            const T p = v * ldg(&xj[(int64_t)(w & kColMask) * ldx]);
-            S.prod[e] = p;
-            S.rowb[e] = (uint8_t)(w >> 27);
+    auto grab = [&]() -> int64_t {
+        uint32_t t = 0;
+        if (lane == 0) t = atomicAdd(&sched[0], 1u);
+        return (int64_t)__shfl_sync(kFull, t, 0);
+    };
+    int64_t tile = grab();
+    uint4 na = make_uint4(0, 0, 0, 0), nb4 = na;
+    if (tile < ntiles) {
+        na = __ldg(&tiles[2 * tile]);
+        nb4 = __ldg(&tiles[2 * tile + 1]);
+    }
+    while (tile < ntiles) {
+        const uint4 ta = na;   // begin, row, counts, pay16
+        const uint4 tb = nb4;  // E, slot, first, ntiles
+        const int64_t next = grab();
+        if (next < ntiles) {
+            na = __ldg(&tiles[2 * next]);
+            nb4 = __ldg(&tiles[2 * next + 1]);
         }
-        // ---- phase 1b: x tiles of CSR/DENSE blocks
-        for (int t0 = 0; t0 < nxt * BS; t0 += 32) {
-            const int t = t0 + lane;
-            const int jb = min(t / BS, nxt - 1);
-            const uint32_t xb = __shfl_sync(kFull, bd.z, ncoo + jb);
-            const uint32_t mb = __shfl_sync(kFull, bd.y, ncoo + jb);
-            const int c = t % BS;
-            const int valid = (mb >> 14) & 63;
-            if (t < nxt * BS) {
-                T xv = T(0);
-                if (c < valid) {
-                    const int64_t col = gather ? (int64_t)__ldg(&block_cols[xb + c])
-                                               : (int64_t)(xb + c);
-                    xv = ldg(&xj[col * ldx]);
-                }
-                S.xt[t] = xv;
-            }
-        }
-        for (int t = lane; t < 2 * BS; t += 32) (&S.acc[0][0])[t] = T(0);
-        __syncwarp();
+        const int nb = ta.z & 0xff;
+        const int ncoo = (ta.z >> 8) & 0xff;
+        const int nxt = (ta.z >> 16) & 0xff;
+        const int E = (int)tb.x;
+        const uint8_t *base = payload + (size_t)ta.w * 16;
+        uint4 bd = make_uint4(0, 0, 0, 0);
+        if (lane < nb) bd = __ldg(&blocks[ta.x + lane]);
+        const uint32_t *cidx = reinterpret_cast<const uint32_t *>(base);
+        const T *cval = reinterpret_cast<const T *>(base + a16(4u * E));
+        const int64_t row0 = (int64_t)ta.y * BS;
 
-        // ---- phase 2a: COO blocks
-        int i = 0;
-        while (i < ncoo) {
-            const uint32_t m0 = __shfl_sync(kFull, bd.y, i);
-            const uint32_t m1 = __shfl_sync(kFull, bd.y, min(i + 1, 31));
-            const int k0 = (m0 >> 3) & 2047;
-            const int k1 = (i + 1 < ncoo) ? (int)((m1 >> 3) & 2047) : 1 << 20;
-            if (k0 <= 16 && k1 <= 16) {
-                const int h = lane >> 4, hl = lane & 15;
-                const uint32_t off = __shfl_sync(kFull, bd.x, i + h);
-                const int k = h ? k1 : k0;
-                const int steps = max((int)((m0 >> 20) & 7), (int)((m1 >> 20) & 7));
-                const bool act = hl < k;
-                T p = act ? S.prod[off + hl] : T(0);
-                int r = act ? (int)S.rowb[off + hl] : 64 + hl;
-                for (int s = 0; s < steps; ++s) {
-                    const int d = 1 << s;
-                    const T pu = __shfl_up_sync(kFull, p, d, 16);
-                    const int ru = __shfl_up_sync(kFull, r, d, 16);
-                    if (hl >= d && ru == r) p += pu;
-                }
-                const int rn = __shfl_down_sync(kFull, r, 1, 16);
-                if (act && (hl == k - 1 || rn != r)) S.acc[h][r] += p;
-                __syncwarp();
-                i += 2;
-            } else {
-                const uint32_t off = __shfl_sync(kFull, bd.x, i);
-                const int steps = (m0 >> 20) & 7;
-                for (int b = 0; b < k0; b += 32) {
-                    const int q = b + lane;
-                    const bool act = q < k0;
-                    T p = act ? S.prod[off + q] : T(0);
-                    int r = act ? (int)S.rowb[off + q] : 64 + lane;
-                    for (int s = 0; s < steps; ++s) {
-                        const int d = 1 << s;
-                        const T pu = __shfl_up_sync(kFull, p, d);
-                        const int ru = __shfl_up_sync(kFull, r, d);
-                        if (lane >= d && ru == r) p += pu;
+        for (int j = 0; j < nrhs; ++j) {
+            const T *xj = x + j;
+            // x tiles of CSR/DENSE blocks (through the gather list if any)
+            for (int t0 = 0; t0 < nxt * BS; t0 += 32) {
+                const int t = t0 + lane;
+                const int jb = min(t / BS, nxt - 1);
+                const uint32_t xb = __shfl_sync(kFull, bd.z, ncoo + jb);
+                const uint32_t mb = __shfl_sync(kFull, bd.y, ncoo + jb);
+                const int c = t % BS;
+                const int valid = (mb >> 14) & 63;
+                if (t < nxt * BS) {
+                    T xv = T(0);
+                    if (c < valid) {
+                        const int64_t col = gather ? (int64_t)__ldg(&block_cols[xb + c])
+                                                   : (int64_t)(xb + c);
+                        xv = ldg(&xj[col * ldx]);
                     }
-                    const int rn = __shfl_down_sync(kFull, r, 1);
-                    if (act && (q == k0 - 1 || lane == 31 || rn != r))
-                        S.acc[0][r] += p;
-                    __syncwarp();
+                    S.xt[t] = xv;
                 }
-                i += 1;
             }
-        }
+            __syncwarp();
 
-        // ---- phase 2b: CSR and DENSE blocks
-        for (int jb = 0; jb < nxt; ++jb) {
-            const uint32_t off = __shfl_sync(kFull, bd.x, ncoo + jb);
-            const uint32_t mb = __shfl_sync(kFull, bd.y, ncoo + jb);
-            const int k = (mb >> 3) & 2047;
-            const uint8_t *pb = base + off;
-            const T *xt = &S.xt[jb * BS];
-            if ((mb & 3) == 1) {
-                using IdxT = typename std::conditional<BS == 16, uint8_t, uint16_t>::type;
-                const IdxT *rp = reinterpret_cast<const IdxT *>(pb);
-                const IdxT *ci = rp + BS + 1;
-                const T *vv = reinterpret_cast<const T *>(
-                    pb + a16((uint32_t)((BS + 1 + k) * sizeof(IdxT))));
-                constexpr int L = 32 / BS;
-                const int row = lane / L, sub = lane % L;
-                const int kb = __ldg(&rp[row]), ke = __ldg(&rp[row + 1]);
-                T sum = T(0);
-                for (int q = kb + sub; q < ke; q += L)
-                    sum += __ldg(&vv[q]) * xt[__ldg(&ci[q])];
-                if (L == 2) sum += __shfl_xor_sync(kFull, sum, 1);
-                if (sub == 0) S.acc[0][row] += sum;
-            } else {
-                const T *vv = reinterpret_cast<const T *>(pb);
-                T sum = T(0);
-                if (BS == 16) {
-                    const int row = lane >> 1, c0 = (lane & 1) * 8;
+            // COO entries: each adds val * x[col] into its row (the
+            // reference's per-entry accumulate_output, cb-spmv-dcu.hpp:
+            // 423-426), here into the lane's private accumulator.
+            for (int c0 = 0; c0 < E; c0 += 32 * kChunk) {
+                uint32_t w[kChunk];
+                T v[kChunk], xv[kChunk];
 #pragma unroll
-                    for (int c = 0; c < 8; ++c)
-                        sum += __ldg(&vv[row * 16 + c0 + c]) * xt[c0 + c];
-                    sum += __shfl_xor_sync(kFull, sum, 1);
-                    if ((lane & 1) == 0) S.acc[0][row] += sum;
-                } else {
-#pragma unroll 8
-                    for (int c = 0; c < BS; ++c)
-                        sum += __ldg(&vv[lane * BS + c]) * xt[c];
-                    S.acc[0][lane] += sum;
-                }
-            }
-            __syncwarp();
-        }
-
-        // ---- phase 3: output
-        T s = T(0);
-        if (lane < BS) s = S.acc[0][lane] + S.acc[1][lane];
-        const int64_t grow = row0 + lane;
-        if (tb.y == 0xffffffffu) {
-            if (lane < BS && grow < m) y[grow * ldy + j] = s;
-        } else {
-            T *part = partials + ((size_t)tb.y * nrhs + j) * BS;
-            if (lane < BS) part[lane] = s;
-            __threadfence();
-            __syncwarp();
-            int last = 0;
-            if (lane == 0) {
-                const int old = atomicAdd(&counters[ta.y], 1);
-                last = old == (int)(tb.w * nrhs) - 1;
-            }
-            last = __shfl_sync(kFull, last, 0);
-            if (last) {
-                __threadfence();
-                if (lane < BS) {
-                    for (int jj = 0; jj < nrhs; ++jj) {
-                        T tot = T(0);
-                        for (uint32_t t = 0; t < tb.w; ++t)
-                            tot += __ldcg(&partials[((size_t)(tb.z + t) * nrhs + jj) * BS + lane]);
-                        if (grow < m) y[grow * ldy + jj] = tot;
+                for (int u = 0; u < kChunk; ++u) {
+                    const int e = c0 + u * 32 + lane;
+                    w[u] = 0;
+                    v[u] = T(0);
+                    if (e < E) {
+                        w[u] = __ldg(&cidx[e]);
+                        v[u] = __ldg(&cval[e]);
                     }
                 }
-                if (lane == 0) atomicExch(&counters[ta.y], 0);
+#pragma unroll
+                for (int u = 0; u < kChunk; ++u) {
+                    const int e = c0 + u * 32 + lane;
+                    xv[u] = e < E ? ldg(&xj[(int64_t)(w[u] & kColMask) * ldx]) : T(0);
+                }
+#pragma unroll
+                for (int u = 0; u < kChunk; ++u) {
+                    const int e = c0 + u * 32 + lane;
+                    if (e < E) myacc[w[u] >> 27] += v[u] * xv[u];
+                }
+            }
+
+            // CSR and DENSE blocks
+            for (int jb = 0; jb < nxt; ++jb) {
+                const uint32_t off = __shfl_sync(kFull, bd.x, ncoo + jb);
+                const uint32_t mb = __shfl_sync(kFull, bd.y, ncoo + jb);
+                const int k = (mb >> 3) & 2047;
+                const uint8_t *pb = base + off;
+                const T *xt = &S.xt[jb * BS];
+                if ((mb & 3) == 1) {
+                    using IdxT = typename std::conditional<BS == 16, uint8_t, uint16_t>::type;
+                    const IdxT *rp = reinterpret_cast<const IdxT *>(pb);
+                    const IdxT *ci = rp + BS + 1;
+                    const T *vv = reinterpret_cast<const T *>(
+                        pb + a16((uint32_t)((BS + 1 + k) * sizeof(IdxT))));
+                    constexpr int L = 32 / BS;
+                    const int row = lane / L, sub = lane % L;
+                    const int kb = __ldg(&rp[row]), ke = __ldg(&rp[row + 1]);
+                    T sum = T(0);
+                    for (int q = kb + sub; q < ke; q += L)
+                        sum += __ldg(&vv[q]) * xt[__ldg(&ci[q])];
+                    myacc[row] += sum;
+                } else {
+                    const T *vv = reinterpret_cast<const T *>(pb);
+                    T sum = T(0);
+                    if (BS == 16) {
+                        const int row = lane >> 1, c0 = (lane & 1) * 8;
+#pragma unroll
+                        for (int c = 0; c < 8; ++c)
+                            sum += __ldg(&vv[row * 16 + c0 + c]) * xt[c0 + c];
+                        myacc[row] += sum;
+                    } else {
+#pragma unroll 8
+                        for (int c = 0; c < BS; ++c)
+                            sum += __ldg(&vv[lane * BS + c]) * xt[c];
+                        myacc[lane] += sum;
+                    }
+                }
+            }
+            __syncwarp();
+            const T s = reduce_rows<T, BS>(S.acc, lane);
+            __syncwarp();
+
+            // output: whole block row -> y; split row -> partial slot, and the
+            // last tile to arrive adds the row's partials in tile order
+            const int64_t grow = row0 + lane;
+            if (tb.y == 0xffffffffu) {
+                if (lane < BS && grow < m) y[grow * ldy + j] = s;
+            } else {
+                T *part = partials + ((size_t)tb.y * nrhs + j) * BS;
+                if (lane < BS) part[lane] = s;
+                __threadfence();
+                __syncwarp();
+                int last = 0;
+                if (lane == 0) {
+                    const int old = atomicAdd(&counters[ta.y], 1);
+                    last = old == (int)(tb.w * nrhs) - 1;
+                }
+                last = __shfl_sync(kFull, last, 0);
+                if (last) {
+                    __threadfence();
+                    if (lane < BS) {
+                        for (int jj = 0; jj < nrhs; ++jj) {
+                            T tot = T(0);
+                            for (uint32_t t = 0; t < tb.w; ++t)
+                                tot += __ldcg(&partials[((size_t)(tb.z + t) * nrhs + jj) * BS + lane]);
+                            if (grow < m) y[grow * ldy + jj] = tot;
+                        }
+                    }
+                    if (lane == 0) atomicExch(&counters[ta.y], 0);
+                }
             }
         }
-        __syncwarp();
+        tile = next;
+    }
+    // this warp has made its last (failing) grab: count it out; the last warp
+    // out resets the scheduler for the next launch
+    if (lane == 0) {
+        __threadfence();
+        const uint32_t done = atomicAdd(&sched[1], 1u);
+        if (done == gridDim.x * kWarps - 1) {
+            atomicExch(&sched[0], 0u);
+            atomicExch(&sched[1], 0u);
+        }
     }
 }
 
@@ -267,26 +298,53 @@ __global__ void cb_grad_vals_kernel(int64_t nvals, const int32_t *__restrict__ v
     out[v] = s;
 }
 
-template <typename T, int BS>
-cudaError_t launch_tiles(const DevLayout &d, const void *x, void *y, int nrhs,
+template <typename T, int BS, int CH>
+cudaError_t launch_chunk(const DevLayout &d, const void *x, void *y, int nrhs,
                          int64_t ldx, int64_t ldy, cudaStream_t stream) {
     const size_t smem = sizeof(WarpSmem<T, BS>) * kWarps;
-    static bool configured = false;  // per instantiation, per process
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(cb_spmv_tile_kernel<T, BS>,
+    static int resident = 0;  // CTAs per SM, per instantiation
+    static int sms = 0;
+    if (!resident) {
+        cudaError_t e = cudaFuncSetAttribute(cb_spmv_tile_kernel<T, BS, CH>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return e;
-        configured = true;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, cb_spmv_tile_kernel<T, BS, CH>,
+                                                      kWarps * 32, smem);
+        if (resident < 1) resident = 1;
     }
-    const int64_t grid = (d.ntiles + kWarps - 1) / kWarps;
+    int64_t grid = (d.ntiles + kWarps - 1) / kWarps;
+    grid = std::min<int64_t>(grid, (int64_t)sms * resident);
     if (grid == 0) return cudaSuccess;
-    cb_spmv_tile_kernel<T, BS><<<(unsigned)grid, kWarps * 32, smem, stream>>>(
+    cb_spmv_tile_kernel<T, BS, CH><<<(unsigned)grid, kWarps * 32, smem, stream>>>(
         static_cast<const uint4 *>(d.tiles), d.ntiles,
         static_cast<const uint4 *>(d.blocks), d.payload, d.block_cols, d.gather,
         static_cast<const T *>(x), static_cast<T *>(y), d.m, nrhs, ldx, ldy,
-        static_cast<T *>(d.partials), d.counters);
+        static_cast<T *>(d.partials), d.counters, d.sched);
     return cudaGetLastError();
+}
+
+int chunk_choice(int vsz) {
+    static int forced = -1;
+    if (forced < 0) {
+        const char *e = std::getenv("CBSPMV_CHUNK");
+        forced = e ? std::atoi(e) : 0;
+    }
+    if (forced == 4 || forced == 6 || forced == 8) return forced;
+    return vsz == 8 ? 6 : 8;
+}
+
+template <typename T, int BS>
+cudaError_t launch_tiles(const DevLayout &d, const void *x, void *y, int nrhs,
+                         int64_t ldx, int64_t ldy, cudaStream_t stream) {
+    switch (chunk_choice(sizeof(T))) {
+        case 4: return launch_chunk<T, BS, 4>(d, x, y, nrhs, ldx, ldy, stream);
+        case 6: return launch_chunk<T, BS, 6>(d, x, y, nrhs, ldx, ldy, stream);
+        default: return launch_chunk<T, BS, 8>(d, x, y, nrhs, ldx, ldy, stream);
+    }
 }
 
 }  // namespace

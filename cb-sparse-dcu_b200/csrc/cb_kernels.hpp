@@ -18,6 +18,7 @@ struct DevLayout {
     int64_t m = 0, n = 0;
     void *partials = nullptr;         // slots * bs values (scratch)
     int32_t *counters = nullptr;      // gb_m arrival counters (scratch)
+    uint32_t *sched = nullptr;        // 2 scheduler counters (scratch, zeroed)
 };
 
 // y = A x; x: n rows, y: m rows, row-major with leading dims for nrhs > 1.
