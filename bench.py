@@ -1,0 +1,353 @@
+"""CB-SpMV benchmark (one JSON line on rank 0).
+
+Workload (the configuration the headline metric is quoted on): plain
+CB-SpMV, FP64, on the power-law matrix n = 2^20 (row lengths power-law with
+exponent 2.1 in [1, 20000], mean 16 nnz/row; 70% of columns within +-4096 of
+the diagonal, 30% uniform; values N(0,1); seed 1), 16x16 blocks.  Synthetic
+and seeded.  A step is one y = A x over the whole matrix.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+value       algorithmic GB/s of the whole job: the bytes of the packed CB
+            matrix the kernel must read (descriptors + payload, no padding),
+            x read once and y written once, divided by the device time of a
+            step (CUDA events, max over ranks); inputs resident in HBM.
+e2e         the same metric through the C ABI with host buffers
+            (cbspmv_spmv_host: pinned x copied in, y copied out every step).
+roofline    the tile kernel against the measured HBM copy bandwidth.
+cpu_baseline  the reference's own CPU SpMV (utils.h:98-111, compiled from its
+            headers into oracle/_ref) on a bounded sample, 1 thread as written.
+--impl reference   times that CPU SpMV as the reference arm (rank 0 only).
+
+Multi-GPU: every rank runs its own copy of the workload (replicas; SpMV of
+one matrix needs no exchange), weak scaling, timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import pathlib
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+REPO = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "cb-sparse-dcu_b200"))
+
+METRIC = "SpMV GB/s (algorithmic CB bytes / t), plain CB-SpMV FP64, power-law n=2^20"
+UNIT = "GB/s"
+WORKLOAD = ("power-law n=2^20, alpha 2.1, lengths [1,20000], mean 16 nnz/row, "
+            "70% within +-4096 of diagonal, N(0,1) values, seed 1; FP64; 16x16 blocks")
+
+
+def _peaks():
+    try:
+        d = json.loads((REPO / "MEASURED_PEAKS.json").read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _ncu_traffic():
+    """DRAM bytes per launch of the tile kernel from the committed ncu
+    summary (profiles/), or None."""
+    for p in sorted((REPO / "profiles").glob("*.md")):
+        m = re.search(r"dram_bytes_per_launch_pl_fp64\s*=\s*([0-9.eE+]+)", p.read_text())
+        if m:
+            return float(m.group(1))
+    return None
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = REPO / "gpurun_out" / f"clocks_rank{index}.csv"
+
+    def __enter__(self):
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}",
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.path.exists():
+            return None
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            f = [v.strip() for v in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def _ref_cpu(coo, x, seconds: float, max_reps: int):
+    """Times the reference's check_results_consistency (its whole CPU SpMV)
+    on the full matrix; returns (seconds per SpMV, kind, reps)."""
+    import numpy as np
+    sys.path.insert(0, str(REPO / "tests"))
+    import cbdump as cd  # the oracle/_ref loader (checker only)
+    lib = cd.ref_lib(16, 1)
+    row, col, val = (np.ascontiguousarray(a) for a in (coo.row, coo.col, coo.val))
+    xv = np.ascontiguousarray(x, np.float64)
+    if lib is not None:
+        P = ctypes.c_void_p
+        ctx = lib.cbref_spmv_prepare(coo.m, coo.n, coo.nnz, row.ctypes.data_as(P),
+                                     col.ctypes.data_as(P), val.ctypes.data_as(P),
+                                     xv.ctypes.data_as(P))
+        y = cd.oracle_spmv(coo, xv)
+        lib.cbref_spmv_set_y(ctx, y.ctypes.data_as(P))
+        run = lambda: lib.cbref_spmv_check(ctx)  # noqa: E731
+        kind = "reference"
+    else:
+        run = lambda: cd.oracle_spmv(coo, xv)  # noqa: E731
+        kind = "port"
+    run()
+    reps, t0 = 0, time.perf_counter()
+    while reps < max_reps and (time.perf_counter() - t0 < seconds or reps < 2):
+        run()
+        reps += 1
+    dt = (time.perf_counter() - t0) / reps
+    if lib is not None:
+        lib.cbref_spmv_free(ctx)
+    return dt, kind, reps
+
+
+def _row_prefix(coo, nnz_target: int):
+    """The first rows of coo holding about nnz_target nonzeros (a bounded
+    sample with the workload's row distribution)."""
+    import numpy as np
+    from cbspmv.gen import Coo
+    k = int(min(coo.nnz, max(1, nnz_target)))
+    rows = int(coo.row[k - 1]) + 1
+    k = int(np.searchsorted(coo.row, rows))
+    return Coo(rows, coo.n, coo.row[:k], coo.col[:k], coo.val[:k])
+
+
+def reference_arm(args, budget_s: float = 150.0):
+    world, rank, _ = _dist()
+    if rank != 0:
+        return
+    from cbspmv import gen
+    import cbspmv
+    coo = gen.power_law()
+    x = gen.uniform_x(coo.n, 0)
+    alg = cbspmv.Plan(coo).info()["algorithmic_bytes"]
+    # size each step so that warm-up + timed steps fit the time budget
+    t_full, kind, _ = _ref_cpu(coo, x, 0.0, 1)
+    frac = min(1.0, budget_s / max(1, args.steps + args.warmup) / t_full)
+    sample = _row_prefix(coo, int(frac * coo.nnz)) if frac < 1.0 else coo
+    share = sample.nnz / coo.nnz
+    _ref_cpu(sample, x, 0.0, max(1, args.warmup))
+    dt, kind, reps = _ref_cpu(sample, x, 1e9, max(1, args.steps))
+    value = alg * share / dt / 1e9
+    desc = (f"{reps} steps, each the reference's CPU SpMV (check_results_consistency, "
+            f"utils.h:85-136, serial as written) over the first {sample.m} rows "
+            f"({sample.nnz} nnz, {share:.4f} of the workload); a full SpMV takes "
+            f"{t_full * 1e3:.1f} ms")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT,
+        "n_gpus": world, "steps": reps, "warmup": args.warmup,
+        "ms_per_step": round(dt * 1e3, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "nnz": coo.nnz, "algorithmic_bytes": alg,
+                   "parallelism": "rank 0 only (CPU)"},
+        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": 1, "kind": kind,
+                         "sample": desc},
+        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--warmup", type=int, default=50)
+    ap.add_argument("--impl", default="cbspmv", choices=["cbspmv", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=300)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+
+    import numpy as np
+    import torch
+    import cbspmv
+    from cbspmv import gen
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+        pg = dist
+
+    coo = gen.power_law()
+    x_host = gen.uniform_x(coo.n, 0)
+    plan = cbspmv.Plan(coo)
+    info = plan.info()
+    alg = info["algorithmic_bytes"]
+    x = torch.from_numpy(x_host).to(dev)
+    y = torch.empty(coo.m, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream()
+
+    # correctness gate: the bench does not report a wrong kernel
+    plan.spmv(x, y)
+    torch.cuda.synchronize()
+    sys.path.insert(0, str(REPO / "tests"))
+    import cbdump as cd
+    yref, ab = cd.oracle_spmm_ld(coo, x_host[None, :])
+    err = float(np.max(np.abs(y.cpu().numpy() - yref[0]) / (ab[0] + 1e-300)))
+    if err > 1e-12:
+        raise SystemExit(f"bench: SpMV error {err:.3g} above 1e-12")
+
+    for _ in range(args.warmup):
+        plan.spmv(x, y)
+    launches0 = cbspmv.launch_count()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            plan.spmv(x, y)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
+    launches = cbspmv.launch_count() - launches0
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if pg:
+        t = torch.tensor([ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * alg / (ms * 1e-3) / 1e9
+    gflops = world * 2.0 * coo.nnz / (ms * 1e-3) / 1e9
+
+    # end to end through the C ABI with host buffers (pinned)
+    xp = torch.from_numpy(x_host).pin_memory()
+    yp = torch.empty(coo.m, dtype=torch.float64).pin_memory()
+    lib = cbspmv.lib()
+    P = ctypes.c_void_p
+    sptr = P(stream.cuda_stream)
+    for _ in range(3):
+        lib.cbspmv_spmv_host(plan._h, P(xp.data_ptr()), P(yp.data_ptr()), 1, sptr)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        rc = lib.cbspmv_spmv_host(plan._h, P(xp.data_ptr()), P(yp.data_ptr()), 1, sptr)
+        if rc:
+            raise SystemExit(f"spmv_host failed: {cbspmv.last_error()}")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e0.elapsed_time(e1) / args.e2e_steps
+    if pg:
+        t = torch.tensor([ms_e2e], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms_e2e = float(t.item())
+    e2e_value = world * alg / (ms_e2e * 1e-3) / 1e9
+
+    peak, peak_kind = _peaks()
+    achieved = alg / (ms * 1e-3) / 1e9
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+            "traffic": _ncu_traffic(), "kernel": "cb_spmv tile kernel"}
+
+    line = None
+    if rank == 0:
+        cpu_dt, kind, reps = _ref_cpu(coo, x_host, args.cpu_seconds, 400)
+        cpu = {"value": round(alg / cpu_dt / 1e9, 3), "unit": UNIT, "cores": 1, "kind": kind,
+               "sample": f"{reps} full SpMVs of the workload on 1 host thread "
+                         "(check_results_consistency, utils.h:85-136)",
+               "ms_per_spmv": round(cpu_dt * 1e3, 3)}
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 5),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded power-law matrix, x ~ U[-1,1])",
+            "config": {"workload": WORKLOAD, "nnz": coo.nnz, "m": coo.m,
+                       "algorithmic_bytes": alg, "device_bytes": info["device_bytes"],
+                       "tiles": info["tiles"], "coo_blocks": info["coo_blocks"],
+                       "gather": info["gather_flag"],
+                       "l2": "inputs larger than L2 (packed matrix > 126 MB)",
+                       "parallelism": f"replicas x{world}"},
+            "gflops": round(gflops, 2),
+            "e2e": {"value": round(e2e_value, 3), "unit": UNIT,
+                    "h2d_bytes_per_step": coo.n * 8, "d2h_bytes_per_step": coo.m * 8,
+                    "ms_per_step": round(ms_e2e, 4)},
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+        }
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    if line:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()
