@@ -227,16 +227,11 @@ def main():
     import cbspmv
     from cbspmv import gen
 
+    from cbspmv.dist import Group
     world, rank, local = _dist()
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    pg = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=dev)
-        pg = dist
+    pg = Group("nccl", dev)
 
     coo = gen.power_law()
     x_host = gen.uniform_x(coo.n, 0)
@@ -260,8 +255,7 @@ def main():
     for _ in range(args.warmup):
         plan.spmv(x, y)
     launches0 = cbspmv.launch_count()
-    if pg:
-        pg.barrier()
+    pg.barrier()
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -271,14 +265,9 @@ def main():
             plan.spmv(x, y)
         ev1.record(stream)
         torch.cuda.synchronize()
-    if pg:
-        pg.barrier()
+    pg.barrier()
     launches = cbspmv.launch_count() - launches0
-    ms = ev0.elapsed_time(ev1) / args.steps
-    if pg:
-        t = torch.tensor([ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = pg.max(ev0.elapsed_time(ev1) / args.steps)
     value = world * alg / (ms * 1e-3) / 1e9
     gflops = world * 2.0 * coo.nnz / (ms * 1e-3) / 1e9
 
@@ -290,8 +279,7 @@ def main():
     sptr = P(stream.cuda_stream)
     for _ in range(3):
         lib.cbspmv_spmv_host(plan._h, P(xp.data_ptr()), P(yp.data_ptr()), 1, sptr)
-    if pg:
-        pg.barrier()
+    pg.barrier()
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -302,11 +290,7 @@ def main():
             raise SystemExit(f"spmv_host failed: {cbspmv.last_error()}")
     e1.record(stream)
     torch.cuda.synchronize()
-    ms_e2e = e0.elapsed_time(e1) / args.e2e_steps
-    if pg:
-        t = torch.tensor([ms_e2e], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms_e2e = float(t.item())
+    ms_e2e = pg.max(e0.elapsed_time(e1) / args.e2e_steps)
     e2e_value = world * alg / (ms_e2e * 1e-3) / 1e9
 
     peak, peak_kind = _peaks()
@@ -342,9 +326,7 @@ def main():
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
-    if pg:
-        pg.barrier()
-        pg.destroy_process_group()
+    pg.close()
     if line:
         print(json.dumps(line), flush=True)
 
