@@ -282,6 +282,38 @@ cbspmv_status cbspmv_spmv(cbspmv_plan *p, const void *x, void *y, int nrhs,
     return run_side(p, p->A, x, y, nrhs, ldx, ldy, (cudaStream_t)stream);
 }
 
+cbspmv_status cbspmv_spmv_noalloc(cbspmv_plan *p, const void *x, void *y, int nrhs,
+                                  int64_t ldx, int64_t ldy, void *stream) {
+    if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
+    if (!p->uploaded) return fail(CBSPMV_ERR_STATE, "plan not uploaded");
+    if (nrhs < 1) return fail(CBSPMV_ERR_INVALID, "nrhs must be >= 1");
+    if (ldx == 0) ldx = nrhs;
+    if (ldy == 0) ldy = nrhs;
+    if (ldx < nrhs || ldy < nrhs)
+        return fail(CBSPMV_ERR_INVALID, "leading dimension smaller than nrhs");
+    DevSide &s = p->A;
+    if ((s.lay.m > 0 && !y) || (s.lay.n > 0 && !x && s.lay.nvals > 0))
+        return fail(CBSPMV_ERR_INVALID, "null x or y");
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev != p->device)
+        return fail(CBSPMV_ERR_STATE, "plan was uploaded to another device");
+    const size_t need = cb::fixed_scratch_need(s.lay.gb_m, s.lay.slots, nrhs, s.lay.bs,
+                                               s.lay.f32);
+    if (need > cb::kFixedScratchBytes)
+        return fail(CBSPMV_ERR_UNSUPPORTED,
+                    "cbspmv_spmv_noalloc: this plan needs " + std::to_string(need) +
+                        " bytes of scratch for nrhs=" + std::to_string(nrhs) +
+                        "; the fixed scratch holds " +
+                        std::to_string(cb::kFixedScratchBytes) +
+                        " bytes (use cbspmv_spmv, fewer right-hand sides or larger tiles)");
+    CB_CUDA(cb::launch_spmv_fixed_scratch(s.d, s.lay.gb_m, s.lay.slots, x, y, nrhs, ldx,
+                                          ldy, (cudaStream_t)stream),
+            "spmv_noalloc launch");
+    if (s.d.ntiles > 0) g_launches++;
+    return CBSPMV_OK;
+}
+
 cbspmv_status cbspmv_spmv_t(cbspmv_plan *p, const void *g, void *gx, int nrhs,
                             int64_t ldg, int64_t ldgx, void *stream) {
     if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");

@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstdlib>
+#include <mutex>
 #include <type_traits>
 
 #include "cb_kernels.hpp"
@@ -362,6 +363,60 @@ cudaError_t launch_spmv(const DevLayout &d, const void *x, void *y, int nrhs,
                      : launch_tiles<double, 16>(d, x, y, nrhs, ldx, ldy, stream);
     return d.f32 ? launch_tiles<float, 32>(d, x, y, nrhs, ldx, ldy, stream)
                  : launch_tiles<double, 32>(d, x, y, nrhs, ldx, ldy, stream);
+}
+
+// ---- fixed scratch, for callers that may not allocate device memory -------
+// A file-scope device array replaces the plan's own scratch (scheduler words,
+// per-block-row arrival counters, split-row partial sums).  Every GPU that
+// loads this library holds it until the process exits.
+static __device__ __align__(256) unsigned char g_fixed_scratch[kFixedScratchBytes];
+
+namespace {
+// Device address of g_fixed_scratch on the current device, looked up once per
+// device (the host-side symbol is not a device address).
+cudaError_t fixed_scratch_ptr(void **ptr) {
+    static std::mutex mu;
+    static void *addr[64] = {};
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_fixed_scratch);
+        if (e != cudaSuccess) return e;
+        addr[dev] = p;
+    }
+    *ptr = addr[dev];
+    return cudaSuccess;
+}
+}  // namespace
+
+size_t fixed_scratch_need(int64_t gb_m, int64_t slots, int nrhs, int bs, int f32) {
+    const size_t words = 16 + 4 * (size_t)gb_m;  // 4 scheduler words, counters
+    const size_t head = (words + 255) & ~size_t(255);
+    return head + (size_t)slots * nrhs * bs * (f32 ? 4 : 8);
+}
+
+cudaError_t launch_spmv_fixed_scratch(const DevLayout &d, int64_t gb_m, int64_t slots,
+                                      const void *x, void *y, int nrhs, int64_t ldx,
+                                      int64_t ldy, cudaStream_t stream) {
+    if (fixed_scratch_need(gb_m, slots, nrhs, d.bs, d.f32) > kFixedScratchBytes)
+        return cudaErrorInvalidValue;
+    void *base = nullptr;
+    cudaError_t e = fixed_scratch_ptr(&base);
+    if (e != cudaSuccess) return e;
+    unsigned char *b = static_cast<unsigned char *>(base);
+    const size_t words = 16 + 4 * (size_t)gb_m;
+    // the scheduler words and arrival counters must start at zero
+    e = cudaMemsetAsync(b, 0, words, stream);
+    if (e != cudaSuccess) return e;
+    DevLayout f = d;
+    f.sched = reinterpret_cast<uint32_t *>(b);
+    f.counters = reinterpret_cast<int32_t *>(b + 16);
+    f.partials = b + ((words + 255) & ~size_t(255));
+    return launch_spmv(f, x, y, nrhs, ldx, ldy, stream);
 }
 
 cudaError_t launch_set_values(int f32, int64_t nvals, const int64_t *vsrc_ptr,

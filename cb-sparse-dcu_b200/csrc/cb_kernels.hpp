@@ -25,6 +25,17 @@ struct DevLayout {
 cudaError_t launch_spmv(const DevLayout &d, const void *x, void *y, int nrhs,
                         int64_t ldx, int64_t ldy, cudaStream_t stream);
 
+// The same SpMV with its scratch (scheduler words, arrival counters, split-row
+// partials) placed in a fixed device array of kFixedScratchBytes instead of
+// the plan's own allocations; no device memory is allocated.  Fails with
+// cudaErrorInvalidValue when the plan needs more scratch than the array holds
+// (fixed_scratch_need tells how much).
+constexpr size_t kFixedScratchBytes = size_t(8) << 20;
+size_t fixed_scratch_need(int64_t gb_m, int64_t slots, int nrhs, int bs, int f32);
+cudaError_t launch_spmv_fixed_scratch(const DevLayout &d, int64_t gb_m, int64_t slots,
+                                      const void *x, void *y, int nrhs, int64_t ldx,
+                                      int64_t ldy, cudaStream_t stream);
+
 // payload value v = sum of in[vsrc[z]] for z in [vsrc_ptr[v], vsrc_ptr[v+1])
 cudaError_t launch_set_values(int f32, int64_t nvals, const int64_t *vsrc_ptr,
                               const int32_t *vsrc, const uint64_t *val_off,

@@ -123,6 +123,26 @@ cbspmv_status cbspmv_upload(cbspmv_plan *plan, void *stream);
 cbspmv_status cbspmv_spmv(cbspmv_plan *plan, const void *x, void *y, int nrhs,
                           int64_t ldx, int64_t ldy, void *stream);
 
+/* cbspmv_spmv for callers that may not allocate device memory while they
+ * run -- e.g. a plugin whose execute step is handed only its inputs and
+ * outputs by a host framework that owns all device memory, or a serving loop
+ * with a fixed memory budget.  No counterpart in the reference (its cb_spmv
+ * allocates on every call).  The plan must already be uploaded; the caller
+ * passes x and y as for cbspmv_spmv.  The split-row partial sums, arrival
+ * counters and scheduler words this call needs live in one fixed device
+ * array of 8 MiB compiled into the library (held on every GPU that loads it
+ * until the process exits), so this call allocates nothing.  A plan needing
+ * more than 8 MiB of scratch (16 B + 4 B per block row + split tiles x nrhs
+ * x bs values) is rejected with CBSPMV_ERR_UNSUPPORTED and a message giving
+ * both sizes.  The first call on each device looks up the array's device
+ * address; make that first call before any stream capture.  All calls share
+ * the array and it keeps the last call's contents (the counters are cleared
+ * at the start of every call), so calls that overlap on the GPU -- on
+ * different streams, or from different plans -- race. */
+cbspmv_status cbspmv_spmv_noalloc(cbspmv_plan *plan, const void *x, void *y,
+                                  int nrhs, int64_t ldx, int64_t ldy,
+                                  void *stream);
+
 /* The same through host buffers: copies x to the device, runs, copies y
  * back, and synchronizes `stream`.  Device buffers are kept in the plan. */
 cbspmv_status cbspmv_spmv_host(cbspmv_plan *plan, const void *x_host,
