@@ -55,6 +55,8 @@ struct DevSide {
     int32_t *block_cols = nullptr;
     void *partials = nullptr;
     int32_t *counters = nullptr;
+    uint32_t *split = nullptr;
+    uint32_t *wpart = nullptr;
     int partial_nrhs = 0;
     int64_t *vsrc_ptr = nullptr;
     int32_t *vsrc = nullptr;
@@ -63,12 +65,13 @@ struct DevSide {
 
     void release() {
         void *ps[] = {tiles, blocks, payload, block_cols, partials, counters,
-                      vsrc_ptr, vsrc, val_off, val_row, val_col};
+                      split, wpart, vsrc_ptr, vsrc, val_off, val_row, val_col};
         for (void *p : ps)
             if (p) cudaFree(p);
         tiles = blocks = partials = nullptr;
         payload = nullptr;
         block_cols = counters = vsrc = val_row = val_col = nullptr;
+        split = wpart = nullptr;
         vsrc_ptr = nullptr;
         val_off = nullptr;
         partial_nrhs = 0;
@@ -113,10 +116,11 @@ cbspmv_status upload_side(DevSide &s, cudaStream_t st) {
     CB_CUDA(upload_vec(L.val_off, &s.val_off, st), "upload value offsets");
     CB_CUDA(upload_vec(L.val_row, &s.val_row, st), "upload value rows");
     CB_CUDA(upload_vec(L.val_col, &s.val_col, st), "upload value columns");
-    // scratch: 2 scheduler counters, then one arrival counter per block row
-    CB_CUDA(cudaMalloc((void **)&s.counters, (L.gb_m + 2) * sizeof(int32_t)),
+    // scratch: 4 scheduler words (next tile, warps done, error word, spare),
+    // then one arrival counter per block row
+    CB_CUDA(cudaMalloc((void **)&s.counters, (L.gb_m + 4) * sizeof(int32_t)),
             "allocate counters");
-    CB_CUDA(cudaMemsetAsync(s.counters, 0, (L.gb_m + 2) * sizeof(int32_t), st),
+    CB_CUDA(cudaMemsetAsync(s.counters, 0, (L.gb_m + 4) * sizeof(int32_t), st),
             "clear counters");
     s.d.tiles = s.tiles;
     s.d.blocks = s.blocks;
@@ -128,8 +132,25 @@ cbspmv_status upload_side(DevSide &s, cudaStream_t st) {
     s.d.gather = L.gather;
     s.d.m = L.m;
     s.d.n = L.n;
+    CB_CUDA(upload_vec(L.split, &s.split, st), "upload split rows");
     s.d.sched = reinterpret_cast<uint32_t *>(s.counters);
-    s.d.counters = s.counters + 2;
+    s.d.counters = s.counters + 4;
+    s.d.max_entries = L.max_entries;
+    s.d.split = s.split;
+    s.d.nsplit = (int64_t)L.split.size() / 4;
+    s.d.coo_share = L.coo_share;
+    return CBSPMV_OK;
+}
+
+// The streaming kernel's per-warp tile ranges, for this device's grid.
+cbspmv_status upload_partition(DevSide &s, int kernel, cudaStream_t st) {
+    s.d.kernel = kernel;
+    const int64_t warps = cb::stream_warps(s.d);
+    if (warps <= 0) return CBSPMV_OK;  // the direct kernel will run
+    const std::vector<uint32_t> part = cb::partition_tiles(s.lay, warps);
+    CB_CUDA(upload_vec(part, &s.wpart, st), "upload tile partition");
+    s.d.wpart = s.wpart;
+    s.d.nwarps = warps;
     return CBSPMV_OK;
 }
 
@@ -190,6 +211,7 @@ void cbspmv_default_opts(cbspmv_opts *o) {
     o->value_type = CBSPMV_F64;
     o->want_transpose = 0;
     o->tile_entries = 0;
+    o->kernel = 0;
 }
 
 cbspmv_status cbspmv_coo2block_gather(const cbspmv_coo *coo,
@@ -202,6 +224,8 @@ cbspmv_status cbspmv_coo2block_gather(const cbspmv_coo *coo,
     if (opts) o = *opts;
     if (o.value_type != CBSPMV_F64 && o.value_type != CBSPMV_F32)
         return fail(CBSPMV_ERR_INVALID, "value_type must be CBSPMV_F64 or CBSPMV_F32");
+    if (o.kernel < 0 || o.kernel > 2)
+        return fail(CBSPMV_ERR_INVALID, "kernel must be 0 (auto), 1 or 2");
     cbspmv_plan *p = new (std::nothrow) cbspmv_plan;
     if (!p) return fail(CBSPMV_ERR_ALLOC, "out of host memory");
     p->opts = o;
@@ -213,7 +237,7 @@ cbspmv_status cbspmv_coo2block_gather(const cbspmv_coo *coo,
             delete p;
             return fail(code, err);
         }
-        err = cb::build_layout(p->host, o.value_type == CBSPMV_F32, o.tile_entries,
+        err = cb::build_layout(p->host, o.value_type == CBSPMV_F32, o.tile_entries, o.kernel,
                                p->A.lay, &code);
         if (!err.empty()) {
             delete p;
@@ -239,7 +263,7 @@ cbspmv_status cbspmv_coo2block_gather(const cbspmv_coo *coo,
                                tv.data(), p->host_t, &code);
             if (err.empty())
                 err = cb::build_layout(p->host_t, o.value_type == CBSPMV_F32,
-                                       o.tile_entries, p->AT.lay, &code);
+                                       o.tile_entries, o.kernel, p->AT.lay, &code);
             if (!err.empty()) {
                 delete p;
                 return fail(code, "transpose: " + err);
@@ -265,7 +289,9 @@ cbspmv_status cbspmv_upload(cbspmv_plan *p, void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
     CB_CUDA(cudaGetDevice(&p->device), "cudaGetDevice");
     cbspmv_status rc = upload_side(p->A, st);
+    if (!rc) rc = upload_partition(p->A, p->opts.kernel, st);
     if (!rc && p->has_t) rc = upload_side(p->AT, st);
+    if (!rc && p->has_t) rc = upload_partition(p->AT, p->opts.kernel, st);
     if (rc) {
         p->A.release();
         p->AT.release();
@@ -483,7 +509,7 @@ cbspmv_status cbspmv_info_get(const cbspmv_plan *p, cbspmv_info *info) {
                                p->A.lay.payload.size() + p->A.lay.block_cols.size() * 4);
     I.algorithmic_bytes = p->A.lay.alg_bytes;
     I.scratch_bytes = (int64_t)(p->A.lay.slots * p->A.lay.bs * vsize(p) +
-                                (p->A.lay.gb_m + 2) * 4);
+                                (p->A.lay.gb_m + 4) * 4);
     *info = I;
     return CBSPMV_OK;
 }

@@ -270,6 +270,340 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
     }
 }
 
+// ============================================================================
+// Streaming tile kernel (TMA-staged), for matrices whose entries are mostly
+// in COO blocks (e.g. gathered power-law matrices).
+//   * each warp double-buffers the COO sections of its tiles in shared memory
+//     with cp.async.bulk (bulk async copies completing on an mbarrier; no
+//     multicast), so the HBM stream runs a tile ahead of the compute;
+//   * each warp owns a contiguous, cost-balanced range of tiles computed on
+//     the host for the launch's grid (no shared counter: same-address atomics
+//     on one counter cannot keep up with ~10^5 tiles per launch), and loads
+//     tile descriptors two tiles ahead of use;
+//   * the x gathers of a chunk are the only global loads on the entry path;
+//   * block rows split over several tiles leave partial sums in their slots;
+//     cb_combine_kernel adds them in tile order afterwards (no fences, no
+//     arrival counters).
+// Every mbarrier wait is bounded (kWaitLimit polls); on give-up the error
+// word sched[2] is set and the warp stops, after waiting (bounded) for its
+// own copies in flight.  sched[0..1] are not used by this kernel.
+// ============================================================================
+constexpr uint32_t kWaitLimit = 1u << 22;
+constexpr int kStreamWarps = 4;  // warps per CTA
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// orders this thread's (and, after a warp barrier, its warp's) generic
+// shared-memory accesses before later async-proxy writes (bulk copies)
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
+                     smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ uint64_t policy_evict_first() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+// global -> this CTA's shared memory, completion counted on `bar`
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
+                                         uint64_t *bar, uint64_t policy) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+        " [%0], [%1], %2, [%3], %4;" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t *err) {
+    for (uint32_t i = 0; i < kWaitLimit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    atomicExch(err, 1u);
+    return false;
+}
+
+// Per-warp shared memory: [acc | xt | mbar[2] | buf[2]]; a buffer holds one
+// tile's COO section (`cap` bytes: indices, then values).
+template <typename T, int BS>
+struct StreamLayout {
+    static constexpr uint32_t acc_bytes = 32 * (BS + 1) * sizeof(T);
+    static constexpr uint32_t xt_bytes = max_xt(BS) * BS * sizeof(T);
+    static constexpr uint32_t head = a16(acc_bytes + xt_bytes + 16);
+    __host__ __device__ static uint32_t bytes(uint32_t cap) { return head + 2 * cap; }
+};
+
+constexpr int kStreamChunk = 8;  // entries per lane: tiles hold <= 256 entries
+
+// One tile's COO entries held in registers: index words, values, gathered x.
+template <typename T>
+struct Staged {
+    uint32_t w[kStreamChunk];
+    T v[kStreamChunk];
+    T x[kStreamChunk];
+};
+
+// Reads a staged COO section into registers and issues its x gathers (the
+// loads stay in flight until the values are used).
+template <typename T>
+__device__ __forceinline__ void gather_tile(const unsigned char *buf, int E,
+                                            const T *__restrict__ x, int lane,
+                                            Staged<T> &g) {
+    const uint32_t *sidx = reinterpret_cast<const uint32_t *>(buf);
+    const T *sval = reinterpret_cast<const T *>(buf + a16(4u * E));
+#pragma unroll
+    for (int u = 0; u < kStreamChunk; ++u) {
+        const int e = u * 32 + lane;
+        g.w[u] = e < E ? sidx[e] : 0u;
+        g.v[u] = e < E ? sval[e] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < kStreamChunk; ++u) {
+        const int e = u * 32 + lane;
+        g.x[u] = e < E ? ldg(&x[g.w[u] & kColMask]) : T(0);
+    }
+}
+
+// Adds a gathered tile into the lane-private accumulators, handles its CSR and
+// DENSE blocks, reduces and stores (or leaves a split row's partials).
+template <typename T, int BS>
+__device__ __forceinline__ void finish_tile(const uint4 ta, const uint4 tb, const Staged<T> &g,
+                                            T *acc, T *xts, const uint4 *__restrict__ blocks,
+                                            const uint8_t *__restrict__ payload,
+                                            const int32_t *__restrict__ block_cols, int gather,
+                                            const T *__restrict__ x, T *__restrict__ y,
+                                            int64_t m, T *__restrict__ partials, int lane) {
+    T *myacc = &acc[lane * (BS + 1)];
+    const int E = (int)tb.x;
+#pragma unroll
+    for (int u = 0; u < kStreamChunk; ++u)
+        if (u * 32 + lane < E) myacc[g.w[u] >> 27] += g.v[u] * g.x[u];
+    const int nb = ta.z & 0xff;
+    const int ncoo = (ta.z >> 8) & 0xff;
+    const int nxtb = (ta.z >> 16) & 0xff;
+    if (nxtb) {  // CSR and DENSE blocks, read from global memory
+        const uint4 bd = lane < nb ? __ldg(&blocks[ta.x + lane]) : make_uint4(0, 0, 0, 0);
+        for (int t0 = 0; t0 < nxtb * BS; t0 += 32) {
+            const int t = t0 + lane;
+            const int jb = min(t / BS, nxtb - 1);
+            const uint32_t xb = __shfl_sync(kFull, bd.z, ncoo + jb);
+            const uint32_t mb = __shfl_sync(kFull, bd.y, ncoo + jb);
+            const int c = t % BS;
+            if (t < nxtb * BS) {
+                T xv = T(0);
+                if (c < (int)((mb >> 14) & 63)) {
+                    const int64_t col = gather ? (int64_t)__ldg(&block_cols[xb + c])
+                                               : (int64_t)(xb + c);
+                    xv = ldg(&x[col]);
+                }
+                xts[t] = xv;
+            }
+        }
+        __syncwarp();
+        const uint8_t *gbase = payload + (size_t)ta.w * 16;
+        for (int jb = 0; jb < nxtb; ++jb) {
+            const uint32_t off = __shfl_sync(kFull, bd.x, ncoo + jb);
+            const uint32_t mb = __shfl_sync(kFull, bd.y, ncoo + jb);
+            const int k = (mb >> 3) & 2047;
+            const uint8_t *pb = gbase + off;
+            const T *xt = &xts[jb * BS];
+            if ((mb & 3) == 1) {
+                using IdxT = typename std::conditional<BS == 16, uint8_t, uint16_t>::type;
+                const IdxT *rp = reinterpret_cast<const IdxT *>(pb);
+                const IdxT *ci = rp + BS + 1;
+                const T *vv = reinterpret_cast<const T *>(
+                    pb + a16((uint32_t)((BS + 1 + k) * sizeof(IdxT))));
+                constexpr int L = 32 / BS;
+                const int row = lane / L, sub = lane % L;
+                const int kb = __ldg(&rp[row]), ke = __ldg(&rp[row + 1]);
+                T sum = T(0);
+                for (int q = kb + sub; q < ke; q += L) sum += __ldg(&vv[q]) * xt[__ldg(&ci[q])];
+                myacc[row] += sum;
+            } else {
+                const T *vv = reinterpret_cast<const T *>(pb);
+                T sum = T(0);
+                if (BS == 16) {
+                    const int row = lane >> 1, cc = (lane & 1) * 8;
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) sum += __ldg(&vv[row * 16 + cc + c]) * xt[cc + c];
+                    myacc[row] += sum;
+                } else {
+#pragma unroll 8
+                    for (int c = 0; c < BS; ++c) sum += __ldg(&vv[lane * BS + c]) * xt[c];
+                    myacc[lane] += sum;
+                }
+            }
+        }
+    }
+    __syncwarp();
+    const T sum = reduce_rows<T, BS>(acc, lane);
+    __syncwarp();
+    if (lane < BS) {
+        const int64_t grow = (int64_t)ta.y * BS + lane;
+        if (tb.y == 0xffffffffu) {
+            if (grow < m) y[grow] = sum;
+        } else {
+            partials[(size_t)tb.y * BS + lane] = sum;
+        }
+    }
+}
+
+// Warp w processes its tiles i = 0, 1, ... of wpart[w] .. wpart[w+1] in a
+// software pipeline: in step i it waits for tile i+1's staged COO section,
+// reads it into registers and issues its x gathers, starts the bulk copy of
+// tile i+3 into the buffer just read, and only then adds up tile i (whose
+// gathers were issued one step earlier).  Tile i lives in buffer i % 2.
+template <typename T, int BS>
+__global__ void __launch_bounds__(kStreamWarps * 32)
+    cb_spmv_stream_kernel(const uint4 *__restrict__ tiles, int64_t ntiles,
+                          const uint4 *__restrict__ blocks,
+                          const uint8_t *__restrict__ payload,
+                          const int32_t *__restrict__ block_cols, int gather,
+                          const T *__restrict__ x, T *__restrict__ y, int64_t m,
+                          T *__restrict__ partials, uint32_t *__restrict__ sched,
+                          const uint32_t *__restrict__ wpart, uint32_t cap) {
+    using SL = StreamLayout<T, BS>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    unsigned char *wbase = smem_raw + (size_t)wib * SL::bytes(cap);
+    T *acc = reinterpret_cast<T *>(wbase);
+    T *xts = reinterpret_cast<T *>(wbase + SL::acc_bytes);
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(wbase + SL::acc_bytes + SL::xt_bytes);
+    unsigned char *const buf0 = wbase + SL::head;  // buffer b at buf0 + b * cap
+    constexpr uint32_t vsz = sizeof(T);
+    const uint64_t pol = policy_evict_first();
+
+    for (int t = lane; t < 32 * (BS + 1); t += 32) acc[t] = T(0);
+    if (lane == 0) {
+        mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
+        fence_mbar_init();
+    }
+    __syncwarp();
+
+    const int64_t gw = (int64_t)blockIdx.x * kStreamWarps + wib;
+    const int64_t t0 = __ldg(&wpart[gw]);
+    const int64_t nt = min((int64_t)__ldg(&wpart[gw + 1]), ntiles) - t0;  // my tiles
+    if (nt <= 0) return;
+    auto desc = [&](int64_t i, uint4 &a, uint4 &b) {
+        if (i < nt) {
+            a = __ldg(&tiles[2 * (t0 + i)]);
+            b = __ldg(&tiles[2 * (t0 + i) + 1]);
+        }
+    };
+    auto stage = [&](const uint4 &a, const uint4 &b, int bi) {
+        if (lane == 0) {
+            const uint32_t bytes = a16(4u * b.x) + a16(vsz * b.x);
+            if (bytes == 0) {
+                mbar_arrive(&mbar[bi]);
+            } else {
+                fence_proxy_async();  // the buffer's previous tile was read
+                mbar_arrive_tx(&mbar[bi], bytes);
+                bulk_g2s(buf0 + bi * cap, payload + (size_t)a.w * 16, bytes, &mbar[bi], pol);
+            }
+        }
+    };
+    uint32_t phase = 0u;     // bit b: parity to wait for on mbar[b]
+    uint32_t inflight = 0u;  // bit b: a copy into buffer b is outstanding
+    auto wait_buf = [&](int bi) -> bool {
+        const bool ok = mbar_wait(&mbar[bi], (phase >> bi) & 1u, &sched[2]);
+        phase ^= 1u << bi;
+        inflight &= ~(1u << bi);
+        return ok;
+    };
+
+    // descriptors of tiles i .. i+4 (d0 = the tile being added up)
+    uint4 a0 = make_uint4(0, 0, 0, 0), b0 = a0, a1 = a0, b1 = a0, a2 = a0, b2 = a0,
+          a3 = a0, b3 = a0, a4 = a0, b4 = a0;
+    desc(0, a0, b0);
+    desc(1, a1, b1);
+    desc(2, a2, b2);
+    desc(3, a3, b3);
+    stage(a0, b0, 0);
+    inflight |= 1u;
+    if (nt > 1) {
+        stage(a1, b1, 1);
+        inflight |= 2u;
+    }
+    Staged<T> g0, g1;  // tile i's registers, tile i+1's registers
+    bool ok = wait_buf(0);
+    if (ok) gather_tile(buf0, (int)b0.x, x, lane, g0);
+    __syncwarp();
+    if (ok && nt > 2) {
+        stage(a2, b2, 0);
+        inflight |= 1u;
+    }
+    for (int64_t i = 0; ok && i < nt; ++i) {
+        const int nb = (int)((i + 1) & 1);  // buffer of tile i+1
+        desc(i + 4, a4, b4);
+        if (i + 1 < nt) {
+            if (!wait_buf(nb)) break;
+            gather_tile(buf0 + nb * cap, (int)b1.x, x, lane, g1);
+            __syncwarp();
+            if (i + 3 < nt) {
+                stage(a3, b3, nb);
+                inflight |= 1u << nb;
+            }
+        }
+        finish_tile<T, BS>(a0, b0, g0, acc, xts, blocks, payload, block_cols, gather, x, y, m,
+                           partials, lane);
+        g0 = g1;
+        a0 = a1; b0 = b1;
+        a1 = a2; b1 = b2;
+        a2 = a3; b2 = b3;
+        a3 = a4; b3 = b4;
+    }
+    // never leave with a bulk copy still writing this warp's buffers
+    for (int q = 0; q < 2; ++q)
+        if ((inflight >> q) & 1u) mbar_wait(&mbar[q], (phase >> q) & 1u, &sched[2]);
+    __syncwarp();
+}
+
+// One warp per split block row: its y rows = the sum of the row's tile
+// partials, in tile order (split = {block_row, first_slot, tiles, 0}).
+template <typename T, int BS>
+__global__ void __launch_bounds__(128)
+    cb_combine_kernel(const uint4 *__restrict__ split, int64_t nsplit,
+                      const T *__restrict__ partials, T *__restrict__ y, int64_t m,
+                      int nrhs, int64_t ldy) {
+    const int lane = threadIdx.x & 31;
+    const int64_t w = (int64_t)blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (w >= nsplit || lane >= BS) return;
+    const uint4 d = __ldg(&split[w]);
+    const int64_t grow = (int64_t)d.x * BS + lane;
+    if (grow >= m) return;
+    for (int j = 0; j < nrhs; ++j) {
+        T tot = T(0);
+        for (uint32_t t = 0; t < d.z; ++t)
+            tot += partials[((size_t)(d.y + t) * nrhs + j) * BS + lane];
+        y[grow * ldy + j] = tot;
+    }
+}
+
 template <typename T>
 __global__ void cb_set_values_kernel(int64_t nvals, const int64_t *__restrict__ ptr,
                                      const int32_t *__restrict__ src,
@@ -339,8 +673,81 @@ int chunk_choice(int vsz) {
 }
 
 template <typename T, int BS>
+struct StreamConfig {
+    uint32_t cap = 0;
+    size_t smem = 0;
+    int64_t warps = 0;  // warps one launch can keep resident
+};
+
+template <typename T, int BS>
+cudaError_t stream_config(const DevLayout &d, StreamConfig<T, BS> &c) {
+    using SL = StreamLayout<T, BS>;
+    const uint32_t E = (uint32_t)d.max_entries;
+    c.cap = std::max<uint32_t>(16, a16(4u * E) + a16((uint32_t)sizeof(T) * E));
+    c.smem = (size_t)SL::bytes(c.cap) * kStreamWarps;
+    static size_t configured = 0;  // largest dynamic smem enabled so far
+    static int sms = 0;
+    if (c.smem > configured) {
+        cudaError_t e = cudaFuncSetAttribute(cb_spmv_stream_kernel<T, BS>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)c.smem);
+        if (e != cudaSuccess) return e;
+        configured = c.smem;
+    }
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    int resident = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &resident, cb_spmv_stream_kernel<T, BS>, kStreamWarps * 32, c.smem);
+    if (e != cudaSuccess) return e;
+    if (resident < 1) resident = 1;
+    const int64_t need = (d.ntiles + kStreamWarps - 1) / kStreamWarps * kStreamWarps;
+    c.warps = std::max<int64_t>(kStreamWarps,
+                                std::min<int64_t>((int64_t)sms * resident * kStreamWarps, need));
+    return cudaSuccess;
+}
+
+template <typename T, int BS>
+cudaError_t launch_stream(const DevLayout &d, const void *x, void *y, cudaStream_t stream) {
+    StreamConfig<T, BS> c;
+    cudaError_t e = stream_config(d, c);
+    if (e != cudaSuccess) return e;
+    if (d.ntiles == 0) return cudaSuccess;
+    if (!d.wpart || d.nwarps % kStreamWarps || d.max_entries > 32 * kStreamChunk)
+        return cudaErrorInvalidValue;
+    cb_spmv_stream_kernel<T, BS>
+        <<<(unsigned)(d.nwarps / kStreamWarps), kStreamWarps * 32, c.smem, stream>>>(
+            static_cast<const uint4 *>(d.tiles), d.ntiles,
+            static_cast<const uint4 *>(d.blocks), d.payload, d.block_cols, d.gather,
+            static_cast<const T *>(x), static_cast<T *>(y), d.m,
+            static_cast<T *>(d.partials), d.sched, d.wpart, c.cap);
+    e = cudaGetLastError();
+    if (e != cudaSuccess || d.nsplit == 0) return e;
+    const unsigned cgrid = (unsigned)((d.nsplit + 3) / 4);
+    cb_combine_kernel<T, BS><<<cgrid, 128, 0, stream>>>(
+        static_cast<const uint4 *>(d.split), d.nsplit,
+        static_cast<const T *>(d.partials), static_cast<T *>(y), d.m, 1, 1);
+    return cudaGetLastError();
+}
+
+// Streaming kernel for COO-dominant matrices, the direct kernel otherwise
+// (or as chosen by the plan's kernel option).
+// (single right-hand side; several go through the direct kernel)
+bool use_stream(const DevLayout &d) {
+    if (d.max_entries > 32 * kStreamChunk) return false;
+    if (d.kernel == 1) return true;
+    if (d.kernel == 2) return false;
+    return d.coo_share >= 0.5;
+}
+
+template <typename T, int BS>
 cudaError_t launch_tiles(const DevLayout &d, const void *x, void *y, int nrhs,
                          int64_t ldx, int64_t ldy, cudaStream_t stream) {
+    if (nrhs == 1 && ldx == 1 && ldy == 1 && use_stream(d))
+        return launch_stream<T, BS>(d, x, y, stream);
     switch (chunk_choice(sizeof(T))) {
         case 4: return launch_chunk<T, BS, 4>(d, x, y, nrhs, ldx, ldy, stream);
         case 6: return launch_chunk<T, BS, 6>(d, x, y, nrhs, ldx, ldy, stream);
@@ -354,6 +761,19 @@ size_t spmv_smem_bytes(int bs, int f32) {
     if (bs == 16)
         return kWarps * (f32 ? sizeof(WarpSmem<float, 16>) : sizeof(WarpSmem<double, 16>));
     return kWarps * (f32 ? sizeof(WarpSmem<float, 32>) : sizeof(WarpSmem<double, 32>));
+}
+
+template <typename T, int BS>
+int64_t stream_warps_t(const DevLayout &d) {
+    if (!use_stream(d)) return 0;
+    StreamConfig<T, BS> c;
+    if (stream_config(d, c) != cudaSuccess) return 0;
+    return c.warps;
+}
+
+int64_t stream_warps(const DevLayout &d) {
+    if (d.bs == 16) return d.f32 ? stream_warps_t<float, 16>(d) : stream_warps_t<double, 16>(d);
+    return d.f32 ? stream_warps_t<float, 32>(d) : stream_warps_t<double, 32>(d);
 }
 
 cudaError_t launch_spmv(const DevLayout &d, const void *x, void *y, int nrhs,

@@ -18,8 +18,19 @@ struct DevLayout {
     int64_t m = 0, n = 0;
     void *partials = nullptr;         // slots * bs values (scratch)
     int32_t *counters = nullptr;      // gb_m arrival counters (scratch)
-    uint32_t *sched = nullptr;        // 2 scheduler counters (scratch, zeroed)
+    uint32_t *sched = nullptr;        // scheduler words (scratch, zeroed)
+    int64_t max_entries = 0;          // largest COO section of a tile
+    const void *split = nullptr;      // uint4 {block_row, first_slot, tiles, 0}
+    int64_t nsplit = 0;               // block rows split over several tiles
+    int kernel = 0;                   // 0 auto, 1 streaming (TMA), 2 direct
+    double coo_share = 1.0;
+    const uint32_t *wpart = nullptr;  // streaming: per-warp tile ranges
+    int64_t nwarps = 0;               // streaming: warps of the launch
 };
+
+// Warps of a streaming-kernel launch for this layout on the current device,
+// or 0 when the direct kernel is the one that runs.
+int64_t stream_warps(const DevLayout &d);
 
 // y = A x; x: n rows, y: m rows, row-major with leading dims for nrhs > 1.
 cudaError_t launch_spmv(const DevLayout &d, const void *x, void *y, int nrhs,

@@ -87,7 +87,7 @@ struct RowTotals {
 
 }  // namespace
 
-std::string build_layout(const HostCB &g, int f32, int tile_entries,
+std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
                          DeviceLayout &L, int *code) {
     *code = CBSPMV_ERR_UNSUPPORTED;
     if (g.n > kMaxCols)
@@ -99,8 +99,20 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries,
     c.bits = c.bs == 16 ? 4 : 5;
     c.vsz = f32 ? 4 : 8;
     c.isz = c.bs == 16 ? 1 : 2;
+    int64_t auto_emax = kTileEntries;
+    if (kernel != 2) {
+        int64_t coo_e = 0, all_e = 0;
+        for (int64_t i = 0; i < g.nnzb; ++i) {
+            if (g.nnz_blk[i] <= 0) continue;
+            all_e += g.nnz_blk[i];
+            if ((g.type_blk[i] & kTypeMask) == kCOO) coo_e += g.nnz_blk[i];
+        }
+        if (kernel == 1 || 2 * coo_e >= all_e) auto_emax = kTileEntriesStream;
+    }
     c.emax = tile_entries > 0 ? std::max(64, std::min(tile_entries, kTileEntries))
-                              : kTileEntries;
+                              : (int)auto_emax;
+    // the streaming kernel holds a whole tile's entries in registers
+    if (auto_emax == kTileEntriesStream) c.emax = std::min(c.emax, kTileEntriesStream);
     c.max_xt = c.bs == 16 ? 16 : 8;
     const int bs = c.bs, vsz = c.vsz, isz = c.isz;
     const int64_t gb_m = g.gb_m;
@@ -386,12 +398,51 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries,
             }
         });
     }
+    {
+        int64_t coo_e = 0, all_e = 0;
+        for (const TileDesc &t : L.tiles) {
+            L.max_entries = std::max<int64_t>(L.max_entries, t.coo_entries);
+            coo_e += t.coo_entries;
+        }
+        for (const BlockDesc &bd : L.blocks) all_e += meta_nnz(bd.meta);
+        L.coo_share = all_e > 0 ? (double)coo_e / (double)all_e : 1.0;
+        for (int64_t R = 0; R < gb_m; ++R)
+            if (tot[R].tiles > 1) {
+                L.split.push_back((uint32_t)R);
+                L.split.push_back((uint32_t)slot0[R]);
+                L.split.push_back((uint32_t)tot[R].tiles);
+                L.split.push_back(0u);
+            }
+    }
     // algorithmic bytes: descriptors, payload without padding, gather-list
     // reads of CSR/dense x tiles, x once, y once, split-row partials
     L.alg_bytes = T.tiles * (int64_t)sizeof(TileDesc) +
                   T.blocks * (int64_t)sizeof(BlockDesc) + T.alg + T.bcols * 4 +
                   g.n * vsz + g.m * vsz + L.slots * bs * vsz * 2;
     return "";
+}
+
+std::vector<uint32_t> partition_tiles(const DeviceLayout &L, int64_t warps) {
+    const int64_t nt = (int64_t)L.tiles.size();
+    std::vector<double> cost(nt);
+    double total = 0;
+    for (int64_t t = 0; t < nt; ++t) {
+        const TileDesc &d = L.tiles[t];
+        double c = 96.0 + d.coo_entries;  // per-tile overhead in entry units
+        const uint32_t nb = d.counts & 0xff, ncoo = (d.counts >> 8) & 0xff;
+        for (uint32_t q = ncoo; q < nb; ++q) c += 1.5 * meta_nnz(L.blocks[d.block_begin + q].meta);
+        cost[t] = c;
+        total += c;
+    }
+    std::vector<uint32_t> part(warps + 1, (uint32_t)nt);
+    part[0] = 0;
+    double acc = 0;
+    int64_t w = 1;
+    for (int64_t t = 0; t < nt && w < warps; ++t) {
+        acc += cost[t];
+        while (w < warps && acc >= total * (double)w / (double)warps) part[w++] = (uint32_t)(t + 1);
+    }
+    return part;
 }
 
 }  // namespace cb

@@ -28,7 +28,8 @@
 namespace cb {
 
 constexpr int kTileBlocks = 32;
-constexpr int kTileEntries = 512;
+constexpr int kTileEntries = 512;        // tile entry cap (the direct kernel's default)
+constexpr int kTileEntriesStream = 256;  // the streaming kernel's default
 constexpr int kColBits = 27;  // COO idx: column in bits 0..26
 constexpr int64_t kMaxCols = int64_t(1) << kColBits;
 
@@ -68,6 +69,10 @@ struct DeviceLayout {
     int64_t slots = 0;                // partial slots (tiles of split rows)
     int64_t split_rows = 0;
     int max_row_tiles = 0;
+    int64_t max_entries = 0;          // largest COO section (entries) of a tile
+    double coo_share = 1.0;           // share of stored entries in COO blocks
+    std::vector<uint32_t> split;      // per split block row: row, first slot,
+                                      // tiles, 0
     // stored values in device order
     int64_t nvals = 0;
     std::vector<uint64_t> val_off;   // byte offset of each value in payload
@@ -80,7 +85,14 @@ struct DeviceLayout {
 };
 
 // Returns "" or an error; *code receives a cbspmv_status.
-std::string build_layout(const HostCB &g, int f32, int tile_entries,
+// kernel: 0 auto, 1 streaming, 2 direct -- the default tile size follows the
+// kernel family (256 COO entries for the streaming kernel, 512 otherwise; the
+// automatic choice is streaming when most stored entries are in COO blocks).
+std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
                          DeviceLayout &L, int *code);
+
+// Cost-balanced contiguous split of the tiles over `warps` warps (the
+// streaming kernel's load balance): part[w] .. part[w+1] are warp w's tiles.
+std::vector<uint32_t> partition_tiles(const DeviceLayout &L, int64_t warps);
 
 }  // namespace cb

@@ -57,6 +57,9 @@ typedef struct cbspmv_opts {
     int value_type;       /* CBSPMV_F64 (default) or CBSPMV_F32 values      */
     int want_transpose;   /* also build the CB layout of A^T for adjoints   */
     int tile_entries;     /* device tile size in stored entries (0 = auto)  */
+    int kernel;           /* SpMV kernel: 0 auto, 1 streaming (TMA-staged
+                             tiles, for COO-dominant matrices), 2 direct
+                             (high occupancy, for CSR/dense-heavy ones)     */
 } cbspmv_opts;
 
 /* Host COO, 0-based, rows in non-decreasing order (the order the reference's

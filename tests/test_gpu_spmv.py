@@ -55,14 +55,15 @@ def _check(y, yref, absrow, f32, what):
 @pytest.mark.parametrize("bs", [16, 32])
 @pytest.mark.parametrize("f32", [False, True])
 @pytest.mark.parametrize("tile_entries", [0, 64])
-def test_spmv_matches_oracle(cuda, name, coo, bs, f32, tile_entries):
+@pytest.mark.parametrize("kernel", [1, 2])
+def test_spmv_matches_oracle(cuda, name, coo, bs, f32, tile_entries, kernel):
     import torch
     import cbspmv
     import cbdump as cd
     from cbspmv import gen
     dt = torch.float32 if f32 else torch.float64
     plan = cbspmv.Plan(coo, block_size=bs, value_type=int(f32),
-                       tile_entries=tile_entries)
+                       tile_entries=tile_entries, kernel=kernel)
     x = gen.uniform_x(coo.n, 5)
     if f32:
         x = x.astype(np.float32).astype(np.float64)  # same x for both
@@ -84,14 +85,15 @@ def test_spmv_matches_oracle(cuda, name, coo, bs, f32, tile_entries):
 
 @pytest.mark.parametrize("nrhs", [2, 5])
 @pytest.mark.parametrize("f32", [False, True])
-def test_multi_rhs(cuda, nrhs, f32):
+@pytest.mark.parametrize("kernel", [1, 2])
+def test_multi_rhs(cuda, nrhs, f32, kernel):
     import torch
     import cbspmv
     import cbdump as cd
     from cbspmv import gen
     coo = gen.power_law(4096, kmax=4096, band=256, seed=3, mean=24)
     dt = torch.float32 if f32 else torch.float64
-    plan = cbspmv.Plan(coo, value_type=int(f32), tile_entries=128)
+    plan = cbspmv.Plan(coo, value_type=int(f32), tile_entries=128, kernel=kernel)
     X = gen.uniform_x(coo.n, 9, nrhs=nrhs)  # (nrhs, n)
     if f32:
         X = X.astype(np.float32).astype(np.float64)
