@@ -69,20 +69,36 @@ class Clocks:
         self.index = index
         self.proc = None
         self.path = REPO / "gpurun_out" / f"clocks_rank{index}.csv"
+        self.err = REPO / "gpurun_out" / f"clocks_rank{index}.err"
+        self.gpu = str(index)
+        try:  # the device as nvidia-smi names it (CUDA_VISIBLE_DEVICES may remap)
+            import torch
+            uuid = str(torch.cuda.get_device_properties(index).uuid)
+            if uuid:
+                self.gpu = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+        except Exception:
+            pass
 
     def __enter__(self):
         try:
             self.path.parent.mkdir(exist_ok=True)
             self.f = open(self.path, "w")
+            self.ferr = open(self.err, "w")
             self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}",
+                ["nvidia-smi", f"--id={self.gpu}",
                  "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
                  "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
                  "clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,"
                  "clocks_event_reasons.sw_power_cap",
                  "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=self.f, stderr=subprocess.DEVNULL)
+                stdout=self.f, stderr=self.ferr)
+            # start timing only once sampling runs (nvidia-smi needs ~1 s)
+            t0 = time.time()
+            while time.time() - t0 < 10 and self.proc.poll() is None:
+                if self.path.stat().st_size > 0:
+                    break
+                time.sleep(0.05)
         except Exception:
             self.proc = None
         return self
@@ -95,6 +111,7 @@ class Clocks:
             except Exception:
                 self.proc.kill()
             self.f.close()
+            self.ferr.close()
 
     def summary(self):
         if not self.path.exists():
@@ -210,7 +227,7 @@ def reference_arm(args, budget_s: float = 150.0):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--steps", type=int, default=10000)
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", default="cbspmv", choices=["cbspmv", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=300)
@@ -297,7 +314,8 @@ def main():
     achieved = alg / (ms * 1e-3) / 1e9
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-            "traffic": _ncu_traffic(), "kernel": "cb_spmv tile kernel"}
+            "traffic": _ncu_traffic(),
+            "kernel": "cb_spmv_stream_kernel (the one launch of each SpMV)"}
 
     line = None
     if rank == 0:

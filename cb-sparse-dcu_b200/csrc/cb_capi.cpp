@@ -19,7 +19,6 @@
 namespace {
 
 thread_local std::string g_error;
-std::atomic<int64_t> g_launches{0};
 
 cbspmv_status fail(cbspmv_status code, const std::string &msg) {
     g_error = msg;
@@ -55,7 +54,6 @@ struct DevSide {
     int32_t *block_cols = nullptr;
     void *partials = nullptr;
     int32_t *counters = nullptr;
-    uint32_t *split = nullptr;
     uint32_t *wpart = nullptr;
     int partial_nrhs = 0;
     int64_t *vsrc_ptr = nullptr;
@@ -65,13 +63,13 @@ struct DevSide {
 
     void release() {
         void *ps[] = {tiles, blocks, payload, block_cols, partials, counters,
-                      split, wpart, vsrc_ptr, vsrc, val_off, val_row, val_col};
+                      wpart, vsrc_ptr, vsrc, val_off, val_row, val_col};
         for (void *p : ps)
             if (p) cudaFree(p);
         tiles = blocks = partials = nullptr;
         payload = nullptr;
         block_cols = counters = vsrc = val_row = val_col = nullptr;
-        split = wpart = nullptr;
+        wpart = nullptr;
         vsrc_ptr = nullptr;
         val_off = nullptr;
         partial_nrhs = 0;
@@ -132,12 +130,9 @@ cbspmv_status upload_side(DevSide &s, cudaStream_t st) {
     s.d.gather = L.gather;
     s.d.m = L.m;
     s.d.n = L.n;
-    CB_CUDA(upload_vec(L.split, &s.split, st), "upload split rows");
     s.d.sched = reinterpret_cast<uint32_t *>(s.counters);
     s.d.counters = s.counters + 4;
     s.d.max_entries = L.max_entries;
-    s.d.split = s.split;
-    s.d.nsplit = (int64_t)L.split.size() / 4;
     s.d.coo_share = L.coo_share;
     return CBSPMV_OK;
 }
@@ -183,7 +178,6 @@ cbspmv_status run_side(cbspmv_plan *p, DevSide &s, const void *x, void *y,
     if (dev != p->device)
         return fail(CBSPMV_ERR_STATE, "plan was uploaded to another device");
     CB_CUDA(cb::launch_spmv(s.d, x, y, nrhs, ldx, ldy, st), "spmv launch");
-    if (s.d.ntiles > 0) g_launches++;
     return CBSPMV_OK;
 }
 
@@ -336,7 +330,6 @@ cbspmv_status cbspmv_spmv_noalloc(cbspmv_plan *p, const void *x, void *y, int nr
     CB_CUDA(cb::launch_spmv_fixed_scratch(s.d, s.lay.gb_m, s.lay.slots, x, y, nrhs, ldx,
                                           ldy, (cudaStream_t)stream),
             "spmv_noalloc launch");
-    if (s.d.ntiles > 0) g_launches++;
     return CBSPMV_OK;
 }
 
@@ -430,7 +423,6 @@ cbspmv_status cbspmv_grad_vals(cbspmv_plan *p, const void *g, const void *x,
     CB_CUDA(cb::launch_grad_vals(s.lay.f32, s.lay.nvals, s.val_row, s.val_col, g,
                                  ldg, x, ldx, nrhs, gvals, (cudaStream_t)stream),
             "grad_vals launch");
-    if (s.lay.nvals) g_launches++;
     return CBSPMV_OK;
 }
 
@@ -447,7 +439,6 @@ cbspmv_status cbspmv_set_values(cbspmv_plan *p, const void *input_values,
         CB_CUDA(cb::launch_set_values(s->lay.f32, s->lay.nvals, s->vsrc_ptr, s->vsrc,
                                       s->val_off, input_values, s->payload, st),
                 "set_values launch");
-        if (s->lay.nvals) g_launches++;
     }
     return CBSPMV_OK;
 }
@@ -587,6 +578,6 @@ size_t cbspmv_last_error(char *buf, size_t len) {
     return g_error.size();
 }
 
-int64_t cbspmv_launch_count(void) { return g_launches.load(); }
+int64_t cbspmv_launch_count(void) { return cb::kernel_launches(); }
 
 }  // extern "C"

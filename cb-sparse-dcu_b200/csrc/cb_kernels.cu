@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstdlib>
 #include <mutex>
@@ -33,6 +34,10 @@
 
 namespace cb {
 namespace {
+
+// kernels this library has launched (all devices, all plans)
+std::atomic<int64_t> g_kernel_launches{0};
+inline void note_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWarps = 8;
@@ -281,12 +286,14 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
 //     on one counter cannot keep up with ~10^5 tiles per launch), and loads
 //     tile descriptors two tiles ahead of use;
 //   * the x gathers of a chunk are the only global loads on the entry path;
-//   * block rows split over several tiles leave partial sums in their slots;
-//     cb_combine_kernel adds them in tile order afterwards (no fences, no
-//     arrival counters).
+//   * consecutive tiles of one block row in a warp's range keep adding into
+//     the same accumulators; only a block row that crosses a warp boundary
+//     leaves one partial sum per warp, and the last of those warps to arrive
+//     on the row's counter adds them in tile order (no tile waits on another).
 // Every mbarrier wait is bounded (kWaitLimit polls); on give-up the error
 // word sched[2] is set and the warp stops, after waiting (bounded) for its
-// own copies in flight.  sched[0..1] are not used by this kernel.
+// own copies in flight.  sched[0..1] are not used by this kernel; the
+// per-block-row arrival counters return to zero by the end of every launch.
 // ============================================================================
 constexpr uint32_t kWaitLimit = 1u << 22;
 constexpr int kStreamWarps = 4;  // warps per CTA
@@ -390,12 +397,11 @@ __device__ __forceinline__ void gather_tile(const unsigned char *buf, int E,
 // Adds a gathered tile into the lane-private accumulators, handles its CSR and
 // DENSE blocks, reduces and stores (or leaves a split row's partials).
 template <typename T, int BS>
-__device__ __forceinline__ void finish_tile(const uint4 ta, const uint4 tb, const Staged<T> &g,
-                                            T *acc, T *xts, const uint4 *__restrict__ blocks,
-                                            const uint8_t *__restrict__ payload,
-                                            const int32_t *__restrict__ block_cols, int gather,
-                                            const T *__restrict__ x, T *__restrict__ y,
-                                            int64_t m, T *__restrict__ partials, int lane) {
+__device__ __forceinline__ void add_tile(const uint4 ta, const uint4 tb, const Staged<T> &g,
+                                         T *acc, T *xts, const uint4 *__restrict__ blocks,
+                                         const uint8_t *__restrict__ payload,
+                                         const int32_t *__restrict__ block_cols, int gather,
+                                         const T *__restrict__ x, int lane) {
     T *myacc = &acc[lane * (BS + 1)];
     const int E = (int)tb.x;
 #pragma unroll
@@ -458,17 +464,59 @@ __device__ __forceinline__ void finish_tile(const uint4 ta, const uint4 tb, cons
             }
         }
     }
+}
+
+// Ends a run of consecutive tiles of one block row in this warp (the last
+// tile `tg`, global index; `runlen` tiles): reduces the accumulators and
+// stores the rows.  A run that holds the whole block row stores y.  Otherwise
+// the row crosses a warp boundary: the run's sum goes to the slot of its first
+// tile, and the last run to arrive on the row's counter adds the row's run
+// sums in tile order and stores y.  Runs start at the row's first tile and at
+// every warp boundary inside the row (wpart), so the order does not depend on
+// which warp arrives last.
+template <typename T, int BS>
+__device__ __forceinline__ void store_run(const uint4 ta, const uint4 tb, int64_t tg,
+                                          int64_t runlen, T *acc, T *__restrict__ y,
+                                          int64_t m, T *__restrict__ partials,
+                                          int32_t *__restrict__ counters,
+                                          const uint32_t *__restrict__ wpart, int64_t gw,
+                                          int lane) {
     __syncwarp();
     const T sum = reduce_rows<T, BS>(acc, lane);
     __syncwarp();
-    if (lane < BS) {
-        const int64_t grow = (int64_t)ta.y * BS + lane;
-        if (tb.y == 0xffffffffu) {
-            if (grow < m) y[grow] = sum;
-        } else {
-            partials[(size_t)tb.y * BS + lane] = sum;
+    const int64_t grow = (int64_t)ta.y * BS + lane;
+    if (tb.y == 0xffffffffu || runlen == (int64_t)tb.w) {
+        if (lane < BS && grow < m) y[grow] = sum;
+        return;
+    }
+    const int64_t first = tg - (int64_t)(tb.y - tb.z);  // the row's first tile
+    const int64_t run0 = tg - runlen + 1;
+    if (lane < BS) partials[(size_t)(tb.z + (run0 - first)) * BS + lane] = sum;
+    __threadfence();
+    __syncwarp();
+    int last = 0;
+    if (lane == 0) {
+        const int old = atomicAdd(&counters[ta.y], (int)runlen);
+        last = old + (int)runlen == (int)tb.w;
+    }
+    last = __shfl_sync(kFull, last, 0);
+    if (!last) return;
+    __threadfence();
+    // warp k holds tiles [wpart[k], wpart[k+1]); find the warp holding `first`
+    int64_t k = gw;
+    while (k > 0 && (int64_t)__ldg(&wpart[k]) > first) --k;
+    const int64_t end = first + (int64_t)tb.w;
+    T tot = T(0);
+    if (lane < BS) tot = __ldcg(&partials[(size_t)tb.z * BS + lane]);
+    int64_t prev = first;
+    for (int64_t b = __ldg(&wpart[k + 1]); b < end; b = __ldg(&wpart[++k + 1])) {
+        if (b > prev) {
+            if (lane < BS) tot += __ldcg(&partials[(size_t)(tb.z + (b - first)) * BS + lane]);
+            prev = b;
         }
     }
+    if (lane < BS && grow < m) y[grow] = tot;
+    if (lane == 0) atomicExch(&counters[ta.y], 0);
 }
 
 // Warp w processes its tiles i = 0, 1, ... of wpart[w] .. wpart[w+1] in a
@@ -483,7 +531,8 @@ __global__ void __launch_bounds__(kStreamWarps * 32)
                           const uint8_t *__restrict__ payload,
                           const int32_t *__restrict__ block_cols, int gather,
                           const T *__restrict__ x, T *__restrict__ y, int64_t m,
-                          T *__restrict__ partials, uint32_t *__restrict__ sched,
+                          T *__restrict__ partials, int32_t *__restrict__ counters,
+                          uint32_t *__restrict__ sched,
                           const uint32_t *__restrict__ wpart, uint32_t cap) {
     using SL = StreamLayout<T, BS>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -557,6 +606,7 @@ __global__ void __launch_bounds__(kStreamWarps * 32)
         stage(a2, b2, 0);
         inflight |= 1u;
     }
+    int64_t runlen = 0;  // tiles of the current block row added so far
     for (int64_t i = 0; ok && i < nt; ++i) {
         const int nb = (int)((i + 1) & 1);  // buffer of tile i+1
         desc(i + 4, a4, b4);
@@ -569,8 +619,13 @@ __global__ void __launch_bounds__(kStreamWarps * 32)
                 inflight |= 1u << nb;
             }
         }
-        finish_tile<T, BS>(a0, b0, g0, acc, xts, blocks, payload, block_cols, gather, x, y, m,
-                           partials, lane);
+        add_tile<T, BS>(a0, b0, g0, acc, xts, blocks, payload, block_cols, gather, x, lane);
+        ++runlen;
+        if (i + 1 >= nt || a1.y != a0.y) {  // the row's run in this warp ends here
+            store_run<T, BS>(a0, b0, t0 + i, runlen, acc, y, m, partials, counters, wpart, gw,
+                             lane);
+            runlen = 0;
+        }
         g0 = g1;
         a0 = a1; b0 = b1;
         a1 = a2; b1 = b2;
@@ -581,27 +636,6 @@ __global__ void __launch_bounds__(kStreamWarps * 32)
     for (int q = 0; q < 2; ++q)
         if ((inflight >> q) & 1u) mbar_wait(&mbar[q], (phase >> q) & 1u, &sched[2]);
     __syncwarp();
-}
-
-// One warp per split block row: its y rows = the sum of the row's tile
-// partials, in tile order (split = {block_row, first_slot, tiles, 0}).
-template <typename T, int BS>
-__global__ void __launch_bounds__(128)
-    cb_combine_kernel(const uint4 *__restrict__ split, int64_t nsplit,
-                      const T *__restrict__ partials, T *__restrict__ y, int64_t m,
-                      int nrhs, int64_t ldy) {
-    const int lane = threadIdx.x & 31;
-    const int64_t w = (int64_t)blockIdx.x * 4 + (threadIdx.x >> 5);
-    if (w >= nsplit || lane >= BS) return;
-    const uint4 d = __ldg(&split[w]);
-    const int64_t grow = (int64_t)d.x * BS + lane;
-    if (grow >= m) return;
-    for (int j = 0; j < nrhs; ++j) {
-        T tot = T(0);
-        for (uint32_t t = 0; t < d.z; ++t)
-            tot += partials[((size_t)(d.y + t) * nrhs + j) * BS + lane];
-        y[grow * ldy + j] = tot;
-    }
 }
 
 template <typename T>
@@ -659,6 +693,7 @@ cudaError_t launch_chunk(const DevLayout &d, const void *x, void *y, int nrhs,
         static_cast<const uint4 *>(d.blocks), d.payload, d.block_cols, d.gather,
         static_cast<const T *>(x), static_cast<T *>(y), d.m, nrhs, ldx, ldy,
         static_cast<T *>(d.partials), d.counters, d.sched);
+    note_launch();
     return cudaGetLastError();
 }
 
@@ -723,13 +758,8 @@ cudaError_t launch_stream(const DevLayout &d, const void *x, void *y, cudaStream
             static_cast<const uint4 *>(d.tiles), d.ntiles,
             static_cast<const uint4 *>(d.blocks), d.payload, d.block_cols, d.gather,
             static_cast<const T *>(x), static_cast<T *>(y), d.m,
-            static_cast<T *>(d.partials), d.sched, d.wpart, c.cap);
-    e = cudaGetLastError();
-    if (e != cudaSuccess || d.nsplit == 0) return e;
-    const unsigned cgrid = (unsigned)((d.nsplit + 3) / 4);
-    cb_combine_kernel<T, BS><<<cgrid, 128, 0, stream>>>(
-        static_cast<const uint4 *>(d.split), d.nsplit,
-        static_cast<const T *>(d.partials), static_cast<T *>(y), d.m, 1, 1);
+            static_cast<T *>(d.partials), d.counters, d.sched, d.wpart, c.cap);
+    note_launch();
     return cudaGetLastError();
 }
 
@@ -756,6 +786,8 @@ cudaError_t launch_tiles(const DevLayout &d, const void *x, void *y, int nrhs,
 }
 
 }  // namespace
+
+int64_t kernel_launches() { return g_kernel_launches.load(); }
 
 size_t spmv_smem_bytes(int bs, int f32) {
     if (bs == 16)
@@ -851,6 +883,7 @@ cudaError_t launch_set_values(int f32, int64_t nvals, const int64_t *vsrc_ptr,
     else
         cb_set_values_kernel<double><<<grid, 256, 0, stream>>>(
             nvals, vsrc_ptr, vsrc, val_off, static_cast<const double *>(in), payload);
+    note_launch();
     return cudaGetLastError();
 }
 
@@ -868,6 +901,7 @@ cudaError_t launch_grad_vals(int f32, int64_t nvals, const int32_t *vrow,
         cb_grad_vals_kernel<double><<<grid, 256, 0, stream>>>(
             nvals, vrow, vcol, static_cast<const double *>(g), ldg,
             static_cast<const double *>(x), ldx, nrhs, static_cast<double *>(gvals));
+    note_launch();
     return cudaGetLastError();
 }
 

@@ -20,8 +20,6 @@ struct DevLayout {
     int32_t *counters = nullptr;      // gb_m arrival counters (scratch)
     uint32_t *sched = nullptr;        // scheduler words (scratch, zeroed)
     int64_t max_entries = 0;          // largest COO section of a tile
-    const void *split = nullptr;      // uint4 {block_row, first_slot, tiles, 0}
-    int64_t nsplit = 0;               // block rows split over several tiles
     int kernel = 0;                   // 0 auto, 1 streaming (TMA), 2 direct
     double coo_share = 1.0;
     const uint32_t *wpart = nullptr;  // streaming: per-warp tile ranges
@@ -59,6 +57,9 @@ cudaError_t launch_grad_vals(int f32, int64_t nvals, const int32_t *vrow,
                              const int32_t *vcol, const void *g, int64_t ldg,
                              const void *x, int64_t ldx, int nrhs, void *gvals,
                              cudaStream_t stream);
+
+// Kernel launches made by this library so far (every launcher above).
+int64_t kernel_launches();
 
 // Dynamic shared memory of the SpMV kernel per CTA.
 size_t spmv_smem_bytes(int bs, int f32);

@@ -406,19 +406,13 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
         }
         for (const BlockDesc &bd : L.blocks) all_e += meta_nnz(bd.meta);
         L.coo_share = all_e > 0 ? (double)coo_e / (double)all_e : 1.0;
-        for (int64_t R = 0; R < gb_m; ++R)
-            if (tot[R].tiles > 1) {
-                L.split.push_back((uint32_t)R);
-                L.split.push_back((uint32_t)slot0[R]);
-                L.split.push_back((uint32_t)tot[R].tiles);
-                L.split.push_back(0u);
-            }
     }
     // algorithmic bytes: descriptors, payload without padding, gather-list
-    // reads of CSR/dense x tiles, x once, y once, split-row partials
+    // reads of CSR/dense x tiles, x once, y once (split-row partial sums are
+    // scratch traffic, not counted)
     L.alg_bytes = T.tiles * (int64_t)sizeof(TileDesc) +
                   T.blocks * (int64_t)sizeof(BlockDesc) + T.alg + T.bcols * 4 +
-                  g.n * vsz + g.m * vsz + L.slots * bs * vsz * 2;
+                  g.n * vsz + g.m * vsz;
     return "";
 }
 

@@ -71,8 +71,6 @@ struct DeviceLayout {
     int max_row_tiles = 0;
     int64_t max_entries = 0;          // largest COO section (entries) of a tile
     double coo_share = 1.0;           // share of stored entries in COO blocks
-    std::vector<uint32_t> split;      // per split block row: row, first slot,
-                                      // tiles, 0
     // stored values in device order
     int64_t nvals = 0;
     std::vector<uint64_t> val_off;   // byte offset of each value in payload
