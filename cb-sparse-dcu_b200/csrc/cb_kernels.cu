@@ -1,26 +1,24 @@
-// sm_100a kernels of the CB-SpMV: the tile kernel (the reference's `comp` and
-// `gather` kernels, cb-spmv-dcu.hpp:159-1084, folded into one: the layout
-// resolves COO columns at build time and stages gathered x columns per
-// CSR/DENSE block), plus value refresh and value-gradient kernels.
-//
-// Mapping (32-lane warps, one warp per tile, 8 warps per CTA):
-//   phase 1  products of all COO entries of the tile, lane-strided with
-//            independent loads (idx, value, x[col]) -> shared memory; x tiles
-//            of the CSR/DENSE blocks (bs values each, through the gather list
-//            when the matrix was gathered) -> shared memory.
-//   phase 2  per COO block: a segmented scan over its row runs (entries are
-//            sorted by row inside a block, coo2block.h:219-227), two blocks of
-//            <= 16 entries per warp, 32-entry passes otherwise; the number of
-//            scan steps is the block's log2(longest run), stored in its
-//            descriptor.  CSR: 32/bs lanes per row (the reference's
-//            LANES_PER_ROW, macros.h:84, re-derived for 32 lanes).  DENSE:
-//            2 lanes per row for bs=16, 1 for bs=32.  Run tails add into two
-//            per-warp row accumulators (one per half-warp), never colliding.
-//   phase 3  the tile's bs row sums go to y, or for a block row split over
-//            several tiles to a partial slot; the last tile to arrive on the
-//            row's counter adds all partials in tile order and stores y.  No
-//            tile waits on another (the reference spins on a row epoch,
-//            cb-spmv-dcu.hpp:238-282).
+// sm_100a kernels of the CB-SpMV.  The reference's `comp` and `gather` kernels
+// (cb-spmv-dcu.hpp:159-1084) become two tile kernels over this library's own
+// device layout, in which COO columns are resolved through the gather list at
+// build time and CSR/DENSE blocks stage their bs gathered x values per block:
+//   * cb_spmv_stream_kernel (COO-dominant matrices, one right-hand side):
+//     per-warp bulk-async (TMA) double-buffered tiles, host-balanced
+//     contiguous tile ranges, x gathers of the next tile in flight while the
+//     current one is added up;
+//   * cb_spmv_tile_kernel ("direct"; CSR/DENSE-heavy matrices and several
+//     right-hand sides): one warp per tile, tiles taken from a global counter.
+// Both add each COO entry's val * x[col] into its row (the reference's
+// per-entry accumulate_output, cb-spmv-dcu.hpp:423-426) in a lane-private
+// shared accumulator -- no atomics, a fixed order, bitwise reproducible -- and
+// reduce the 32 copies of a row once per tile (direct) or once per run of a
+// block row's tiles (streaming).  CSR blocks use 32/bs lanes per row (the
+// reference's LANES_PER_ROW, macros.h:84, re-derived for 32 lanes), DENSE
+// blocks 2 lanes per row (bs = 16) or 1 (bs = 32).  A block row split over
+// several tiles (or warps) leaves partial sums; the last tile (or warp) to
+// arrive on the row's counter adds them in a fixed order and stores y.  No
+// tile waits on another (the reference spins on a row epoch,
+// cb-spmv-dcu.hpp:238-282).  Also: value refresh and value-gradient kernels.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -46,13 +44,15 @@ constexpr uint32_t kColMask = (1u << 27) - 1;
 __host__ __device__ constexpr int max_xt(int bs) { return bs == 16 ? 16 : 8; }
 __host__ __device__ constexpr uint32_t a16(uint32_t x) { return (x + 15u) & ~15u; }
 
-// Per-warp shared memory.  acc holds one private row accumulator per lane
-// (lane l owns acc[l * (BS + 1) + r]; the +1 pad spreads a column over the
-// banks), so entries accumulate without atomics and in a fixed order.
+// Per-warp shared memory.  acc holds one private accumulator per lane and row:
+// lane l's copy of row r is acc[r * 32 + l].  Entries accumulate without
+// atomics and in a fixed order; a lane only ever touches its own column, so the
+// updates of a warp hit 32 distinct banks (fp32) or 16 distinct bank pairs per
+// half-warp (fp64) whatever the rows.
 template <typename T, int BS>
 struct WarpSmem {
     T xt[max_xt(BS) * BS];      // x tiles of the tile's CSR/DENSE blocks
-    T acc[32 * (BS + 1)];
+    T acc[BS * 32];
 };
 
 template <typename T>
@@ -60,25 +60,27 @@ __device__ __forceinline__ T ldg(const T *p) {
     return __ldg(p);
 }
 
-// Sums the 32 lane-private accumulators of row r = lane % BS, clearing them
-// for the next tile.  Lanes >= BS (BS = 16) sum the upper 16 lanes' copies and
-// hand their half over by shuffle.  Result valid in lanes < BS.
+// Sums the 32 lane-private copies of row r = lane % BS, clearing them for the
+// next tile.  BS = 16: lanes 0-15 sum lanes 0-15's copies, lanes 16-31 the
+// upper 16 and hand their half over by shuffle.  Lane r reads the copies in
+// the rotated order l = r, r+1, ..., so the 16 (or 32) lanes of one step read
+// distinct banks.  Result valid in lanes < BS.
 template <typename T, int BS>
 __device__ __forceinline__ T reduce_rows(T *acc, int lane) {
     T s = T(0);
     if (BS == 16) {
-        const int r = lane & 15, l0 = (lane >> 4) * 16;
+        const int r = lane & 15, l0 = lane & 16;
 #pragma unroll
-        for (int l = 0; l < 16; ++l) {
-            T *p = &acc[(l0 + l) * (BS + 1) + r];
+        for (int q = 0; q < 16; ++q) {
+            T *p = &acc[r * 32 + l0 + ((q + r) & 15)];
             s += *p;
             *p = T(0);
         }
         s += __shfl_down_sync(kFull, s, 16);
     } else {
 #pragma unroll 8
-        for (int l = 0; l < 32; ++l) {
-            T *p = &acc[l * (BS + 1) + lane];
+        for (int q = 0; q < 32; ++q) {
+            T *p = &acc[lane * 32 + ((q + lane) & 31)];
             s += *p;
             *p = T(0);
         }
@@ -106,8 +108,8 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     WarpSmem<T, BS> &S = reinterpret_cast<WarpSmem<T, BS> *>(smem_raw)[wib];
-    T *myacc = &S.acc[lane * (BS + 1)];
-    for (int t = lane; t < 32 * (BS + 1); t += 32) S.acc[t] = T(0);
+    T *myacc = &S.acc[lane];  // row r at myacc[r * 32]
+    for (int t = lane; t < 32 * BS; t += 32) S.acc[t] = T(0);
     __syncwarp();
 
     auto grab = [&]() -> int64_t {
@@ -186,7 +188,7 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
 #pragma unroll
                 for (int u = 0; u < kChunk; ++u) {
                     const int e = c0 + u * 32 + lane;
-                    if (e < E) myacc[w[u] >> 27] += v[u] * xv[u];
+                    if (e < E) myacc[(w[u] >> 27) * 32] += v[u] * xv[u];
                 }
             }
 
@@ -209,7 +211,7 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
                     T sum = T(0);
                     for (int q = kb + sub; q < ke; q += L)
                         sum += __ldg(&vv[q]) * xt[__ldg(&ci[q])];
-                    myacc[row] += sum;
+                    myacc[row * 32] += sum;
                 } else {
                     const T *vv = reinterpret_cast<const T *>(pb);
                     T sum = T(0);
@@ -218,12 +220,12 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
 #pragma unroll
                         for (int c = 0; c < 8; ++c)
                             sum += __ldg(&vv[row * 16 + c0 + c]) * xt[c0 + c];
-                        myacc[row] += sum;
+                        myacc[row * 32] += sum;
                     } else {
 #pragma unroll 8
                         for (int c = 0; c < BS; ++c)
                             sum += __ldg(&vv[lane * BS + c]) * xt[c];
-                        myacc[lane] += sum;
+                        myacc[lane * 32] += sum;
                     }
                 }
             }
@@ -357,7 +359,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32
 // tile's COO section (`cap` bytes: indices, then values).
 template <typename T, int BS>
 struct StreamLayout {
-    static constexpr uint32_t acc_bytes = 32 * (BS + 1) * sizeof(T);
+    static constexpr uint32_t acc_bytes = BS * 32 * sizeof(T);
     static constexpr uint32_t xt_bytes = max_xt(BS) * BS * sizeof(T);
     static constexpr uint32_t head = a16(acc_bytes + xt_bytes + 16);
     __host__ __device__ static uint32_t bytes(uint32_t cap) { return head + 2 * cap; }
@@ -402,11 +404,11 @@ __device__ __forceinline__ void add_tile(const uint4 ta, const uint4 tb, const S
                                          const uint8_t *__restrict__ payload,
                                          const int32_t *__restrict__ block_cols, int gather,
                                          const T *__restrict__ x, int lane) {
-    T *myacc = &acc[lane * (BS + 1)];
+    T *myacc = &acc[lane];  // row r at myacc[r * 32]
     const int E = (int)tb.x;
 #pragma unroll
     for (int u = 0; u < kStreamChunk; ++u)
-        if (u * 32 + lane < E) myacc[g.w[u] >> 27] += g.v[u] * g.x[u];
+        if (u * 32 + lane < E) myacc[(g.w[u] >> 27) * 32] += g.v[u] * g.x[u];
     const int nb = ta.z & 0xff;
     const int ncoo = (ta.z >> 8) & 0xff;
     const int nxtb = (ta.z >> 16) & 0xff;
@@ -447,7 +449,7 @@ __device__ __forceinline__ void add_tile(const uint4 ta, const uint4 tb, const S
                 const int kb = __ldg(&rp[row]), ke = __ldg(&rp[row + 1]);
                 T sum = T(0);
                 for (int q = kb + sub; q < ke; q += L) sum += __ldg(&vv[q]) * xt[__ldg(&ci[q])];
-                myacc[row] += sum;
+                myacc[row * 32] += sum;
             } else {
                 const T *vv = reinterpret_cast<const T *>(pb);
                 T sum = T(0);
@@ -455,11 +457,11 @@ __device__ __forceinline__ void add_tile(const uint4 ta, const uint4 tb, const S
                     const int row = lane >> 1, cc = (lane & 1) * 8;
 #pragma unroll
                     for (int c = 0; c < 8; ++c) sum += __ldg(&vv[row * 16 + cc + c]) * xt[cc + c];
-                    myacc[row] += sum;
+                    myacc[row * 32] += sum;
                 } else {
 #pragma unroll 8
                     for (int c = 0; c < BS; ++c) sum += __ldg(&vv[lane * BS + c]) * xt[c];
-                    myacc[lane] += sum;
+                    myacc[lane * 32] += sum;
                 }
             }
         }
@@ -546,7 +548,7 @@ __global__ void __launch_bounds__(kStreamWarps * 32)
     constexpr uint32_t vsz = sizeof(T);
     const uint64_t pol = policy_evict_first();
 
-    for (int t = lane; t < 32 * (BS + 1); t += 32) acc[t] = T(0);
+    for (int t = lane; t < 32 * BS; t += 32) acc[t] = T(0);
     if (lane == 0) {
         mbar_init(&mbar[0], 1);
         mbar_init(&mbar[1], 1);
