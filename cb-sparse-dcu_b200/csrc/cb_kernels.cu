@@ -88,6 +88,39 @@ __device__ __forceinline__ T reduce_rows(T *acc, int lane) {
     return s;
 }
 
+// Adds K COO entries held by this lane -- slot u is the tile entry at
+// position pos0 + 32u, valid while below E -- into the lane's accumulators
+// (row r at myacc[r * 32]).  A tile's COO entries are stored sorted by row, so
+// the rows of a lane's slots never decrease: equal-row slots are summed in
+// registers, each run of them adds to the accumulator once, and since
+// different runs are different rows every load can be issued before any store.
+template <typename T, int K>
+__device__ __forceinline__ void add_entries(T *myacc, const uint32_t *w, const T *v,
+                                            const T *xv, int pos0, int E) {
+    uint32_t r[K];
+    T s[K];
+#pragma unroll
+    for (int u = 0; u < K; ++u) r[u] = w[u] >> 27;
+#pragma unroll
+    for (int u = 0; u < K; ++u)
+        s[u] = fma(v[u], xv[u], (u > 0 && r[u] == r[u > 0 ? u - 1 : 0]) ? s[u > 0 ? u - 1 : 0]
+                                                                          : T(0));
+    bool f[K];
+#pragma unroll
+    for (int u = 0; u < K; ++u) {
+        const bool valid = pos0 + 32 * u < E;
+        const bool more = u + 1 < K && pos0 + 32 * (u + 1) < E &&
+                          r[u + 1 < K ? u + 1 : u] == r[u];
+        f[u] = valid && !more;
+    }
+    T a[K];
+#pragma unroll
+    for (int u = 0; u < K; ++u) a[u] = f[u] ? myacc[r[u] * 32] : T(0);
+#pragma unroll
+    for (int u = 0; u < K; ++u)
+        if (f[u]) myacc[r[u] * 32] = a[u] + s[u];
+}
+
 // Persistent warps fetch tiles from a global counter (sched[0]); the warp
 // whose exit completes sched[1] == number of warps resets both for the next
 // launch, so no launch waits on another and no host reset is needed.
@@ -131,13 +164,12 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
             na = __ldg(&tiles[2 * next]);
             nb4 = __ldg(&tiles[2 * next + 1]);
         }
-        const int nb = ta.z & 0xff;
         const int ncoo = (ta.z >> 8) & 0xff;
         const int nxt = (ta.z >> 16) & 0xff;
         const int E = (int)tb.x;
         const uint8_t *base = payload + (size_t)ta.w * 16;
-        uint4 bd = make_uint4(0, 0, 0, 0);
-        if (lane < nb) bd = __ldg(&blocks[ta.x + lane]);
+        uint4 bd = make_uint4(0, 0, 0, 0);  // lane j: CSR/DENSE block j of the tile
+        if (lane < nxt) bd = __ldg(&blocks[ta.x + ncoo + lane]);
         const uint32_t *cidx = reinterpret_cast<const uint32_t *>(base);
         const T *cval = reinterpret_cast<const T *>(base + a16(4u * E));
         const int64_t row0 = (int64_t)ta.y * BS;
@@ -148,8 +180,8 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
             for (int t0 = 0; t0 < nxt * BS; t0 += 32) {
                 const int t = t0 + lane;
                 const int jb = min(t / BS, nxt - 1);
-                const uint32_t xb = __shfl_sync(kFull, bd.z, ncoo + jb);
-                const uint32_t mb = __shfl_sync(kFull, bd.y, ncoo + jb);
+                const uint32_t xb = __shfl_sync(kFull, bd.z, jb);
+                const uint32_t mb = __shfl_sync(kFull, bd.y, jb);
                 const int c = t % BS;
                 const int valid = (mb >> 14) & 63;
                 if (t < nxt * BS) {
@@ -194,8 +226,8 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
 
             // CSR and DENSE blocks
             for (int jb = 0; jb < nxt; ++jb) {
-                const uint32_t off = __shfl_sync(kFull, bd.x, ncoo + jb);
-                const uint32_t mb = __shfl_sync(kFull, bd.y, ncoo + jb);
+                const uint32_t off = __shfl_sync(kFull, bd.x, jb);
+                const uint32_t mb = __shfl_sync(kFull, bd.y, jb);
                 const int k = (mb >> 3) & 2047;
                 const uint8_t *pb = base + off;
                 const T *xt = &S.xt[jb * BS];
@@ -406,19 +438,17 @@ __device__ __forceinline__ void add_tile(const uint4 ta, const uint4 tb, const S
                                          const T *__restrict__ x, int lane) {
     T *myacc = &acc[lane];  // row r at myacc[r * 32]
     const int E = (int)tb.x;
-#pragma unroll
-    for (int u = 0; u < kStreamChunk; ++u)
-        if (u * 32 + lane < E) myacc[(g.w[u] >> 27) * 32] += g.v[u] * g.x[u];
-    const int nb = ta.z & 0xff;
+    add_entries<T, kStreamChunk>(myacc, g.w, g.v, g.x, lane, E);
     const int ncoo = (ta.z >> 8) & 0xff;
     const int nxtb = (ta.z >> 16) & 0xff;
     if (nxtb) {  // CSR and DENSE blocks, read from global memory
-        const uint4 bd = lane < nb ? __ldg(&blocks[ta.x + lane]) : make_uint4(0, 0, 0, 0);
+        const uint4 bd =
+            lane < nxtb ? __ldg(&blocks[ta.x + ncoo + lane]) : make_uint4(0, 0, 0, 0);
         for (int t0 = 0; t0 < nxtb * BS; t0 += 32) {
             const int t = t0 + lane;
             const int jb = min(t / BS, nxtb - 1);
-            const uint32_t xb = __shfl_sync(kFull, bd.z, ncoo + jb);
-            const uint32_t mb = __shfl_sync(kFull, bd.y, ncoo + jb);
+            const uint32_t xb = __shfl_sync(kFull, bd.z, jb);
+            const uint32_t mb = __shfl_sync(kFull, bd.y, jb);
             const int c = t % BS;
             if (t < nxtb * BS) {
                 T xv = T(0);
@@ -433,8 +463,8 @@ __device__ __forceinline__ void add_tile(const uint4 ta, const uint4 tb, const S
         __syncwarp();
         const uint8_t *gbase = payload + (size_t)ta.w * 16;
         for (int jb = 0; jb < nxtb; ++jb) {
-            const uint32_t off = __shfl_sync(kFull, bd.x, ncoo + jb);
-            const uint32_t mb = __shfl_sync(kFull, bd.y, ncoo + jb);
+            const uint32_t off = __shfl_sync(kFull, bd.x, jb);
+            const uint32_t mb = __shfl_sync(kFull, bd.y, jb);
             const int k = (mb >> 3) & 2047;
             const uint8_t *pb = gbase + off;
             const T *xt = &xts[jb * BS];

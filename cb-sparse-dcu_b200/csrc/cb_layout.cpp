@@ -83,6 +83,7 @@ void split_row(const Ctx &c, int64_t b0, int64_t b1, Fn fn) {
 
 struct RowTotals {
     int64_t tiles = 0, blocks = 0, bytes = 0, vals = 0, alg = 0, bcols = 0;
+    int64_t xblocks = 0;  // CSR and DENSE blocks (the kernels read their descriptors)
 };
 
 }  // namespace
@@ -147,6 +148,7 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
                 if (c.is_coo(i)) {
                     E += c.k(i);
                 } else {
+                    t.xblocks++;
                     t.bytes += c.payload_bytes(i);
                     if (g.gather_flag) t.bcols += c.valid_cols(i);
                 }
@@ -163,6 +165,7 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
         pre[R + 1].vals = pre[R].vals + tot[R].vals;
         pre[R + 1].alg = pre[R].alg + tot[R].alg;
         pre[R + 1].bcols = pre[R].bcols + tot[R].bcols;
+        pre[R + 1].xblocks = pre[R].xblocks + tot[R].xblocks;
     }
     const RowTotals &T = pre[gb_m];
     if (T.bytes / 16 > (int64_t)UINT32_MAX || T.tiles > INT32_MAX) {
@@ -217,6 +220,15 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
         int64_t t_in_row = 0;
         const int64_t nt = tot[R].tiles;
         std::vector<int64_t> tb;
+        std::vector<double> sorted_val;
+        auto put_tile_val = [&](int64_t at_byte, double x) {
+            if (f32) {
+                const float f = (float)x;
+                std::memcpy(L.payload.data() + at_byte, &f, 4);
+            } else {
+                std::memcpy(L.payload.data() + at_byte, &x, 8);
+            }
+        };
         split_row(c, c.rowptr[R], c.rowptr[R + 1], [&](int64_t s, int64_t e) {
             tb.clear();
             for (int64_t p = s; p < e; ++p)
@@ -247,7 +259,6 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
                 const int ty = c.type(i);
                 const int64_t kk = c.k(i);
                 const uint32_t *pu = g.pay_u32.data() + g.u32_off[o];
-                const double *pf = g.pay_f64.data() + g.f64_off[o];
                 BlockDesc &bd = L.blocks[blk + q];
                 const int64_t vc = c.valid_cols(i);
                 bd.xbase = g.gather_flag
@@ -256,14 +267,6 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
                 bd.gb_col = (uint32_t)g.gb_col[i];
                 uint32_t steps = 0;
                 const uint32_t uni = (g.type_blk[i] & kUniform) ? 1u : 0u;
-                auto put_val = [&](int64_t at_byte, double x) {
-                    if (f32) {
-                        const float f = (float)x;
-                        std::memcpy(L.payload.data() + at_byte, &f, 4);
-                    } else {
-                        std::memcpy(L.payload.data() + at_byte, &x, 8);
-                    }
-                };
                 if (ty == kCOO) {
                     bd.off = (uint32_t)e0;
                     int run = 0, maxrun = 0, prev = -1;
@@ -285,10 +288,7 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
                         prev = (int)r;
                         maxrun = std::max(maxrun, run);
                         idx[e0 + q2] = (r << kColBits) | (uint32_t)col;
-                        const int64_t at = byte + vals_at + (e0 + q2) * vsz;
-                        put_val(at, pf[q2]);
                         const int64_t v = val + (e0 + q2);
-                        L.val_off[v] = (uint64_t)at;
                         L.val_row[v] = (int32_t)(R * bs + r);
                         L.val_col[v] = (int32_t)col;
                     }
@@ -310,6 +310,31 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
                 bd.meta = (uint32_t)ty | uni << 2 | (uint32_t)kk << 3 |
                           (uint32_t)vc << 14 | steps << 20;
                 if (ty == kCOO) e0 += kk;
+            }
+            // The tile's COO section is stored sorted by (row, column) over all
+            // of its COO blocks (keys are unique: distinct blocks hold distinct
+            // columns), so the entries a lane reads, 32 apart, never go down a
+            // row.  Stored value v keeps its block-major number; only its
+            // payload position moves.
+            if (E > 0) {
+                std::vector<uint64_t> key((size_t)E);
+                sorted_val.resize((size_t)E);
+                for (int64_t q2 = 0; q2 < E; ++q2)
+                    key[q2] = (uint64_t)idx[q2] << 16 | (uint64_t)q2;
+                std::sort(key.begin(), key.end());
+                int64_t e1 = 0;
+                for (size_t q = 0; q < (size_t)ncoo; ++q) {
+                    const int64_t i = tb[q];
+                    const double *pf = g.pay_f64.data() + g.f64_off[c.origin(i)];
+                    for (int64_t q2 = 0; q2 < c.k(i); ++q2, ++e1) sorted_val[e1] = pf[q2];
+                }
+                for (int64_t q2 = 0; q2 < E; ++q2) {
+                    const int64_t from = (int64_t)(key[q2] & 0xffff);
+                    idx[q2] = (uint32_t)(key[q2] >> 16);
+                    const int64_t at = byte + vals_at + q2 * vsz;
+                    put_tile_val(at, sorted_val[from]);
+                    L.val_off[val + from] = (uint64_t)at;
+                }
             }
             // value slots of CSR/DENSE blocks come after the tile's COO values
             int64_t v = val + E;
@@ -407,11 +432,12 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
         for (const BlockDesc &bd : L.blocks) all_e += meta_nnz(bd.meta);
         L.coo_share = all_e > 0 ? (double)coo_e / (double)all_e : 1.0;
     }
-    // algorithmic bytes: descriptors, payload without padding, gather-list
-    // reads of CSR/dense x tiles, x once, y once (split-row partial sums are
-    // scratch traffic, not counted)
+    // algorithmic bytes: tile descriptors, CSR/DENSE block descriptors (COO
+    // blocks need none: their entries carry row and column), payload without
+    // padding, gather-list reads of CSR/DENSE x tiles, x once, y once
+    // (split-row partial sums are scratch traffic, not counted)
     L.alg_bytes = T.tiles * (int64_t)sizeof(TileDesc) +
-                  T.blocks * (int64_t)sizeof(BlockDesc) + T.alg + T.bcols * 4 +
+                  T.xblocks * (int64_t)sizeof(BlockDesc) + T.alg + T.bcols * 4 +
                   g.n * vsz + g.m * vsz;
     return "";
 }
