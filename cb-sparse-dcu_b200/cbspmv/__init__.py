@@ -106,6 +106,12 @@ def _load():
         "cbspmv_destroy": (ctypes.c_int, [_P]),
         "cbspmv_last_error": (ctypes.c_size_t, [ctypes.c_char_p, ctypes.c_size_t]),
         "cbspmv_launch_count": (_I64, []),
+        "cbspmv_batch_create": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.POINTER(_P)]),
+        "cbspmv_batch_bind": (ctypes.c_int, [_P, _P, _P, _P]),
+        "cbspmv_batch_run": (ctypes.c_int, [_P, _P]),
+        "cbspmv_batch_run_each": (ctypes.c_int, [_P, _P]),
+        "cbspmv_batch_graph_launch": (ctypes.c_int, [_P, ctypes.c_int, _P]),
+        "cbspmv_batch_destroy": (ctypes.c_int, [_P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -344,6 +350,59 @@ class Plan:
                                    ctypes.byref(met)))
         self._uploaded = True
         return y, {"runtime": met.runtime_ms, "gflops": met.gflops}
+
+
+class Batch:
+    """Several uploaded plans run together (cbspmv_batch_*): Y_k = A_k X_k,
+    X_k (n_k, nrhs[k]) and Y_k (m_k, nrhs[k]) contiguous CUDA tensors.
+    ``run`` is one persistent kernel launch over all matrices, ``run_each``
+    one launch per matrix, ``graph_launch`` replays a CUDA graph of either."""
+
+    def __init__(self, plans, nrhs, stream=None):
+        self.plans = list(plans)
+        for p in self.plans:
+            p.upload(stream)
+        self.nrhs = [int(k) for k in nrhs]
+        if len(self.nrhs) != len(self.plans):
+            raise CBSpMVError(1, "one nrhs value per plan")
+        arr = (_P * len(self.plans))(*[p._h for p in self.plans])
+        k = np.ascontiguousarray(self.nrhs, np.int32)
+        h = ctypes.c_void_p()
+        _check(_lib.cbspmv_batch_create(ctypes.cast(arr, _P), len(self.plans),
+                                        _np_ptr(k), ctypes.byref(h)))
+        self._h = h
+        self._io = None
+
+    def bind(self, xs, ys, stream=None):
+        """Binds lists of CUDA tensors (kept referenced by the batch)."""
+        for p, x, y in zip(self.plans, xs, ys):
+            p._check_dev(x, y)
+        xa = (_P * len(xs))(*[t.data_ptr() for t in xs])
+        ya = (_P * len(ys))(*[t.data_ptr() for t in ys])
+        _check(_lib.cbspmv_batch_bind(self._h, ctypes.cast(xa, _P), ctypes.cast(ya, _P),
+                                      _stream(stream)))
+        self._io = (list(xs), list(ys))
+        return self
+
+    def run(self, stream=None):
+        _check(_lib.cbspmv_batch_run(self._h, _stream(stream)))
+
+    def run_each(self, stream=None):
+        _check(_lib.cbspmv_batch_run_each(self._h, _stream(stream)))
+
+    def graph_launch(self, per_matrix: bool = False, stream=None):
+        _check(_lib.cbspmv_batch_graph_launch(self._h, int(per_matrix), _stream(stream)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.cbspmv_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def coo2block_gather(row, col, val, m, n, **opts) -> Plan:

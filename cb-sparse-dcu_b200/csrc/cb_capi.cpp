@@ -3,6 +3,7 @@
 // returns a status and records a message; none exits or throws.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cstring>
@@ -579,5 +580,233 @@ size_t cbspmv_last_error(char *buf, size_t len) {
 }
 
 int64_t cbspmv_launch_count(void) { return cb::kernel_launches(); }
+
+}  // extern "C"
+
+// ---- batches ---------------------------------------------------------------
+
+struct cbspmv_batch {
+    std::vector<cbspmv_plan *> plans;
+    std::vector<int> nrhs;
+    std::vector<cb::MatView> views;  // host copy of the device table
+    int bs = 16, f32 = 0, device = -1;
+    bool bound = false;
+    cb::MatView *d_views = nullptr;
+    int64_t *d_toff = nullptr, *d_wpart = nullptr;
+    int64_t nwarps = 0;
+    cudaStream_t cap[8] = {};
+    cudaEvent_t ev[9] = {};
+    cudaGraphExec_t exec[2] = {};
+    ~cbspmv_batch() {
+        for (cudaGraphExec_t &g : exec)
+            if (g) cudaGraphExecDestroy(g);
+        for (cudaEvent_t &e : ev)
+            if (e) cudaEventDestroy(e);
+        for (cudaStream_t &c : cap)
+            if (c) cudaStreamDestroy(c);
+        if (d_views) cudaFree(d_views);
+        if (d_toff) cudaFree(d_toff);
+        if (d_wpart) cudaFree(d_wpart);
+    }
+};
+
+namespace {
+
+cbspmv_status batch_check(cbspmv_batch *b, bool need_bound) {
+    if (!b) return fail(CBSPMV_ERR_INVALID, "null batch");
+    if (need_bound && !b->bound) return fail(CBSPMV_ERR_STATE, "batch has no bound x/y arrays");
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev != b->device) return fail(CBSPMV_ERR_STATE, "batch was created on another device");
+    return CBSPMV_OK;
+}
+
+cbspmv_status batch_each(cbspmv_batch *b, cudaStream_t st) {
+    for (size_t k = 0; k < b->plans.size(); ++k) {
+        const cb::MatView &v = b->views[k];
+        cbspmv_status rc = run_side(b->plans[k], b->plans[k]->A, v.x, v.y, v.nrhs, v.ldx,
+                                    v.ldy, st);
+        if (rc) return rc;
+    }
+    return CBSPMV_OK;
+}
+
+cbspmv_status batch_one(cbspmv_batch *b, cudaStream_t st) {
+    CB_CUDA(cb::launch_batch(b->bs, b->f32, b->d_views, (int)b->views.size(), b->d_toff,
+                             b->d_wpart, b->nwarps, st),
+            "batch launch");
+    return CBSPMV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+cbspmv_status cbspmv_batch_create(cbspmv_plan *const *plans, int count, const int *nrhs,
+                                  cbspmv_batch **out) {
+    if (!plans || !nrhs || !out || count < 1)
+        return fail(CBSPMV_ERR_INVALID, "batch needs count >= 1 plans and nrhs values");
+    *out = nullptr;
+    int dev = -1;
+    cudaGetDevice(&dev);
+    for (int k = 0; k < count; ++k) {
+        const cbspmv_plan *p = plans[k];
+        if (!p) return fail(CBSPMV_ERR_INVALID, "null plan in batch");
+        if (!p->uploaded) return fail(CBSPMV_ERR_STATE, "batch plan not uploaded");
+        if (p->device != dev)
+            return fail(CBSPMV_ERR_STATE, "batch plans must be uploaded to the current device");
+        if (p->opts.block_size != plans[0]->opts.block_size ||
+            p->opts.value_type != plans[0]->opts.value_type)
+            return fail(CBSPMV_ERR_INVALID, "batch plans must share block size and value type");
+        if (nrhs[k] < 1) return fail(CBSPMV_ERR_INVALID, "nrhs must be >= 1");
+    }
+    cbspmv_batch *b = new (std::nothrow) cbspmv_batch();
+    if (!b) return fail(CBSPMV_ERR_ALLOC, "out of host memory");
+    b->plans.assign(plans, plans + count);
+    b->nrhs.assign(nrhs, nrhs + count);
+    b->bs = plans[0]->opts.block_size;
+    b->f32 = plans[0]->opts.value_type == CBSPMV_F32;
+    b->device = dev;
+    // per-matrix views (x, y bound later) and the concatenated tile list
+    std::vector<int64_t> toff(count + 1, 0);
+    std::vector<int64_t> cost;
+    for (int k = 0; k < count; ++k) {
+        DevSide &s = plans[k]->A;
+        cbspmv_status rc = ensure_partials(s, nrhs[k], vsize(plans[k]));
+        if (rc) {
+            delete b;
+            return rc;
+        }
+        b->views.push_back(cb::mat_view(s.d, nullptr, nullptr, nrhs[k], nrhs[k], nrhs[k]));
+        const int64_t nt = (int64_t)s.lay.tiles.size();
+        toff[k + 1] = toff[k] + nt;
+        const uint32_t *t8 = reinterpret_cast<const uint32_t *>(s.lay.tiles.data());
+        const uint32_t *b4 = reinterpret_cast<const uint32_t *>(s.lay.blocks.data());
+        for (int64_t t = 0; t < nt; ++t) cost.push_back(cb::batch_tile_cost(t8 + 8 * t, b4, nrhs[k]));
+    }
+    // warps: what one launch keeps resident, rounded to whole CTAs
+    b->nwarps = std::max<int64_t>(8, cb::batch_warps(b->bs, b->f32));
+    b->nwarps = (b->nwarps + 7) / 8 * 8;
+    const int64_t ntot = toff[count];
+    std::vector<int64_t> part(b->nwarps + 1, ntot);
+    part[0] = 0;
+    {
+        double total = 0, acc = 0;
+        for (int64_t c : cost) total += (double)c;
+        int64_t w = 1;
+        for (int64_t t = 0; t < ntot && w < b->nwarps; ++t) {
+            acc += (double)cost[t];
+            while (w < b->nwarps && acc >= total * (double)w / (double)b->nwarps)
+                part[w++] = t + 1;
+        }
+    }
+    cudaError_t e = cudaMalloc((void **)&b->d_views, count * sizeof(cb::MatView));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_toff, toff.size() * sizeof(int64_t));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_wpart, part.size() * sizeof(int64_t));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_toff, toff.data(), toff.size() * sizeof(int64_t),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_wpart, part.data(), part.size() * sizeof(int64_t),
+                       cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        delete b;
+        return cuda_fail(e, "allocate batch tables");
+    }
+    *out = b;
+    return CBSPMV_OK;
+}
+
+cbspmv_status cbspmv_batch_bind(cbspmv_batch *b, const void *const *x, void *const *y,
+                                void *stream) {
+    cbspmv_status rc = batch_check(b, false);
+    if (rc) return rc;
+    if (!x || !y) return fail(CBSPMV_ERR_INVALID, "null x or y array");
+    for (size_t k = 0; k < b->views.size(); ++k) {
+        const DevSide &s = b->plans[k]->A;
+        if ((s.lay.m > 0 && !y[k]) || (s.lay.n > 0 && !x[k]))
+            return fail(CBSPMV_ERR_INVALID, "null x or y in batch");
+        b->views[k].x = x[k];
+        b->views[k].y = y[k];
+    }
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    CB_CUDA(cudaMemcpyAsync(b->d_views, b->views.data(), b->views.size() * sizeof(cb::MatView),
+                            cudaMemcpyHostToDevice, st),
+            "upload batch table");
+    CB_CUDA(cudaStreamSynchronize(st), "upload batch table");
+    if (b->exec[1]) {  // captured with the old pointers
+        cudaGraphExecDestroy(b->exec[1]);
+        b->exec[1] = nullptr;
+    }
+    b->bound = true;
+    return CBSPMV_OK;
+}
+
+cbspmv_status cbspmv_batch_run(cbspmv_batch *b, void *stream) {
+    cbspmv_status rc = batch_check(b, true);
+    if (rc) return rc;
+    return batch_one(b, static_cast<cudaStream_t>(stream));
+}
+
+cbspmv_status cbspmv_batch_run_each(cbspmv_batch *b, void *stream) {
+    cbspmv_status rc = batch_check(b, true);
+    if (rc) return rc;
+    return batch_each(b, static_cast<cudaStream_t>(stream));
+}
+
+cbspmv_status cbspmv_batch_graph_launch(cbspmv_batch *b, int per_matrix, void *stream) {
+    cbspmv_status rc = batch_check(b, true);
+    if (rc) return rc;
+    const int mode = per_matrix ? 1 : 0;
+    if (!b->exec[mode]) {
+        for (int q = 0; q < 8; ++q)
+            if (!b->cap[q]) CB_CUDA(cudaStreamCreateWithFlags(&b->cap[q], cudaStreamNonBlocking),
+                                    "create capture stream");
+        for (int q = 0; q < 9; ++q)
+            if (!b->ev[q]) CB_CUDA(cudaEventCreateWithFlags(&b->ev[q], cudaEventDisableTiming),
+                                   "create capture event");
+        // one eager run first: launchers configure their kernels on first use
+        rc = mode ? batch_each(b, b->cap[0]) : batch_one(b, b->cap[0]);
+        if (rc) return rc;
+        CB_CUDA(cudaStreamSynchronize(b->cap[0]), "batch warm-up");
+        CB_CUDA(cudaStreamBeginCapture(b->cap[0], cudaStreamCaptureModeRelaxed), "begin capture");
+        cbspmv_status crc = CBSPMV_OK;
+        if (!mode) {
+            crc = batch_one(b, b->cap[0]);
+        } else {  // fork into 8 branches, round-robin over the matrices, join
+            cudaEventRecord(b->ev[8], b->cap[0]);
+            for (int q = 1; q < 8; ++q) cudaStreamWaitEvent(b->cap[q], b->ev[8], 0);
+            for (size_t k = 0; k < b->plans.size() && !crc; ++k) {
+                const cb::MatView &v = b->views[k];
+                crc = run_side(b->plans[k], b->plans[k]->A, v.x, v.y, v.nrhs, v.ldx, v.ldy,
+                               b->cap[k % 8]);
+            }
+            for (int q = 1; q < 8; ++q) {
+                cudaEventRecord(b->ev[q], b->cap[q]);
+                cudaStreamWaitEvent(b->cap[0], b->ev[q], 0);
+            }
+        }
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(b->cap[0], &graph);
+        if (crc) {
+            if (graph) cudaGraphDestroy(graph);
+            return crc;
+        }
+        if (ce != cudaSuccess) return cuda_fail(ce, "end capture");
+        const cudaError_t ie = cudaGraphInstantiate(&b->exec[mode], graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) {
+            b->exec[mode] = nullptr;
+            return cuda_fail(ie, "instantiate batch graph");
+        }
+    }
+    CB_CUDA(cudaGraphLaunch(b->exec[mode], static_cast<cudaStream_t>(stream)), "graph launch");
+    return CBSPMV_OK;
+}
+
+cbspmv_status cbspmv_batch_destroy(cbspmv_batch *b) {
+    delete b;
+    return CBSPMV_OK;
+}
 
 }  // extern "C"

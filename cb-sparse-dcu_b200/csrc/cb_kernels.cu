@@ -28,6 +28,7 @@
 #include <mutex>
 #include <type_traits>
 
+#include "cb_device.cuh"
 #include "cb_kernels.hpp"
 
 namespace cb {
@@ -35,14 +36,14 @@ namespace {
 
 // kernels this library has launched (all devices, all plans)
 std::atomic<int64_t> g_kernel_launches{0};
-inline void note_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
 
-constexpr unsigned kFull = 0xffffffffu;
+using dev::a16;
+using dev::add_entries;
+using dev::kColMask;
+using dev::kFull;
 constexpr int kWarps = 8;
-constexpr uint32_t kColMask = (1u << 27) - 1;
 
 __host__ __device__ constexpr int max_xt(int bs) { return bs == 16 ? 16 : 8; }
-__host__ __device__ constexpr uint32_t a16(uint32_t x) { return (x + 15u) & ~15u; }
 
 // Per-warp shared memory.  acc holds one private accumulator per lane and row:
 // lane l's copy of row r is acc[r * 32 + l].  Entries accumulate without
@@ -86,39 +87,6 @@ __device__ __forceinline__ T reduce_rows(T *acc, int lane) {
         }
     }
     return s;
-}
-
-// Adds K COO entries held by this lane -- slot u is the tile entry at
-// position pos0 + 32u, valid while below E -- into the lane's accumulators
-// (row r at myacc[r * 32]).  A tile's COO entries are stored sorted by row, so
-// the rows of a lane's slots never decrease: equal-row slots are summed in
-// registers, each run of them adds to the accumulator once, and since
-// different runs are different rows every load can be issued before any store.
-template <typename T, int K>
-__device__ __forceinline__ void add_entries(T *myacc, const uint32_t *w, const T *v,
-                                            const T *xv, int pos0, int E) {
-    uint32_t r[K];
-    T s[K];
-#pragma unroll
-    for (int u = 0; u < K; ++u) r[u] = w[u] >> 27;
-#pragma unroll
-    for (int u = 0; u < K; ++u)
-        s[u] = fma(v[u], xv[u], (u > 0 && r[u] == r[u > 0 ? u - 1 : 0]) ? s[u > 0 ? u - 1 : 0]
-                                                                          : T(0));
-    bool f[K];
-#pragma unroll
-    for (int u = 0; u < K; ++u) {
-        const bool valid = pos0 + 32 * u < E;
-        const bool more = u + 1 < K && pos0 + 32 * (u + 1) < E &&
-                          r[u + 1 < K ? u + 1 : u] == r[u];
-        f[u] = valid && !more;
-    }
-    T a[K];
-#pragma unroll
-    for (int u = 0; u < K; ++u) a[u] = f[u] ? myacc[r[u] * 32] : T(0);
-#pragma unroll
-    for (int u = 0; u < K; ++u)
-        if (f[u]) myacc[r[u] * 32] = a[u] + s[u];
 }
 
 // Persistent warps fetch tiles from a global counter (sched[0]); the warp
@@ -438,7 +406,7 @@ __device__ __forceinline__ void add_tile(const uint4 ta, const uint4 tb, const S
                                          const T *__restrict__ x, int lane) {
     T *myacc = &acc[lane];  // row r at myacc[r * 32]
     const int E = (int)tb.x;
-    add_entries<T, kStreamChunk>(myacc, g.w, g.v, g.x, lane, E);
+    add_entries<T, kStreamChunk>(myacc, g.w, g.v, g.x, lane, 32, E);
     const int ncoo = (ta.z >> 8) & 0xff;
     const int nxtb = (ta.z >> 16) & 0xff;
     if (nxtb) {  // CSR and DENSE blocks, read from global memory
@@ -810,6 +778,7 @@ cudaError_t launch_tiles(const DevLayout &d, const void *x, void *y, int nrhs,
                          int64_t ldx, int64_t ldy, cudaStream_t stream) {
     if (nrhs == 1 && ldx == 1 && ldy == 1 && use_stream(d))
         return launch_stream<T, BS>(d, x, y, stream);
+    if (nrhs > 1) return launch_spmm(d, x, y, nrhs, ldx, ldy, 0, stream);
     switch (chunk_choice(sizeof(T))) {
         case 4: return launch_chunk<T, BS, 4>(d, x, y, nrhs, ldx, ldy, stream);
         case 6: return launch_chunk<T, BS, 6>(d, x, y, nrhs, ldx, ldy, stream);
@@ -820,6 +789,7 @@ cudaError_t launch_tiles(const DevLayout &d, const void *x, void *y, int nrhs,
 }  // namespace
 
 int64_t kernel_launches() { return g_kernel_launches.load(); }
+void note_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
 
 size_t spmv_smem_bytes(int bs, int f32) {
     if (bs == 16)

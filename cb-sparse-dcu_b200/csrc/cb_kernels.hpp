@@ -26,6 +26,40 @@ struct DevLayout {
     int64_t nwarps = 0;               // streaming: warps of the launch
 };
 
+// One matrix as the multi-right-hand-side and batch kernels see it (plain
+// data, copied to the device as a table for batches).
+struct MatView {
+    const uint4 *tiles = nullptr;
+    const uint4 *blocks = nullptr;
+    const uint8_t *payload = nullptr;
+    const int32_t *block_cols = nullptr;
+    const void *x = nullptr;    // n x nrhs, row stride ldx
+    void *y = nullptr;          // m x nrhs, row stride ldy
+    void *partials = nullptr;   // slots * nrhs * bs values
+    int32_t *counters = nullptr;
+    int64_t ntiles = 0, m = 0, ldx = 1, ldy = 1;
+    int nrhs = 1, gather = 0;
+    int lanes = 1;              // lanes per entry (spmm_lanes(nrhs))
+};
+
+// Lanes per stored entry of the multi-right-hand-side kernel for nrhs
+// right-hand sides: the next power of two, at most 32.
+int spmm_lanes(int nrhs);
+MatView mat_view(const DevLayout &d, const void *x, void *y, int nrhs, int64_t ldx,
+                 int64_t ldy);
+// Y = A X through the multi-right-hand-side kernel (lanes = 0: spmm_lanes).
+cudaError_t launch_spmm(const DevLayout &d, const void *x, void *y, int nrhs, int64_t ldx,
+                        int64_t ldy, int lanes, cudaStream_t stream);
+// Batch: warps one launch keeps resident on the current device, and the
+// launch itself over a device table of nmats matrices (tile offsets
+// toff[nmats + 1], warp ranges wpart[nwarps + 1] over the concatenated tiles).
+int64_t batch_warps(int bs, int f32);
+cudaError_t launch_batch(int bs, int f32, const MatView *mats, int nmats, const int64_t *toff,
+                         const int64_t *wpart, int64_t nwarps, cudaStream_t stream);
+// Relative cost of one tile (TileDesc words, the layout's BlockDesc words)
+// with nrhs right-hand sides, for balancing warps over a batch.
+int64_t batch_tile_cost(const uint32_t *tile8, const uint32_t *blocks4, int nrhs);
+
 // Warps of a streaming-kernel launch for this layout on the current device,
 // or 0 when the direct kernel is the one that runs.
 int64_t stream_warps(const DevLayout &d);
@@ -58,8 +92,10 @@ cudaError_t launch_grad_vals(int f32, int64_t nvals, const int32_t *vrow,
                              const void *x, int64_t ldx, int nrhs, void *gvals,
                              cudaStream_t stream);
 
-// Kernel launches made by this library so far (every launcher above).
+// Kernel launches made by this library so far (every launcher above);
+// note_launch() counts one.
 int64_t kernel_launches();
+void note_launch();
 
 // Dynamic shared memory of the SpMV kernel per CTA.
 size_t spmv_smem_bytes(int bs, int f32);

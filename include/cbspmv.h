@@ -207,6 +207,43 @@ cbspmv_status cbspmv_destroy(cbspmv_plan *plan);
  * length. */
 size_t cbspmv_last_error(char *buf, size_t len);
 
+/* ---- batches (no counterpart in the reference) ------------------------ */
+
+/* Many uploaded plans -- same block size and value type, same device -- run
+ * together: Y_k = A_k X_k for k < count, X_k row-major n_k x nrhs[k] and Y_k
+ * row-major m_k x nrhs[k] (contiguous rows), nrhs[k] >= 1 per matrix.  One
+ * batch launch runs every matrix in ONE persistent kernel whose warps take
+ * host-balanced ranges of all the matrices' tiles; the warp ranges are
+ * computed here for the current device.  A plan may belong to several
+ * batches but is run by one of them (or by itself) at a time. */
+typedef struct cbspmv_batch cbspmv_batch;
+
+cbspmv_status cbspmv_batch_create(cbspmv_plan *const *plans, int count,
+                                  const int *nrhs, cbspmv_batch **out);
+
+/* Binds the device arrays X_k (x[k]) and Y_k (y[k]) used by every later run
+ * (host arrays of `count` device pointers).  Re-binding is allowed; a
+ * per-matrix graph (below) is captured again after it. */
+cbspmv_status cbspmv_batch_bind(cbspmv_batch *batch, const void *const *x,
+                                void *const *y, void *stream);
+
+/* One kernel launch over all matrices; allocates and copies nothing, so it
+ * can be captured in a CUDA graph by the caller. */
+cbspmv_status cbspmv_batch_run(cbspmv_batch *batch, void *stream);
+
+/* The same result as one cbspmv_spmv launch per matrix, in order (the
+ * unbatched way, kept for comparison). */
+cbspmv_status cbspmv_batch_run_each(cbspmv_batch *batch, void *stream);
+
+/* Replays a CUDA graph held by the batch: per_matrix = 0 captures
+ * cbspmv_batch_run, per_matrix = 1 captures the per-matrix launches spread
+ * over 8 parallel branches.  Captured on first use (and after a re-bind),
+ * then launched on `stream`. */
+cbspmv_status cbspmv_batch_graph_launch(cbspmv_batch *batch, int per_matrix,
+                                        void *stream);
+
+cbspmv_status cbspmv_batch_destroy(cbspmv_batch *batch);
+
 /* Number of kernels this library launched in the calling process. */
 int64_t cbspmv_launch_count(void);
 
