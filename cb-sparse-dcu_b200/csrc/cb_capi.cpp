@@ -56,6 +56,7 @@ struct DevSide {
     void *partials = nullptr;
     int32_t *counters = nullptr;
     uint32_t *wpart = nullptr;
+    int64_t *ustart = nullptr;
     int partial_nrhs = 0;
     int64_t *vsrc_ptr = nullptr;
     int32_t *vsrc = nullptr;
@@ -64,13 +65,14 @@ struct DevSide {
 
     void release() {
         void *ps[] = {tiles, blocks, payload, block_cols, partials, counters,
-                      wpart, vsrc_ptr, vsrc, val_off, val_row, val_col};
+                      wpart, ustart, vsrc_ptr, vsrc, val_off, val_row, val_col};
         for (void *p : ps)
             if (p) cudaFree(p);
         tiles = blocks = partials = nullptr;
         payload = nullptr;
         block_cols = counters = vsrc = val_row = val_col = nullptr;
         wpart = nullptr;
+        ustart = nullptr;
         vsrc_ptr = nullptr;
         val_off = nullptr;
         partial_nrhs = 0;
@@ -131,6 +133,7 @@ cbspmv_status upload_side(DevSide &s, cudaStream_t st) {
     s.d.gather = L.gather;
     s.d.m = L.m;
     s.d.n = L.n;
+    s.d.pay16_end = (uint32_t)(L.payload.size() / 16);
     s.d.sched = reinterpret_cast<uint32_t *>(s.counters);
     s.d.counters = s.counters + 4;
     s.d.max_entries = L.max_entries;
@@ -138,15 +141,38 @@ cbspmv_status upload_side(DevSide &s, cudaStream_t st) {
     return CBSPMV_OK;
 }
 
-// The streaming kernel's per-warp tile ranges, for this device's grid.
+// The streaming kernel's per-warp tile ranges for this device's grid, and the
+// multi-right-hand-side kernel's tile buffer size.
 cbspmv_status upload_partition(DevSide &s, int kernel, cudaStream_t st) {
     s.d.kernel = kernel;
     const int64_t warps = cb::stream_warps(s.d);
-    if (warps <= 0) return CBSPMV_OK;  // the direct kernel will run
-    const std::vector<uint32_t> part = cb::partition_tiles(s.lay, warps);
-    CB_CUDA(upload_vec(part, &s.wpart, st), "upload tile partition");
-    s.d.wpart = s.wpart;
-    s.d.nwarps = warps;
+    if (warps > 0) {  // else the direct kernel runs single vectors
+        const std::vector<uint32_t> part = cb::partition_tiles(s.lay, warps);
+        CB_CUDA(upload_vec(part, &s.wpart, st), "upload tile partition");
+        s.d.wpart = s.wpart;
+        s.d.nwarps = warps;
+    }
+    // several right-hand sides: tile buffer size and scheduling units
+    s.d.mcap = cb::ms_cap(s.lay.max_tile_bytes);
+    const int64_t nt = (int64_t)s.lay.tiles.size();
+    if (nt > 0) {  // one cost-balanced range of tiles per resident warp
+        const int64_t warps = std::min<int64_t>(nt, cb::ms_warps(s.lay.bs, s.lay.f32, s.d.mcap));
+        if (warps <= 0) return fail(CBSPMV_ERR_CUDA, "multi-right-hand-side kernel setup");
+        const uint32_t *t8 = reinterpret_cast<const uint32_t *>(s.lay.tiles.data());
+        const uint32_t *b4 = reinterpret_cast<const uint32_t *>(s.lay.blocks.data());
+        double total = 0, acc = 0;
+        std::vector<int64_t> cost(nt);
+        for (int64_t t = 0; t < nt; ++t) total += (double)(cost[t] = cb::ms_tile_cost(t8 + 8 * t, b4));
+        std::vector<int64_t> us(1, 0);
+        for (int64_t t = 0; t < nt && (int64_t)us.size() < warps; ++t) {
+            acc += (double)cost[t];
+            if (acc >= total * (double)us.size() / (double)warps && t + 1 < nt) us.push_back(t + 1);
+        }
+        s.d.nunits = (int64_t)us.size();
+        us.push_back(nt);
+        CB_CUDA(upload_vec(us, &s.ustart, st), "upload scheduling units");
+        s.d.ustart = s.ustart;
+    }
     return CBSPMV_OK;
 }
 
@@ -585,15 +611,26 @@ int64_t cbspmv_launch_count(void) { return cb::kernel_launches(); }
 
 // ---- batches ---------------------------------------------------------------
 
+// Matrices of one launch class share a launch: their views are contiguous in
+// the device table from `first`, their tiles concatenated (toff) and split
+// over the launch's warps (wpart).
+struct BatchGroup {
+    cb::MsClass c;
+    int first = 0, count = 0;
+    int64_t *d_toff = nullptr, *d_ustart = nullptr;
+    int64_t ntot = 0, nunits = 0;  // tiles and scheduling units of the group
+    uint32_t *d_sched = nullptr;  // 4 scheduler words (unit counter, warps out, error)
+};
+
 struct cbspmv_batch {
-    std::vector<cbspmv_plan *> plans;
-    std::vector<int> nrhs;
-    std::vector<cb::MatView> views;  // host copy of the device table
+    std::vector<cbspmv_plan *> plans;  // in group order
+    std::vector<int> slot;             // caller's index k -> position in plans
+    std::vector<cb::MatView> views;    // host copy of the device table
+    std::vector<BatchGroup> groups;
     int bs = 16, f32 = 0, device = -1;
     bool bound = false;
     cb::MatView *d_views = nullptr;
-    int64_t *d_toff = nullptr, *d_wpart = nullptr;
-    int64_t nwarps = 0;
+    uint32_t tile_cap = 16;     // shared buffer bytes: every plan's largest tile
     cudaStream_t cap[8] = {};
     cudaEvent_t ev[9] = {};
     cudaGraphExec_t exec[2] = {};
@@ -604,9 +641,12 @@ struct cbspmv_batch {
             if (e) cudaEventDestroy(e);
         for (cudaStream_t &c : cap)
             if (c) cudaStreamDestroy(c);
+        for (BatchGroup &g : groups) {
+            if (g.d_toff) cudaFree(g.d_toff);
+            if (g.d_sched) cudaFree(g.d_sched);
+            if (g.d_ustart) cudaFree(g.d_ustart);
+        }
         if (d_views) cudaFree(d_views);
-        if (d_toff) cudaFree(d_toff);
-        if (d_wpart) cudaFree(d_wpart);
     }
 };
 
@@ -632,9 +672,10 @@ cbspmv_status batch_each(cbspmv_batch *b, cudaStream_t st) {
 }
 
 cbspmv_status batch_one(cbspmv_batch *b, cudaStream_t st) {
-    CB_CUDA(cb::launch_batch(b->bs, b->f32, b->d_views, (int)b->views.size(), b->d_toff,
-                             b->d_wpart, b->nwarps, st),
-            "batch launch");
+    for (const BatchGroup &g : b->groups)
+        CB_CUDA(cb::launch_batch(b->bs, b->f32, g.c, b->d_views + g.first, g.count, g.d_toff,
+                                 g.d_ustart, g.nunits, b->tile_cap, g.d_sched, st),
+                "batch launch");
     return CBSPMV_OK;
 }
 
@@ -662,53 +703,66 @@ cbspmv_status cbspmv_batch_create(cbspmv_plan *const *plans, int count, const in
     }
     cbspmv_batch *b = new (std::nothrow) cbspmv_batch();
     if (!b) return fail(CBSPMV_ERR_ALLOC, "out of host memory");
-    b->plans.assign(plans, plans + count);
-    b->nrhs.assign(nrhs, nrhs + count);
     b->bs = plans[0]->opts.block_size;
     b->f32 = plans[0]->opts.value_type == CBSPMV_F32;
     b->device = dev;
-    // per-matrix views (x, y bound later) and the concatenated tile list
-    std::vector<int64_t> toff(count + 1, 0);
-    std::vector<int64_t> cost;
     for (int k = 0; k < count; ++k) {
-        DevSide &s = plans[k]->A;
-        cbspmv_status rc = ensure_partials(s, nrhs[k], vsize(plans[k]));
+        cbspmv_status rc = ensure_partials(plans[k]->A, nrhs[k], vsize(plans[k]));
         if (rc) {
             delete b;
             return rc;
         }
-        b->views.push_back(cb::mat_view(s.d, nullptr, nullptr, nrhs[k], nrhs[k], nrhs[k]));
-        const int64_t nt = (int64_t)s.lay.tiles.size();
-        toff[k + 1] = toff[k] + nt;
-        const uint32_t *t8 = reinterpret_cast<const uint32_t *>(s.lay.tiles.data());
-        const uint32_t *b4 = reinterpret_cast<const uint32_t *>(s.lay.blocks.data());
-        for (int64_t t = 0; t < nt; ++t) cost.push_back(cb::batch_tile_cost(t8 + 8 * t, b4, nrhs[k]));
+        b->tile_cap = std::max(b->tile_cap, plans[k]->A.d.mcap);
     }
-    // warps: what one launch keeps resident, rounded to whole CTAs
-    b->nwarps = std::max<int64_t>(8, cb::batch_warps(b->bs, b->f32));
-    b->nwarps = (b->nwarps + 7) / 8 * 8;
-    const int64_t ntot = toff[count];
-    std::vector<int64_t> part(b->nwarps + 1, ntot);
-    part[0] = 0;
-    {
-        double total = 0, acc = 0;
-        for (int64_t c : cost) total += (double)c;
-        int64_t w = 1;
-        for (int64_t t = 0; t < ntot && w < b->nwarps; ++t) {
-            acc += (double)cost[t];
-            while (w < b->nwarps && acc >= total * (double)w / (double)b->nwarps)
-                part[w++] = t + 1;
+    // group by launch class, keeping the caller's order inside a group
+    std::vector<int> order(count);
+    std::iota(order.begin(), order.end(), 0);
+    auto key = [&](int k) {
+        const cb::MsClass c = cb::ms_class(nrhs[k], b->f32);
+        return c.V * 64 + c.RL;
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return key(a) < key(c); });
+    b->slot.assign(count, 0);
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < count;) {
+        BatchGroup g;
+        g.c = cb::ms_class(nrhs[order[i]], b->f32);
+        g.first = i;
+        std::vector<int64_t> toff(1, 0);
+        for (; i < count && key(order[i]) == key(order[g.first]); ++i) {
+            const int k = order[i];
+            b->slot[k] = i;
+            DevSide &s = plans[k]->A;
+            b->plans.push_back(plans[k]);
+            b->views.push_back(cb::mat_view(s.d, nullptr, nullptr, nrhs[k], nrhs[k], nrhs[k]));
+            toff.push_back(toff.back() + (int64_t)s.lay.tiles.size());
         }
+        g.count = i - g.first;
+        g.ntot = toff.back();
+        std::vector<int64_t> us;
+        // about four units per resident warp, at least two tiles each
+        const int64_t target = std::max<int64_t>(
+            2, g.ntot / (std::max<int64_t>(1, cb::ms_warps(b->bs, b->f32, b->tile_cap)) * 4));
+        for (int q = g.first; q < i; ++q) {
+            const DevSide &s = b->plans[q]->A;
+            cb::ms_unit_starts(reinterpret_cast<const uint32_t *>(s.lay.tiles.data()),
+                               (int64_t)s.lay.tiles.size(), target, toff[q - g.first], us);
+        }
+        g.nunits = (int64_t)us.size();
+        us.push_back(g.ntot);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&g.d_ustart, us.size() * sizeof(int64_t));
+        if (e == cudaSuccess)
+            e = cudaMemcpy(g.d_ustart, us.data(), us.size() * sizeof(int64_t),
+                           cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMalloc((void **)&g.d_toff, toff.size() * sizeof(int64_t));
+        if (e == cudaSuccess) e = cudaMalloc((void **)&g.d_sched, 16);
+        if (e == cudaSuccess) e = cudaMemset(g.d_sched, 0, 16);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(g.d_toff, toff.data(), toff.size() * sizeof(int64_t),
+                           cudaMemcpyHostToDevice);
+        b->groups.push_back(g);
     }
-    cudaError_t e = cudaMalloc((void **)&b->d_views, count * sizeof(cb::MatView));
-    if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_toff, toff.size() * sizeof(int64_t));
-    if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_wpart, part.size() * sizeof(int64_t));
-    if (e == cudaSuccess)
-        e = cudaMemcpy(b->d_toff, toff.data(), toff.size() * sizeof(int64_t),
-                       cudaMemcpyHostToDevice);
-    if (e == cudaSuccess)
-        e = cudaMemcpy(b->d_wpart, part.data(), part.size() * sizeof(int64_t),
-                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_views, count * sizeof(cb::MatView));
     if (e != cudaSuccess) {
         delete b;
         return cuda_fail(e, "allocate batch tables");
@@ -722,12 +776,13 @@ cbspmv_status cbspmv_batch_bind(cbspmv_batch *b, const void *const *x, void *con
     cbspmv_status rc = batch_check(b, false);
     if (rc) return rc;
     if (!x || !y) return fail(CBSPMV_ERR_INVALID, "null x or y array");
-    for (size_t k = 0; k < b->views.size(); ++k) {
-        const DevSide &s = b->plans[k]->A;
+    for (size_t k = 0; k < b->slot.size(); ++k) {
+        const int i = b->slot[k];
+        const DevSide &s = b->plans[i]->A;
         if ((s.lay.m > 0 && !y[k]) || (s.lay.n > 0 && !x[k]))
             return fail(CBSPMV_ERR_INVALID, "null x or y in batch");
-        b->views[k].x = x[k];
-        b->views[k].y = y[k];
+        cb::MatView &v = b->views[i];
+        v = cb::mat_view(s.d, x[k], y[k], v.nrhs, v.nrhs, v.nrhs);
     }
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
     CB_CUDA(cudaMemcpyAsync(b->d_views, b->views.data(), b->views.size() * sizeof(cb::MatView),

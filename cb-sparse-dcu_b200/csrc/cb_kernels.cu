@@ -297,63 +297,16 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
 // own copies in flight.  sched[0..1] are not used by this kernel; the
 // per-block-row arrival counters return to zero by the end of every launch.
 // ============================================================================
-constexpr uint32_t kWaitLimit = 1u << 22;
+using dev::bulk_g2s;
+using dev::fence_mbar_init;
+using dev::fence_proxy_async;
+using dev::kWaitLimit;
+using dev::mbar_arrive;
+using dev::mbar_arrive_tx;
+using dev::mbar_init;
+using dev::mbar_wait;
+using dev::policy_evict_first;
 constexpr int kStreamWarps = 4;  // warps per CTA
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
-                 : "memory");
-}
-__device__ __forceinline__ void fence_mbar_init() {
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-// orders this thread's (and, after a warp barrier, its warp's) generic
-// shared-memory accesses before later async-proxy writes (bulk copies)
-__device__ __forceinline__ void fence_proxy_async() {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(
-                     smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ uint64_t policy_evict_first() {
-    uint64_t p;
-    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
-// global -> this CTA's shared memory, completion counted on `bar`
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
-                                         uint64_t *bar, uint64_t policy) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
-        " [%0], [%1], %2, [%3], %4;" ::"r"(smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
-        : "memory");
-}
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t *err) {
-    for (uint32_t i = 0; i < kWaitLimit; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
-    atomicExch(err, 1u);
-    return false;
-}
 
 // Per-warp shared memory: [acc | xt | mbar[2] | buf[2]]; a buffer holds one
 // tile's COO section (`cap` bytes: indices, then values).
@@ -778,7 +731,7 @@ cudaError_t launch_tiles(const DevLayout &d, const void *x, void *y, int nrhs,
                          int64_t ldx, int64_t ldy, cudaStream_t stream) {
     if (nrhs == 1 && ldx == 1 && ldy == 1 && use_stream(d))
         return launch_stream<T, BS>(d, x, y, stream);
-    if (nrhs > 1) return launch_spmm(d, x, y, nrhs, ldx, ldy, 0, stream);
+    if (nrhs > 1) return launch_spmm(d, x, y, nrhs, ldx, ldy, stream);
     switch (chunk_choice(sizeof(T))) {
         case 4: return launch_chunk<T, BS, 4>(d, x, y, nrhs, ldx, ldy, stream);
         case 6: return launch_chunk<T, BS, 6>(d, x, y, nrhs, ldx, ldy, stream);

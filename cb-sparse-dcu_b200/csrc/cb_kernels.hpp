@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <vector>
 
 namespace cb {
 
@@ -24,6 +25,11 @@ struct DevLayout {
     double coo_share = 1.0;
     const uint32_t *wpart = nullptr;  // streaming: per-warp tile ranges
     int64_t nwarps = 0;               // streaming: warps of the launch
+    uint32_t pay16_end = 0;           // payload size in 16-byte units
+    // several right-hand sides: tile buffer bytes, scheduling units
+    uint32_t mcap = 0;
+    const int64_t *ustart = nullptr;  // nunits + 1 tile indices
+    int64_t nunits = 0;
 };
 
 // One matrix as the multi-right-hand-side and batch kernels see it (plain
@@ -39,26 +45,45 @@ struct MatView {
     int32_t *counters = nullptr;
     int64_t ntiles = 0, m = 0, ldx = 1, ldy = 1;
     int nrhs = 1, gather = 0;
-    int lanes = 1;              // lanes per entry (spmm_lanes(nrhs))
+    int xvec = 0;               // x rows allow vector loads of V values
+    uint32_t pay16_end = 0;     // payload size in 16-byte units
 };
 
-// Lanes per stored entry of the multi-right-hand-side kernel for nrhs
-// right-hand sides: the next power of two, at most 32.
-int spmm_lanes(int nrhs);
+// Launch class of the multi-right-hand-side kernel: RL lanes per stored
+// entry, V right-hand sides per lane (RL * V per pass).
+struct MsClass {
+    int RL = 1, V = 1;
+};
+
+// The class used for nrhs right-hand sides of the given value type.
+MsClass ms_class(int nrhs, int f32);
+// Shared-memory buffer bytes for tiles of at most max_tile_bytes.
+uint32_t ms_cap(int64_t max_tile_bytes);
 MatView mat_view(const DevLayout &d, const void *x, void *y, int nrhs, int64_t ldx,
                  int64_t ldy);
-// Y = A X through the multi-right-hand-side kernel (lanes = 0: spmm_lanes).
+// Scheduling units of the multi-right-hand-side kernel.  ms_warps: warps one
+// launch keeps resident on the current device; ms_tile_cost: relative cost of
+// one tile (TileDesc words, the layout's BlockDesc words), for cost-balanced
+// static units (one per warp) of a single matrix; ms_unit_starts: dynamic
+// units of a batch -- the unit starts of one matrix's tiles (TileDesc words;
+// tile indices offset by `base`) appended to ustart, boundaries at block-row
+// starts once a unit holds `target` tiles, anywhere at twice that.  The
+// caller appends the end (total tiles).
+int64_t ms_warps(int bs, int f32, uint32_t cap);
+int64_t ms_tile_cost(const uint32_t *tile8, const uint32_t *blocks4);
+void ms_unit_starts(const uint32_t *tile8, int64_t ntiles, int64_t target, int64_t base,
+                    std::vector<int64_t> &ustart);
+// Y = A X through the multi-right-hand-side kernel (d.mcap, d.ustart,
+// d.nunits set; scheduler words d.sched[0..1], error word d.sched[2]).
 cudaError_t launch_spmm(const DevLayout &d, const void *x, void *y, int nrhs, int64_t ldx,
-                        int64_t ldy, int lanes, cudaStream_t stream);
-// Batch: warps one launch keeps resident on the current device, and the
-// launch itself over a device table of nmats matrices (tile offsets
-// toff[nmats + 1], warp ranges wpart[nwarps + 1] over the concatenated tiles).
-int64_t batch_warps(int bs, int f32);
-cudaError_t launch_batch(int bs, int f32, const MatView *mats, int nmats, const int64_t *toff,
-                         const int64_t *wpart, int64_t nwarps, cudaStream_t stream);
-// Relative cost of one tile (TileDesc words, the layout's BlockDesc words)
-// with nrhs right-hand sides, for balancing warps over a batch.
-int64_t batch_tile_cost(const uint32_t *tile8, const uint32_t *blocks4, int nrhs);
+                        int64_t ldy, cudaStream_t stream);
+// The same kernel over a device table of nmats matrices of one class: tile
+// offsets toff[nmats + 1], units ustart[nunits + 1] over the concatenated
+// tiles, shared buffers of cap bytes (>= every matrix's largest tile), four
+// scheduler words (zero before the first launch; the kernel leaves them zero).
+cudaError_t launch_batch(int bs, int f32, MsClass c, const MatView *mats, int nmats,
+                         const int64_t *toff, const int64_t *ustart, int64_t nunits,
+                         uint32_t cap, uint32_t *sched, cudaStream_t stream);
 
 // Warps of a streaming-kernel launch for this layout on the current device,
 // or 0 when the direct kernel is the one that runs.

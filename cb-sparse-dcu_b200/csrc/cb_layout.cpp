@@ -22,6 +22,7 @@ inline int64_t a16(int64_t x) { return (x + 15) & ~int64_t(15); }
 struct Ctx {
     const HostCB &g;
     int bs, bits, vsz, isz, emax, max_xt;
+    int64_t max_bytes;  // tile payload cap (a larger single block is a tile alone)
     std::vector<int64_t> rowptr;  // device block order grouped by block row
     std::vector<int64_t> order;   // final block indices
     explicit Ctx(const HostCB &h) : g(h) {}
@@ -59,24 +60,33 @@ struct Ctx {
 
 // Greedy split of one block row's blocks (device order [b0, b1)) into tiles.
 // fn(tile_begin, tile_end) for each tile, in order; COO blocks first inside.
+// A tile also ends before its payload (COO section plus CSR/DENSE payloads)
+// would pass max_bytes, so a tile fits the multi-right-hand-side kernel's
+// shared-memory buffer.
 template <class Fn>
 void split_row(const Ctx &c, int64_t b0, int64_t b1, Fn fn) {
-    int64_t s = b0, nb = 0, e = 0, nxt = 0;
+    int64_t s = b0, nb = 0, e = 0, nxt = 0, xbytes = 0;
+    auto bytes = [&](int64_t ee, int64_t xb) { return a16(ee * 4) + a16(ee * c.vsz) + xb; };
     for (int64_t p = b0; p < b1; ++p) {
         const int64_t i = c.order[p];
         const bool coo = c.is_coo(i);
-        const bool full = nb == kTileBlocks || (coo && e + c.k(i) > c.emax) ||
-                          (!coo && nxt == c.max_xt);
+        const int64_t e2 = coo ? e + c.k(i) : e;
+        const int64_t x2 = coo ? xbytes : xbytes + c.payload_bytes(i);
+        const bool full = nb == kTileBlocks || (coo && e2 > c.emax) ||
+                          (!coo && nxt == c.max_xt) ||
+                          (nb > 0 && bytes(e2, x2) > c.max_bytes);
         if (full) {
             fn(s, p);
             s = p;
-            nb = e = nxt = 0;
+            nb = e = nxt = xbytes = 0;
         }
         ++nb;
-        if (coo)
+        if (coo) {
             e += c.k(i);
-        else
+        } else {
             ++nxt;
+            xbytes += c.payload_bytes(i);
+        }
     }
     fn(s, b1);  // also the single empty tile of an empty block row
 }
@@ -115,6 +125,7 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
     // the streaming kernel holds a whole tile's entries in registers
     if (auto_emax == kTileEntriesStream) c.emax = std::min(c.emax, kTileEntriesStream);
     c.max_xt = c.bs == 16 ? 16 : 8;
+    c.max_bytes = kTileBytes[c.bs == 16 ? 0 : 1][f32 ? 0 : 1];
     const int bs = c.bs, vsz = c.vsz, isz = c.isz;
     const int64_t gb_m = g.gb_m;
 
@@ -428,6 +439,13 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
         for (const TileDesc &t : L.tiles) {
             L.max_entries = std::max<int64_t>(L.max_entries, t.coo_entries);
             coo_e += t.coo_entries;
+        }
+        // tiles are contiguous in the payload, in order
+        for (size_t t = 0; t < L.tiles.size(); ++t) {
+            const int64_t end = t + 1 < L.tiles.size() ? (int64_t)L.tiles[t + 1].payload16 * 16
+                                                       : (int64_t)L.payload.size();
+            L.max_tile_bytes =
+                std::max<int64_t>(L.max_tile_bytes, end - (int64_t)L.tiles[t].payload16 * 16);
         }
         for (const BlockDesc &bd : L.blocks) all_e += meta_nnz(bd.meta);
         L.coo_share = all_e > 0 ? (double)coo_e / (double)all_e : 1.0;

@@ -28,6 +28,10 @@
 namespace cb {
 
 constexpr int kTileBlocks = 32;
+// Tile payload cap in bytes, [bs 16, bs 32][f32, f64]: at least one block of
+// the largest kind (bs 32 FP64 CSR: 9.7 KB) and a whole COO section of 512
+// entries.
+constexpr int64_t kTileBytes[2][2] = {{4096, 6144}, {8192, 12288}};
 constexpr int kTileEntries = 512;        // tile entry cap (the direct kernel's default)
 constexpr int kTileEntriesStream = 256;  // the streaming kernel's default
 constexpr int kColBits = 27;  // COO idx: column in bits 0..26
@@ -70,6 +74,7 @@ struct DeviceLayout {
     int64_t split_rows = 0;
     int max_row_tiles = 0;
     int64_t max_entries = 0;          // largest COO section (entries) of a tile
+    int64_t max_tile_bytes = 0;       // largest tile payload (bytes)
     double coo_share = 1.0;           // share of stored entries in COO blocks
     // stored values in device order
     int64_t nvals = 0;
