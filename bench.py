@@ -137,6 +137,117 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def _timed(fn, reps: int, warmup: int, flush=None):
+    """Mean device time (ms) of fn over reps runs after warmup runs, CUDA
+    events on the current stream around each run; flush(), when given, runs
+    before each timed run outside the events (an L2 flush for workloads that
+    fit in L2)."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    total = 0.0
+    for _ in range(reps):
+        if flush is not None:
+            flush()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    return total / reps
+
+
+def secondary_configs(dev, peak: float) -> dict:
+    """The other workloads of the benchmark suite, each timed on the device:
+    LAP (5-point Laplacian 256^2, FP64), PL in FP32, ST (27-point x 3 dof
+    stencil on 64^3, FP64 and FP32), DIFF (power-law n = 2^18, 8 right-hand
+    sides, FP32: forward, adjoint A^T G and the value gradient) and BAT (512
+    uneven FP32 matrices with 1-16 right-hand sides: one batched launch per
+    lane class, its CUDA graph, one launch per matrix, and a graph of those).
+    Every plan is autotuned first (cbspmv_autotune).  Algorithmic bytes: the
+    packed matrix the kernel must read, x and y once per right-hand side."""
+    import numpy as np
+    import torch
+    import cbspmv
+    from cbspmv import gen
+
+    l2_flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    flush = lambda: l2_flush.zero_()  # noqa: E731
+    out = {}
+
+    def single(name, coo, f32, reps=50):
+        plan = cbspmv.Plan(coo, value_type=int(f32))
+        kernel, _ = plan.autotune(1)
+        dt = torch.float32 if f32 else torch.float64
+        x = torch.from_numpy(gen.uniform_x(coo.n, 0)).to(dev, dt)
+        y = torch.empty(coo.m, dtype=dt, device=dev)
+        info = plan.info()
+        small = info["device_bytes"] < (200 << 20)
+        ms = _timed(lambda: plan.spmv(x, y), reps, 5, flush if small else None)
+        alg = info["algorithmic_bytes"]
+        out[name] = {"nnz": coo.nnz, "kernel": kernel, "ms": round(ms, 4),
+                     "gbs": round(alg / ms / 1e6, 1), "gflops": round(2 * coo.nnz / ms / 1e6, 1),
+                     "frac": round(alg / ms / 1e6 / peak, 4),
+                     "l2": "flushed before each step" if small else "inputs larger than L2"}
+        del plan
+
+    single("LAP fp64 (256^2 5-point)", gen.laplacian_2d(), False)
+    single("PL fp32 (n=2^20)", gen.power_law(), True)
+    st = gen.stencil_27pt()
+    single("ST fp64 (64^3 x 3 dof 27-point)", st, False, reps=20)
+    single("ST fp32 (64^3 x 3 dof 27-point)", st, True, reps=20)
+    del st
+
+    # DIFF: Y = A X, then G -> A^T G and the value gradient
+    coo = gen.power_law(1 << 18, seed=3, mean=24)
+    k = 8
+    plan = cbspmv.Plan(coo, value_type=1, want_transpose=1)
+    plan.autotune(k)
+    X = torch.from_numpy(np.ascontiguousarray(gen.uniform_x(coo.n, 1, nrhs=k).T)).to(dev, torch.float32)
+    G = torch.from_numpy(np.ascontiguousarray(gen.uniform_x(coo.m, 2, nrhs=k).T)).to(dev, torch.float32)
+    Y = torch.empty(coo.m, k, device=dev)
+    GX = torch.empty(coo.n, k, device=dev)
+    GV = torch.empty(plan.num_values(), device=dev)
+    info = plan.info()
+    xy = 4 * (coo.n + coo.m) * (k - 1)
+    fwd_bytes = info["algorithmic_bytes"] + xy
+    adj_bytes = fwd_bytes + plan.num_values() * (8 + 4) + 4 * (coo.n + coo.m) * k
+    t_f = _timed(lambda: plan.spmv(X, Y), 30, 5, flush)
+    t_a = _timed(lambda: (plan.spmv_t(G, GX), plan.grad_vals(G, X, GV)), 30, 5, flush)
+    out["DIFF fp32 (n=2^18, 8 rhs)"] = {
+        "nnz": coo.nnz, "fwd_ms": round(t_f, 4), "adj_ms": round(t_a, 4),
+        "fwd_plus_adj_over_fwd": round((t_f + t_a) / t_f, 3),
+        "fwd_gbs": round(fwd_bytes / t_f / 1e6, 1), "fwd_frac": round(fwd_bytes / t_f / 1e6 / peak, 4),
+        "adj_gbs": round(adj_bytes / t_a / 1e6, 1),
+        "gflops_fwd": round(2 * coo.nnz * k / t_f / 1e6, 1), "l2": "flushed before each step"}
+    del plan
+
+    # BAT
+    items = gen.batch_uneven()
+    plans = [cbspmv.Plan(it.coo, value_type=1) for it in items]
+    xs = [torch.rand(it.coo.n, it.nrhs, device=dev) for it in items]
+    ys = [torch.empty(it.coo.m, it.nrhs, device=dev) for it in items]
+    b = cbspmv.Batch(plans, [it.nrhs for it in items]).bind(xs, ys)
+    alg = sum(p.info()["algorithmic_bytes"] + 4 * (it.coo.n + it.coo.m) * (it.nrhs - 1)
+              for p, it in zip(plans, items))
+    r = {"matrices": len(items), "nnz": sum(it.coo.nnz for it in items), "algorithmic_bytes": alg}
+    for name, fn in (("batched", b.run), ("batched_graph", lambda: b.graph_launch(False)),
+                     ("per_matrix", b.run_each), ("per_matrix_graph", lambda: b.graph_launch(True))):
+        ms = _timed(fn, 5, 3)
+        r[name + "_ms"] = round(ms, 3)
+        r[name + "_gbs"] = round(alg / ms / 1e6, 1)
+    r["batched_frac"] = round(r["batched_gbs"] / peak, 4)
+    r["batched_over_per_matrix"] = round(r["per_matrix_ms"] / r["batched_ms"], 2)
+    r["l2"] = "inputs larger than L2"
+    out["BAT fp32 (512 matrices, 1-16 rhs)"] = r
+    b.close()
+    return out
+
+
 def _dist():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -232,6 +343,8 @@ def main():
     ap.add_argument("--impl", default="cbspmv", choices=["cbspmv", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=300)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--configs", default="all", choices=["all", "none"],
+                    help="also time the other workloads (rank 0, N=1 only)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -318,6 +431,9 @@ def main():
             "kernel": "cb_spmv_stream_kernel (the one launch of each SpMV)"}
 
     line = None
+    configs = None
+    if rank == 0 and world == 1 and args.configs == "all":
+        configs = secondary_configs(dev, peak)
     if rank == 0:
         cpu_dt, kind, reps = _ref_cpu(coo, x_host, args.cpu_seconds, 400)
         cpu = {"value": round(alg / cpu_dt / 1e9, 3), "unit": UNIT, "cores": 1, "kind": kind,
@@ -344,6 +460,8 @@ def main():
             "gpu_launches": launches,
             "clocks": clk.summary(),
         }
+        if configs is not None:
+            line["configs"] = configs
     pg.close()
     if line:
         print(json.dumps(line), flush=True)

@@ -106,6 +106,7 @@ def _load():
         "cbspmv_destroy": (ctypes.c_int, [_P]),
         "cbspmv_last_error": (ctypes.c_size_t, [ctypes.c_char_p, ctypes.c_size_t]),
         "cbspmv_launch_count": (_I64, []),
+        "cbspmv_autotune": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _P]),
         "cbspmv_batch_create": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.POINTER(_P)]),
         "cbspmv_batch_bind": (ctypes.c_int, [_P, _P, _P, _P]),
         "cbspmv_batch_run": (ctypes.c_int, [_P, _P]),
@@ -295,6 +296,17 @@ class Plan:
         _check(_lib.cbspmv_spmv(self._h, _dptr(x), _dptr(y), k, k, k,
                                 _stream(stream)))
         return y
+
+    def autotune(self, nrhs: int = 1, stream=None):
+        """Times the kernels that can run this plan for nrhs right-hand sides
+        and keeps the fastest; returns (kernel, ms)."""
+        self.upload(stream)
+        k = ctypes.c_int()
+        ms = ctypes.c_double()
+        _check(_lib.cbspmv_autotune(self._h, int(nrhs), _stream(stream), ctypes.byref(k),
+                                    ctypes.byref(ms)))
+        self.opts.kernel = k.value
+        return k.value, ms.value
 
     def spmv_t(self, g, gx=None, stream=None):
         """gx = A^T g (needs want_transpose=1)."""

@@ -144,8 +144,11 @@ cbspmv_status upload_side(DevSide &s, cudaStream_t st) {
 // The streaming kernel's per-warp tile ranges for this device's grid, and the
 // multi-right-hand-side kernel's tile buffer size.
 cbspmv_status upload_partition(DevSide &s, int kernel, cudaStream_t st) {
-    s.d.kernel = kernel;
+    // the streaming partition whenever the layout allows that kernel, so a
+    // later kernel choice (cbspmv_autotune) needs no new upload
+    s.d.kernel = kernel == 0 || kernel == 1 ? kernel : 1;
     const int64_t warps = cb::stream_warps(s.d);
+    s.d.kernel = kernel;
     if (warps > 0) {  // else the direct kernel runs single vectors
         const std::vector<uint32_t> part = cb::partition_tiles(s.lay, warps);
         CB_CUDA(upload_vec(part, &s.wpart, st), "upload tile partition");
@@ -245,8 +248,8 @@ cbspmv_status cbspmv_coo2block_gather(const cbspmv_coo *coo,
     if (opts) o = *opts;
     if (o.value_type != CBSPMV_F64 && o.value_type != CBSPMV_F32)
         return fail(CBSPMV_ERR_INVALID, "value_type must be CBSPMV_F64 or CBSPMV_F32");
-    if (o.kernel < 0 || o.kernel > 2)
-        return fail(CBSPMV_ERR_INVALID, "kernel must be 0 (auto), 1 or 2");
+    if (o.kernel < 0 || o.kernel > 3)
+        return fail(CBSPMV_ERR_INVALID, "kernel must be 0 (auto), 1, 2 or 3");
     cbspmv_plan *p = new (std::nothrow) cbspmv_plan;
     if (!p) return fail(CBSPMV_ERR_ALLOC, "out of host memory");
     p->opts = o;
@@ -357,6 +360,72 @@ cbspmv_status cbspmv_spmv_noalloc(cbspmv_plan *p, const void *x, void *y, int nr
     CB_CUDA(cb::launch_spmv_fixed_scratch(s.d, s.lay.gb_m, s.lay.slots, x, y, nrhs, ldx,
                                           ldy, (cudaStream_t)stream),
             "spmv_noalloc launch");
+    return CBSPMV_OK;
+}
+
+cbspmv_status cbspmv_autotune(cbspmv_plan *p, int nrhs, void *stream, int *kernel, double *ms) {
+    if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
+    if (!p->uploaded) return fail(CBSPMV_ERR_STATE, "plan not uploaded");
+    if (nrhs < 1) return fail(CBSPMV_ERR_INVALID, "nrhs must be >= 1");
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    DevSide &s = p->A;
+    std::vector<int> cands;
+    if (nrhs == 1) {
+        cb::DevLayout probe = s.d;
+        probe.kernel = 1;
+        if (s.d.wpart && cb::stream_warps(probe) > 0) cands.push_back(1);
+        cands.push_back(2);
+    }
+    cands.push_back(3);
+    const size_t vsz = vsize(p);
+    void *x = nullptr, *y = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    auto cleanup = [&]() {
+        if (x) cudaFree(x);
+        if (y) cudaFree(y);
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    };
+    cudaError_t e = cudaMalloc(&x, std::max<size_t>(1, (size_t)s.lay.n * nrhs * vsz));
+    if (e == cudaSuccess) e = cudaMalloc(&y, std::max<size_t>(1, (size_t)s.lay.m * nrhs * vsz));
+    if (e == cudaSuccess) e = cudaMemsetAsync(x, 0, (size_t)s.lay.n * nrhs * vsz, st);
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e != cudaSuccess) {
+        cleanup();
+        return cuda_fail(e, "autotune scratch");
+    }
+    const int keep = s.d.kernel;
+    int best = -1;
+    float best_ms = 0.f;
+    for (int k : cands) {
+        s.d.kernel = k;
+        cbspmv_status rc = CBSPMV_OK;
+        for (int i = 0; i < 3 && !rc; ++i) rc = run_side(p, s, x, y, nrhs, nrhs, nrhs, st);
+        constexpr int reps = 10;
+        cudaEventRecord(e0, st);
+        for (int i = 0; i < reps && !rc; ++i) rc = run_side(p, s, x, y, nrhs, nrhs, nrhs, st);
+        cudaEventRecord(e1, st);
+        e = cudaEventSynchronize(e1);
+        if (rc || e != cudaSuccess) {
+            s.d.kernel = keep;
+            cleanup();
+            return rc ? rc : cuda_fail(e, "autotune timing");
+        }
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        t /= reps;
+        if (best < 0 || t < best_ms) {
+            best = k;
+            best_ms = t;
+        }
+    }
+    cleanup();
+    s.d.kernel = best;
+    p->opts.kernel = best;
+    if (p->has_t) p->AT.d.kernel = best == 1 && !p->AT.d.wpart ? 2 : best;
+    if (kernel) *kernel = best;
+    if (ms) *ms = best_ms;
     return CBSPMV_OK;
 }
 

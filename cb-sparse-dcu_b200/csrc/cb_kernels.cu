@@ -717,12 +717,12 @@ cudaError_t launch_stream(const DevLayout &d, const void *x, void *y, cudaStream
 }
 
 // Streaming kernel for COO-dominant matrices, the direct kernel otherwise
-// (or as chosen by the plan's kernel option).
+// (or as chosen by the plan's kernel option; 3 = the staged kernel).
 // (single right-hand side; several go through the direct kernel)
 bool use_stream(const DevLayout &d) {
     if (d.max_entries > 32 * kStreamChunk) return false;
     if (d.kernel == 1) return true;
-    if (d.kernel == 2) return false;
+    if (d.kernel == 2 || d.kernel == 3) return false;
     return d.coo_share >= 0.5;
 }
 
@@ -731,7 +731,7 @@ cudaError_t launch_tiles(const DevLayout &d, const void *x, void *y, int nrhs,
                          int64_t ldx, int64_t ldy, cudaStream_t stream) {
     if (nrhs == 1 && ldx == 1 && ldy == 1 && use_stream(d))
         return launch_stream<T, BS>(d, x, y, stream);
-    if (nrhs > 1) return launch_spmm(d, x, y, nrhs, ldx, ldy, stream);
+    if (nrhs > 1 || d.kernel == 3) return launch_spmm(d, x, y, nrhs, ldx, ldy, stream);
     switch (chunk_choice(sizeof(T))) {
         case 4: return launch_chunk<T, BS, 4>(d, x, y, nrhs, ldx, ldy, stream);
         case 6: return launch_chunk<T, BS, 6>(d, x, y, nrhs, ldx, ldy, stream);

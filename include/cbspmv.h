@@ -57,9 +57,11 @@ typedef struct cbspmv_opts {
     int value_type;       /* CBSPMV_F64 (default) or CBSPMV_F32 values      */
     int want_transpose;   /* also build the CB layout of A^T for adjoints   */
     int tile_entries;     /* device tile size in stored entries (0 = auto)  */
-    int kernel;           /* SpMV kernel: 0 auto, 1 streaming (TMA-staged
-                             tiles, for COO-dominant matrices), 2 direct
-                             (high occupancy, for CSR/dense-heavy ones)     */
+    int kernel;           /* single-vector SpMV kernel: 0 auto, 1 streaming
+                             (TMA-staged tiles, for COO-dominant matrices),
+                             2 direct (high occupancy, for CSR/dense-heavy
+                             ones), 3 staged (the several-right-hand-side
+                             kernel, one vector); see cbspmv_autotune      */
 } cbspmv_opts;
 
 /* Host COO, 0-based, rows in non-decreasing order (the order the reference's
@@ -206,6 +208,16 @@ cbspmv_status cbspmv_destroy(cbspmv_plan *plan);
 /* Message of the calling thread's last error ("" if none); returns its full
  * length. */
 size_t cbspmv_last_error(char *buf, size_t len);
+
+/* Times the kernels that can run this plan for nrhs right-hand sides (one
+ * vector: streaming when the layout allows it, direct, staged; several: the
+ * staged kernel) on scratch vectors, keeps the fastest for later calls and
+ * returns it in *kernel (1, 2 or 3) with its mean time in *ms (either may be
+ * NULL).  The plan must be uploaded; allocates and frees scratch device
+ * memory and synchronizes `stream`.  No counterpart in the reference (its
+ * kernel choice is compile-time, cb-spmv-dcu.hpp:1428-1450). */
+cbspmv_status cbspmv_autotune(cbspmv_plan *plan, int nrhs, void *stream, int *kernel,
+                              double *ms);
 
 /* ---- batches (no counterpart in the reference) ------------------------ */
 

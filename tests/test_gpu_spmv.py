@@ -55,7 +55,7 @@ def _check(y, yref, absrow, f32, what):
 @pytest.mark.parametrize("bs", [16, 32])
 @pytest.mark.parametrize("f32", [False, True])
 @pytest.mark.parametrize("tile_entries", [0, 64])
-@pytest.mark.parametrize("kernel", [1, 2])
+@pytest.mark.parametrize("kernel", [1, 2, 3])
 def test_spmv_matches_oracle(cuda, name, coo, bs, f32, tile_entries, kernel):
     import torch
     import cbspmv
@@ -101,6 +101,37 @@ def test_multi_rhs(cuda, nrhs, f32, kernel):
     Y = plan.spmv(torch.from_numpy(np.ascontiguousarray(X.T)).to(cuda, dt))
     torch.cuda.synchronize()
     _check(Y.cpu().numpy().T, yref, ab, f32, f"nrhs={nrhs}")
+
+
+@pytest.mark.parametrize("name", ["pl8192", "st6", "lap64", "rand-dense"])
+@pytest.mark.parametrize("nrhs", [1, 4])
+def test_autotune_keeps_a_correct_kernel(cuda, name, nrhs):
+    """cbspmv_autotune picks one of the kernels that can run the plan and later
+    calls use it with unchanged results."""
+    import torch
+    import cbspmv
+    import cbdump as cd
+    from cbspmv import gen
+    coo = dict(CASES)[name]
+    plan = cbspmv.Plan(coo, want_transpose=1)
+    k, ms = plan.autotune(nrhs)
+    assert k in ((1, 2, 3) if nrhs == 1 else (3,)) and ms > 0
+    X = gen.uniform_x(coo.n, 31, nrhs=max(nrhs, 2))[:nrhs]
+    yref, ab = cd.oracle_spmm_ld(coo, X)
+    xd = torch.from_numpy(np.ascontiguousarray(X.T)).to(cuda)
+    if nrhs == 1:
+        xd = xd[:, 0].contiguous()
+    y = plan.spmv(xd)
+    torch.cuda.synchronize()
+    _check(y.cpu().numpy().reshape(coo.m, nrhs).T, yref, ab, False, f"autotuned {k}")
+    G = gen.uniform_x(coo.m, 32, nrhs=max(nrhs, 2))[:nrhs]
+    gref, gab = cd.oracle_spmm_ld(coo, G, transpose=True)
+    gd = torch.from_numpy(np.ascontiguousarray(G.T)).to(cuda)
+    if nrhs == 1:
+        gd = gd[:, 0].contiguous()
+    gx = plan.spmv_t(gd)
+    torch.cuda.synchronize()
+    _check(gx.cpu().numpy().reshape(coo.n, nrhs).T, gref, gab, False, f"autotuned {k} A^T")
 
 
 def test_host_entry_points(cuda):
