@@ -14,9 +14,14 @@ value       algorithmic GB/s of the whole job: the bytes of the packed CB
             step (CUDA events, max over ranks); inputs resident in HBM.
 e2e         the same metric through the C ABI with host buffers
             (cbspmv_spmv_host: pinned x copied in, y copied out every step).
-roofline    the tile kernel against the measured HBM copy bandwidth.
+roofline    the streaming kernel (the one launch of a step) against the
+            measured HBM copy bandwidth; traffic = its DRAM bytes per launch
+            from the committed ncu summary (profiles/).
 cpu_baseline  the reference's own CPU SpMV (utils.h:98-111, compiled from its
             headers into oracle/_ref) on a bounded sample, 1 thread as written.
+configs     the other workloads (LAP, PL FP32, ST FP64/FP32, DIFF forward and
+            adjoint with 8 right-hand sides, BAT 512-matrix batch), each timed
+            on the device with its roofline fraction (--configs none skips).
 --impl reference   times that CPU SpMV as the reference arm (rank 0 only).
 
 Multi-GPU: every rank runs its own copy of the workload (replicas; SpMV of
