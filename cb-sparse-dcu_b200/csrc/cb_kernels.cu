@@ -604,7 +604,9 @@ __global__ void cb_set_values_kernel(int64_t nvals, const int64_t *__restrict__ 
     *reinterpret_cast<T *>(payload + off[v]) = s;
 }
 
-template <typename T>
+// VEC right-hand sides per load (16-byte vectors) when both rows are aligned
+// to them and nrhs is a multiple of VEC; VEC = 1 otherwise.
+template <typename T, int VEC>
 __global__ void cb_grad_vals_kernel(int64_t nvals, const int32_t *__restrict__ vrow,
                                     const int32_t *__restrict__ vcol,
                                     const T *__restrict__ g, int64_t ldg,
@@ -612,11 +614,35 @@ __global__ void cb_grad_vals_kernel(int64_t nvals, const int32_t *__restrict__ v
                                     T *__restrict__ out) {
     const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= nvals) return;
-    const int32_t r = vrow[v], c = vcol[v];
+    const int32_t r = __ldg(&vrow[v]), c = __ldg(&vcol[v]);
     T s = T(0);
-    if (r >= 0 && c >= 0)
-        for (int j = 0; j < nrhs; ++j)
-            s += __ldg(&g[(int64_t)r * ldg + j]) * __ldg(&x[(int64_t)c * ldx + j]);
+    if (r >= 0 && c >= 0) {
+        const T *gr = g + (int64_t)r * ldg;
+        const T *xr = x + (int64_t)c * ldx;
+        if constexpr (VEC == 1) {
+            for (int j = 0; j < nrhs; ++j) s += __ldg(&gr[j]) * __ldg(&xr[j]);
+        } else if constexpr (sizeof(T) == 4) {
+            T s2 = T(0);
+            for (int j = 0; j < nrhs; j += 4) {
+                const float4 a = __ldg(reinterpret_cast<const float4 *>(gr + j));
+                const float4 b = __ldg(reinterpret_cast<const float4 *>(xr + j));
+                s = fma(a.x, b.x, s);
+                s2 = fma(a.y, b.y, s2);
+                s = fma(a.z, b.z, s);
+                s2 = fma(a.w, b.w, s2);
+            }
+            s += s2;
+        } else {
+            T s2 = T(0);
+            for (int j = 0; j < nrhs; j += 2) {
+                const double2 a = __ldg(reinterpret_cast<const double2 *>(gr + j));
+                const double2 b = __ldg(reinterpret_cast<const double2 *>(xr + j));
+                s = fma(a.x, b.x, s);
+                s2 = fma(a.y, b.y, s2);
+            }
+            s += s2;
+        }
+    }
     out[v] = s;
 }
 
@@ -848,14 +874,29 @@ cudaError_t launch_grad_vals(int f32, int64_t nvals, const int32_t *vrow,
                              cudaStream_t stream) {
     if (nvals == 0) return cudaSuccess;
     const unsigned grid = (unsigned)((nvals + 255) / 256);
-    if (f32)
-        cb_grad_vals_kernel<float><<<grid, 256, 0, stream>>>(
-            nvals, vrow, vcol, static_cast<const float *>(g), ldg,
-            static_cast<const float *>(x), ldx, nrhs, static_cast<float *>(gvals));
-    else
-        cb_grad_vals_kernel<double><<<grid, 256, 0, stream>>>(
-            nvals, vrow, vcol, static_cast<const double *>(g), ldg,
-            static_cast<const double *>(x), ldx, nrhs, static_cast<double *>(gvals));
+    const int vec = f32 ? 4 : 2;
+    const bool vok = nrhs % vec == 0 && ldg % vec == 0 && ldx % vec == 0 &&
+                     reinterpret_cast<uintptr_t>(g) % 16 == 0 &&
+                     reinterpret_cast<uintptr_t>(x) % 16 == 0;
+    if (f32) {
+        const float *gp = static_cast<const float *>(g), *xp = static_cast<const float *>(x);
+        float *op = static_cast<float *>(gvals);
+        if (vok)
+            cb_grad_vals_kernel<float, 4><<<grid, 256, 0, stream>>>(nvals, vrow, vcol, gp, ldg, xp,
+                                                                   ldx, nrhs, op);
+        else
+            cb_grad_vals_kernel<float, 1><<<grid, 256, 0, stream>>>(nvals, vrow, vcol, gp, ldg, xp,
+                                                                   ldx, nrhs, op);
+    } else {
+        const double *gp = static_cast<const double *>(g), *xp = static_cast<const double *>(x);
+        double *op = static_cast<double *>(gvals);
+        if (vok)
+            cb_grad_vals_kernel<double, 2><<<grid, 256, 0, stream>>>(nvals, vrow, vcol, gp, ldg,
+                                                                    xp, ldx, nrhs, op);
+        else
+            cb_grad_vals_kernel<double, 1><<<grid, 256, 0, stream>>>(nvals, vrow, vcol, gp, ldg,
+                                                                    xp, ldx, nrhs, op);
+    }
     note_launch();
     return cudaGetLastError();
 }
