@@ -13,7 +13,8 @@ value       algorithmic GB/s of the whole job: the bytes of the packed CB
             x read once and y written once, divided by the device time of a
             step (CUDA events, max over ranks); inputs resident in HBM.
 e2e         the same metric through the C ABI with host buffers
-            (cbspmv_spmv_host: pinned x copied in, y copied out every step).
+            (cbspmv_spmv_host_async: pinned x copied in, y copied out every
+            step; consecutive steps overlap copy in, kernel and copy out).
 roofline    the streaming kernel (the one launch of a step) against the
             measured HBM copy bandwidth; traffic = its DRAM bytes per launch
             from the committed ncu summary (profiles/).
@@ -166,7 +167,8 @@ def _timed(fn, reps: int, warmup: int, flush=None):
     return total / reps
 
 
-def secondary_configs(dev, peak: float) -> dict:
+def secondary_configs(dev, peak: float, want=("lap", "pl32", "st", "diff", "bat"),
+                      bat_count: int = 512) -> dict:
     """The other workloads of the benchmark suite, each timed on the device:
     LAP (5-point Laplacian 256^2, FP64), PL in FP32, ST (27-point x 3 dof
     stencil on 64^3, FP64 and FP32), DIFF (power-law n = 2^18, 8 right-hand
@@ -200,14 +202,29 @@ def secondary_configs(dev, peak: float) -> dict:
                      "l2": "flushed before each step" if small else "inputs larger than L2"}
         del plan
 
-    single("LAP fp64 (256^2 5-point)", gen.laplacian_2d(), False)
-    single("PL fp32 (n=2^20)", gen.power_law(), True)
-    st = gen.stencil_27pt()
-    single("ST fp64 (64^3 x 3 dof 27-point)", st, False, reps=20)
-    single("ST fp32 (64^3 x 3 dof 27-point)", st, True, reps=20)
-    del st
+    if "lap" in want:
+        single("LAP fp64 (256^2 5-point)", gen.laplacian_2d(), False)
+    if "pl32" in want:
+        single("PL fp32 (n=2^20)", gen.power_law(), True)
+    if "st" in want:
+        st = gen.stencil_27pt()
+        single("ST fp64 (64^3 x 3 dof 27-point)", st, False, reps=20)
+        single("ST fp32 (64^3 x 3 dof 27-point)", st, True, reps=20)
+        del st
+    if "diff" in want:
+        diff_config(dev, peak, flush, out)
+    if "bat" in want:
+        bat_config(dev, peak, bat_count, out)
+    return out
 
-    # DIFF: Y = A X, then G -> A^T G and the value gradient
+
+def diff_config(dev, peak, flush, out):
+    """DIFF: Y = A X, then G -> A^T G and the value gradient."""
+    import numpy as np
+    import torch
+    import cbspmv
+    from cbspmv import gen
+
     coo = gen.power_law(1 << 18, seed=3, mean=24)
     k = 8
     plan = cbspmv.Plan(coo, value_type=1, want_transpose=1)
@@ -231,8 +248,13 @@ def secondary_configs(dev, peak: float) -> dict:
         "gflops_fwd": round(2 * coo.nnz * k / t_f / 1e6, 1), "l2": "flushed before each step"}
     del plan
 
-    # BAT
-    items = gen.batch_uneven()
+
+def bat_config(dev, peak, count, out):
+    """BAT: `count` uneven FP32 matrices (512 is the workload)."""
+    import torch
+    import cbspmv
+    from cbspmv import gen
+    items = gen.batch_uneven(count=count)
     plans = [cbspmv.Plan(it.coo, value_type=1) for it in items]
     xs = [torch.rand(it.coo.n, it.nrhs, device=dev) for it in items]
     ys = [torch.empty(it.coo.m, it.nrhs, device=dev) for it in items]
@@ -248,9 +270,8 @@ def secondary_configs(dev, peak: float) -> dict:
     r["batched_frac"] = round(r["batched_gbs"] / peak, 4)
     r["batched_over_per_matrix"] = round(r["per_matrix_ms"] / r["batched_ms"], 2)
     r["l2"] = "inputs larger than L2"
-    out["BAT fp32 (512 matrices, 1-16 rhs)"] = r
+    out[f"BAT fp32 ({len(items)} matrices, 1-16 rhs)"] = r
     b.close()
-    return out
 
 
 def _dist():
@@ -348,8 +369,12 @@ def main():
     ap.add_argument("--impl", default="cbspmv", choices=["cbspmv", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=300)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
-    ap.add_argument("--configs", default="all", choices=["all", "none"],
-                    help="also time the other workloads (rank 0, N=1 only)")
+    ap.add_argument("--configs", default="all",
+                    help="other workloads to time (rank 0, N=1 only): all, none, or a "
+                         "comma list of lap,pl32,st,diff,bat")
+    ap.add_argument("--bat-count", type=int, default=512,
+                    help="matrices in the BAT batch (512 is the workload; fewer for "
+                         "profiling captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -413,18 +438,22 @@ def main():
     P = ctypes.c_void_p
     sptr = P(stream.cuda_stream)
     for _ in range(3):
-        lib.cbspmv_spmv_host(plan._h, P(xp.data_ptr()), P(yp.data_ptr()), 1, sptr)
+        lib.cbspmv_spmv_host_async(plan._h, P(xp.data_ptr()), P(yp.data_ptr()), 1, sptr)
     pg.barrier()
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.e2e_steps):
-        rc = lib.cbspmv_spmv_host(plan._h, P(xp.data_ptr()), P(yp.data_ptr()), 1, sptr)
+        rc = lib.cbspmv_spmv_host_async(plan._h, P(xp.data_ptr()), P(yp.data_ptr()), 1, sptr)
         if rc:
-            raise SystemExit(f"spmv_host failed: {cbspmv.last_error()}")
-    e1.record(stream)
+            raise SystemExit(f"spmv_host_async failed: {cbspmv.last_error()}")
+    e1.record(stream)  # after every step's copy out (the stream waits for each)
     torch.cuda.synchronize()
+    # the last step's y, read back through the pipeline, is the oracle's
+    err_e2e = float(np.max(np.abs(yp.numpy() - yref[0]) / (ab[0] + 1e-300)))
+    if err_e2e > 1e-12:
+        raise SystemExit(f"bench: pipelined host SpMV error {err_e2e:.3g} above 1e-12")
     ms_e2e = pg.max(e0.elapsed_time(e1) / args.e2e_steps)
     e2e_value = world * alg / (ms_e2e * 1e-3) / 1e9
 
@@ -437,8 +466,10 @@ def main():
 
     line = None
     configs = None
-    if rank == 0 and world == 1 and args.configs == "all":
-        configs = secondary_configs(dev, peak)
+    if rank == 0 and world == 1 and args.configs != "none":
+        want = {"lap", "pl32", "st", "diff", "bat"} if args.configs == "all" \
+            else set(args.configs.split(","))
+        configs = secondary_configs(dev, peak, want, args.bat_count)
     if rank == 0:
         cpu_dt, kind, reps = _ref_cpu(coo, x_host, args.cpu_seconds, 400)
         cpu = {"value": round(alg / cpu_dt / 1e9, 3), "unit": UNIT, "cores": 1, "kind": kind,

@@ -92,6 +92,7 @@ def _load():
         "cbspmv_upload": (ctypes.c_int, [_P, _P]),
         "cbspmv_spmv": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, _I64, _I64, _P]),
         "cbspmv_spmv_host": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, _P]),
+        "cbspmv_spmv_host_async": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, _P]),
         "cbspmv_spmv_t": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, _I64, _I64, _P]),
         "cbspmv_grad_vals": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int, _I64,
                                             _I64, _P]),

@@ -82,6 +82,33 @@ struct DevSide {
 
 }  // namespace
 
+// Pipelined host-buffer calls (cbspmv_spmv_host_async): copy in, compute and
+// copy out on three streams of their own, two sets of device buffers, so call
+// i+1's copy in overlaps call i's kernel and call i-1's copy out.
+struct HostPipe {
+    cudaStream_t in = nullptr, comp = nullptr, out = nullptr;
+    void *x[2] = {}, *y[2] = {};
+    size_t xb = 0, yb = 0;  // bytes of each buffer
+    // x_ready: copy in done; x_free: kernel done reading x; y_ready: kernel
+    // done writing y; y_free: copy out done
+    cudaEvent_t x_ready[2] = {}, x_free[2] = {}, y_ready[2] = {}, y_free[2] = {};
+    bool used[2] = {false, false};
+    int64_t calls = 0;
+    void release() {
+        for (int b = 0; b < 2; ++b) {
+            if (x[b]) cudaFree(x[b]);
+            if (y[b]) cudaFree(y[b]);
+            x[b] = y[b] = nullptr;
+            for (cudaEvent_t *e : {&x_ready[b], &x_free[b], &y_ready[b], &y_free[b]})
+                if (*e) cudaEventDestroy(*e), *e = nullptr;
+            used[b] = false;
+        }
+        for (cudaStream_t *st : {&in, &comp, &out})
+            if (*st) cudaStreamDestroy(*st), *st = nullptr;
+        xb = yb = 0;
+    }
+};
+
 struct cbspmv_plan {
     cbspmv_opts opts;
     cb::HostCB host, host_t;
@@ -92,7 +119,10 @@ struct cbspmv_plan {
     // staging for the host-buffer entry points
     void *hx = nullptr, *hy = nullptr;
     size_t hx_bytes = 0, hy_bytes = 0;
+    HostPipe pipe;
     ~cbspmv_plan() {
+        if (pipe.comp) cudaStreamSynchronize(pipe.out ? pipe.out : pipe.comp);
+        pipe.release();
         A.release();
         AT.release();
         if (hx) cudaFree(hx);
@@ -464,6 +494,57 @@ cbspmv_status cbspmv_spmv_host(cbspmv_plan *p, const void *x_host, void *y_host,
     if (rc) return rc;
     if (yb) CB_CUDA(cudaMemcpyAsync(y_host, p->hy, yb, cudaMemcpyDeviceToHost, st), "copy y");
     CB_CUDA(cudaStreamSynchronize(st), "spmv_host");
+    return CBSPMV_OK;
+}
+
+cbspmv_status cbspmv_spmv_host_async(cbspmv_plan *p, const void *x_host, void *y_host,
+                                     int nrhs, void *stream) {
+    if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
+    if (nrhs < 1) return fail(CBSPMV_ERR_INVALID, "nrhs must be >= 1");
+    cbspmv_status rc = cbspmv_upload(p, stream);
+    if (rc) return rc;
+    HostPipe &q = p->pipe;
+    const cudaStream_t user = static_cast<cudaStream_t>(stream);
+    const size_t xb = (size_t)p->host.n * nrhs * vsize(p);
+    const size_t yb = (size_t)p->host.m * nrhs * vsize(p);
+    if (!q.comp || xb > q.xb || yb > q.yb) {  // set up, or grow for more rhs
+        if (q.comp) {
+            CB_CUDA(cudaStreamSynchronize(q.out), "drain host pipeline");
+            CB_CUDA(cudaStreamSynchronize(q.comp), "drain host pipeline");
+        }
+        q.release();
+        for (cudaStream_t *st : {&q.in, &q.comp, &q.out})
+            CB_CUDA(cudaStreamCreateWithFlags(st, cudaStreamNonBlocking), "create stream");
+        for (int b = 0; b < 2; ++b) {
+            CB_CUDA(cudaMalloc(&q.x[b], std::max<size_t>(16, xb)), "allocate x");
+            CB_CUDA(cudaMalloc(&q.y[b], std::max<size_t>(16, yb)), "allocate y");
+            for (cudaEvent_t *e : {&q.x_ready[b], &q.x_free[b], &q.y_ready[b], &q.y_free[b]})
+                CB_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming), "create event");
+        }
+        q.xb = std::max<size_t>(16, xb);
+        q.yb = std::max<size_t>(16, yb);
+    }
+    const int b = (int)(q.calls & 1);
+    // copy in (x_host holds the input now), after the kernel that last read
+    // this buffer; not after the caller's stream, which waits for earlier
+    // calls' copies out
+    if (q.used[b]) CB_CUDA(cudaStreamWaitEvent(q.in, q.x_free[b], 0), "wait");
+    if (xb) CB_CUDA(cudaMemcpyAsync(q.x[b], x_host, xb, cudaMemcpyHostToDevice, q.in), "copy x");
+    CB_CUDA(cudaEventRecord(q.x_ready[b], q.in), "record");
+    // compute, once x is in and the previous copy out of this y is done
+    CB_CUDA(cudaStreamWaitEvent(q.comp, q.x_ready[b], 0), "wait");
+    if (q.used[b]) CB_CUDA(cudaStreamWaitEvent(q.comp, q.y_free[b], 0), "wait");
+    rc = run_side(p, p->A, q.x[b], q.y[b], nrhs, nrhs, nrhs, q.comp);
+    if (rc) return rc;
+    CB_CUDA(cudaEventRecord(q.x_free[b], q.comp), "record");
+    CB_CUDA(cudaEventRecord(q.y_ready[b], q.comp), "record");
+    // copy out; the caller's stream waits for it
+    CB_CUDA(cudaStreamWaitEvent(q.out, q.y_ready[b], 0), "wait");
+    if (yb) CB_CUDA(cudaMemcpyAsync(y_host, q.y[b], yb, cudaMemcpyDeviceToHost, q.out), "copy y");
+    CB_CUDA(cudaEventRecord(q.y_free[b], q.out), "record");
+    CB_CUDA(cudaStreamWaitEvent(user, q.y_free[b], 0), "wait");
+    q.used[b] = true;
+    ++q.calls;
     return CBSPMV_OK;
 }
 

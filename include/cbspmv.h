@@ -153,6 +153,19 @@ cbspmv_status cbspmv_spmv_noalloc(cbspmv_plan *plan, const void *x, void *y,
 cbspmv_status cbspmv_spmv_host(cbspmv_plan *plan, const void *x_host,
                                void *y_host, int nrhs, void *stream);
 
+/* cbspmv_spmv_host without the wait, for a stream of solves: copies x in,
+ * runs and copies y out on three streams the plan keeps (two sets of device
+ * buffers), so one call's copy in overlaps the previous call's kernel and the
+ * one before's copy out, and returns at once.  x_host must hold the input
+ * when the call is made (the copy in does not wait for `stream`).  `stream`
+ * waits for this call's copy out; synchronize it before reading y_host, and
+ * keep x_host unchanged and both buffers alive until then (pinned host memory
+ * lets the copies run asynchronously).  The first call, and a call with more right-hand sides
+ * than before, allocates the device buffers.  No counterpart in the
+ * reference (its cb_spmv copies, runs and copies back one call at a time). */
+cbspmv_status cbspmv_spmv_host_async(cbspmv_plan *plan, const void *x_host,
+                                     void *y_host, int nrhs, void *stream);
+
 /* Adjoint: gx = A^T g (g: m rows, gx: n rows, same conventions).  Needs the
  * plan built with want_transpose. */
 cbspmv_status cbspmv_spmv_t(cbspmv_plan *plan, const void *g, void *gx,

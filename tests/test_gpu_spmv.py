@@ -150,6 +150,45 @@ def test_host_entry_points(cuda):
     _check(y2, yref[0], ab[0], False, "spmv_host")
 
 
+@pytest.mark.parametrize("nrhs", [1, 3])
+def test_host_async_pipeline(cuda, nrhs):
+    """cbspmv_spmv_host_async: several calls in flight on pinned host buffers,
+    each result equal to the oracle's once the caller's stream is synced; a
+    call with more right-hand sides regrows the pipeline."""
+    import ctypes
+    import torch
+    import cbspmv
+    import cbdump as cd
+    from cbspmv import gen
+    coo = gen.power_law(20000, kmax=5000, band=600, seed=9)
+    plan = cbspmv.Plan(coo).upload()
+    lib = cbspmv.lib()
+    stream = torch.cuda.current_stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    calls = []
+    for i in range(5):
+        X = gen.uniform_x(coo.n, 40 + i, nrhs=max(nrhs, 2))[:nrhs]
+        xh = torch.from_numpy(np.ascontiguousarray(X.T)).pin_memory()
+        yh = torch.full((coo.m, nrhs), float("nan"), dtype=torch.float64).pin_memory()
+        rc = lib.cbspmv_spmv_host_async(plan._h, ctypes.c_void_p(xh.data_ptr()),
+                                        ctypes.c_void_p(yh.data_ptr()), nrhs, sp)
+        assert rc == 0, cbspmv.last_error()
+        calls.append((X, xh, yh))
+    stream.synchronize()
+    for i, (X, _, yh) in enumerate(calls):
+        yref, ab = cd.oracle_spmm_ld(coo, X)
+        _check(yh.numpy().T, yref, ab, False, f"async call {i}")
+    # more right-hand sides than before: the buffers grow
+    X = gen.uniform_x(coo.n, 60, nrhs=nrhs + 2)
+    xh = torch.from_numpy(np.ascontiguousarray(X.T)).pin_memory()
+    yh = torch.zeros((coo.m, nrhs + 2), dtype=torch.float64).pin_memory()
+    assert lib.cbspmv_spmv_host_async(plan._h, ctypes.c_void_p(xh.data_ptr()),
+                                      ctypes.c_void_p(yh.data_ptr()), nrhs + 2, sp) == 0
+    stream.synchronize()
+    yref, ab = cd.oracle_spmm_ld(coo, X)
+    _check(yh.numpy().T, yref, ab, False, "async regrown")
+
+
 def test_empty_and_degenerate(cuda):
     import torch
     import cbspmv
