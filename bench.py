@@ -464,6 +464,30 @@ def main():
             "traffic": _ncu_traffic(),
             "kernel": "cb_spmv_stream_kernel (the one launch of each SpMV)"}
 
+    # library comparator: cuSPARSE CSR SpMV (through torch) on the same matrix
+    comparator = None
+    if rank == 0:
+        try:
+            import warnings
+            crow = np.zeros(coo.m + 1, np.int64)
+            np.add.at(crow, coo.row.astype(np.int64) + 1, 1)
+            with warnings.catch_warnings():
+                warnings.simplefilter("ignore")
+                A = torch.sparse_csr_tensor(
+                    torch.from_numpy(np.cumsum(crow).astype(np.int32)).to(dev),
+                    torch.from_numpy(coo.col.astype(np.int32)).to(dev),
+                    torch.from_numpy(coo.val).to(dev), (coo.m, coo.n))
+            xs = x.view(-1, 1)
+            ms_cs = _timed(lambda: torch.sparse.mm(A, xs), 200, 10)
+            csr_bytes = coo.nnz * (4 + 8) + (coo.m + 1) * 4 + (coo.n + coo.m) * 8
+            comparator = {"library": "cuSPARSE CSR SpMV via torch.sparse.mm (FP64, int32 indices)",
+                          "ms": round(ms_cs, 4), "csr_bytes": csr_bytes,
+                          "csr_gbs": round(csr_bytes / ms_cs / 1e6, 1),
+                          "this_library_speedup": round(ms_cs / ms, 2)}
+            del A
+        except Exception as exc:  # the comparator is informative only
+            comparator = {"unavailable": str(exc)[:200]}
+
     line = None
     configs = None
     if rank == 0 and world == 1 and args.configs != "none":
@@ -494,6 +518,7 @@ def main():
             "roofline": roof,
             "cpu_baseline": cpu,
             "gpu_launches": launches,
+            "comparator": comparator,
             "clocks": clk.summary(),
         }
         if configs is not None:

@@ -56,6 +56,7 @@ struct DevSide {
     void *partials = nullptr;
     int32_t *counters = nullptr;
     uint32_t *wpart = nullptr;
+    uint32_t *dunit = nullptr;
     int64_t *ustart = nullptr;
     int partial_nrhs = 0;
     int64_t *vsrc_ptr = nullptr;
@@ -65,13 +66,14 @@ struct DevSide {
 
     void release() {
         void *ps[] = {tiles, blocks, payload, block_cols, partials, counters,
-                      wpart, ustart, vsrc_ptr, vsrc, val_off, val_row, val_col};
+                      wpart, dunit, ustart, vsrc_ptr, vsrc, val_off, val_row, val_col};
         for (void *p : ps)
             if (p) cudaFree(p);
         tiles = blocks = partials = nullptr;
         payload = nullptr;
         block_cols = counters = vsrc = val_row = val_col = nullptr;
         wpart = nullptr;
+        dunit = nullptr;
         ustart = nullptr;
         vsrc_ptr = nullptr;
         val_off = nullptr;
@@ -185,9 +187,16 @@ cbspmv_status upload_partition(DevSide &s, int kernel, cudaStream_t st) {
         s.d.wpart = s.wpart;
         s.d.nwarps = warps;
     }
+    const int64_t nt = (int64_t)s.lay.tiles.size();
+    if (nt > 0) {  // the direct kernel's block-row units
+        const std::vector<uint32_t> du =
+            cb::direct_units(reinterpret_cast<const uint32_t *>(s.lay.tiles.data()), nt);
+        CB_CUDA(upload_vec(du, &s.dunit, st), "upload direct units");
+        s.d.dunit = s.dunit;
+        s.d.ndunits = (int64_t)du.size() - 1;
+    }
     // several right-hand sides: tile buffer size and scheduling units
     s.d.mcap = cb::ms_cap(s.lay.max_tile_bytes);
-    const int64_t nt = (int64_t)s.lay.tiles.size();
     if (nt > 0) {  // one cost-balanced range of tiles per resident warp
         const int64_t warps = std::min<int64_t>(nt, cb::ms_warps(s.lay.bs, s.lay.f32, s.d.mcap));
         if (warps <= 0) return fail(CBSPMV_ERR_CUDA, "multi-right-hand-side kernel setup");

@@ -27,6 +27,7 @@
 #include <cstdlib>
 #include <mutex>
 #include <type_traits>
+#include <vector>
 
 #include "cb_device.cuh"
 #include "cb_kernels.hpp"
@@ -89,22 +90,25 @@ __device__ __forceinline__ T reduce_rows(T *acc, int lane) {
     return s;
 }
 
-// Persistent warps fetch tiles from a global counter (sched[0]); the warp
+// One vector (x column stride ldx, y stride ldy).  Persistent warps take
+// units from a global counter (sched[0]): unit u is tiles [ustart[u],
+// ustart[u+1]) of one block row -- the whole row, or pieces of `unit_tiles`
+// tiles starting at its first tile -- and add all of the unit's tiles into
+// their lane-private accumulators before one reduction and store, so a row's
+// tiles need no partial sums unless the row is longer than a unit.  The warp
 // whose exit completes sched[1] == number of warps resets both for the next
-// launch, so no launch waits on another and no host reset is needed.
-// kChunk COO entries per lane have their loads in flight together; nrhs
-// right-hand sides are handled one after another (x column j at
-// x[col * ldx + j]).
+// launch, so no launch waits on another and no host reset is needed.  kChunk
+// COO entries per lane have their loads in flight together.
 template <typename T, int BS, int kChunk>
 __global__ void __launch_bounds__(kWarps * 32, 4)
-    cb_spmv_tile_kernel(const uint4 *__restrict__ tiles, int64_t ntiles,
-                        const uint4 *__restrict__ blocks,
+    cb_spmv_tile_kernel(const uint4 *__restrict__ tiles, const uint4 *__restrict__ blocks,
                         const uint8_t *__restrict__ payload,
                         const int32_t *__restrict__ block_cols, int gather,
                         const T *__restrict__ x, T *__restrict__ y, int64_t m,
-                        int nrhs, int64_t ldx, int64_t ldy,
-                        T *__restrict__ partials, int32_t *__restrict__ counters,
-                        uint32_t *__restrict__ sched) {
+                        int64_t ldx, int64_t ldy, T *__restrict__ partials,
+                        int32_t *__restrict__ counters, uint32_t *__restrict__ sched,
+                        const uint32_t *__restrict__ ustart, int64_t nunits,
+                        int unit_tiles) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -118,35 +122,29 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
         if (lane == 0) t = atomicAdd(&sched[0], 1u);
         return (int64_t)__shfl_sync(kFull, t, 0);
     };
-    int64_t tile = grab();
-    uint4 na = make_uint4(0, 0, 0, 0), nb4 = na;
-    if (tile < ntiles) {
-        na = __ldg(&tiles[2 * tile]);
-        nb4 = __ldg(&tiles[2 * tile + 1]);
-    }
-    while (tile < ntiles) {
-        const uint4 ta = na;   // begin, row, counts, pay16
-        const uint4 tb = nb4;  // E, slot, first, ntiles
+    int64_t unit = grab();
+    while (unit < nunits) {
         const int64_t next = grab();
-        if (next < ntiles) {
-            na = __ldg(&tiles[2 * next]);
-            nb4 = __ldg(&tiles[2 * next + 1]);
-        }
-        const int ncoo = (ta.z >> 8) & 0xff;
-        const int nxt = (ta.z >> 16) & 0xff;
-        const int E = (int)tb.x;
-        const uint8_t *base = payload + (size_t)ta.w * 16;
-        uint4 bd = make_uint4(0, 0, 0, 0);  // lane j: CSR/DENSE block j of the tile
-        if (lane < nxt) bd = __ldg(&blocks[ta.x + ncoo + lane]);
-        const uint32_t *cidx = reinterpret_cast<const uint32_t *>(base);
-        const T *cval = reinterpret_cast<const T *>(base + a16(4u * E));
-        const int64_t row0 = (int64_t)ta.y * BS;
+        const int64_t t0 = __ldg(&ustart[unit]), t1 = __ldg(&ustart[unit + 1]);
+        uint4 ta = __ldg(&tiles[2 * t0]), tb = __ldg(&tiles[2 * t0 + 1]);
+        for (int64_t tile = t0; tile < t1; ++tile) {
+            uint4 na = ta, nb4 = tb;  // the next tile's descriptors, in flight
+            if (tile + 1 < t1) {
+                na = __ldg(&tiles[2 * tile + 2]);
+                nb4 = __ldg(&tiles[2 * tile + 3]);
+            }
+            const int ncoo = (ta.z >> 8) & 0xff;
+            const int nxt = (ta.z >> 16) & 0xff;
+            const int E = (int)tb.x;
+            const uint8_t *base = payload + (size_t)ta.w * 16;
+            uint4 bd = make_uint4(0, 0, 0, 0);  // lane j: CSR/DENSE block j of the tile
+            if (lane < nxt) bd = __ldg(&blocks[ta.x + ncoo + lane]);
+            const uint32_t *cidx = reinterpret_cast<const uint32_t *>(base);
+            const T *cval = reinterpret_cast<const T *>(base + a16(4u * E));
 
-        for (int j = 0; j < nrhs; ++j) {
-            const T *xj = x + j;
             // x tiles of CSR/DENSE blocks (through the gather list if any)
-            for (int t0 = 0; t0 < nxt * BS; t0 += 32) {
-                const int t = t0 + lane;
+            for (int c0 = 0; c0 < nxt * BS; c0 += 32) {
+                const int t = c0 + lane;
                 const int jb = min(t / BS, nxt - 1);
                 const uint32_t xb = __shfl_sync(kFull, bd.z, jb);
                 const uint32_t mb = __shfl_sync(kFull, bd.y, jb);
@@ -157,7 +155,7 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
                     if (c < valid) {
                         const int64_t col = gather ? (int64_t)__ldg(&block_cols[xb + c])
                                                    : (int64_t)(xb + c);
-                        xv = ldg(&xj[col * ldx]);
+                        xv = ldg(&x[col * ldx]);
                     }
                     S.xt[t] = xv;
                 }
@@ -183,7 +181,7 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
 #pragma unroll
                 for (int u = 0; u < kChunk; ++u) {
                     const int e = c0 + u * 32 + lane;
-                    xv[u] = e < E ? ldg(&xj[(int64_t)(w[u] & kColMask) * ldx]) : T(0);
+                    xv[u] = e < E ? ldg(&x[(int64_t)(w[u] & kColMask) * ldx]) : T(0);
                 }
 #pragma unroll
                 for (int u = 0; u < kChunk; ++u) {
@@ -229,41 +227,47 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
                     }
                 }
             }
-            __syncwarp();
-            const T s = reduce_rows<T, BS>(S.acc, lane);
-            __syncwarp();
-
-            // output: whole block row -> y; split row -> partial slot, and the
-            // last tile to arrive adds the row's partials in tile order
-            const int64_t grow = row0 + lane;
-            if (tb.y == 0xffffffffu) {
-                if (lane < BS && grow < m) y[grow * ldy + j] = s;
-            } else {
-                T *part = partials + ((size_t)tb.y * nrhs + j) * BS;
-                if (lane < BS) part[lane] = s;
-                __threadfence();
-                __syncwarp();
-                int last = 0;
-                if (lane == 0) {
-                    const int old = atomicAdd(&counters[ta.y], 1);
-                    last = old == (int)(tb.w * nrhs) - 1;
-                }
-                last = __shfl_sync(kFull, last, 0);
-                if (last) {
-                    __threadfence();
-                    if (lane < BS) {
-                        for (int jj = 0; jj < nrhs; ++jj) {
-                            T tot = T(0);
-                            for (uint32_t t = 0; t < tb.w; ++t)
-                                tot += __ldcg(&partials[((size_t)(tb.z + t) * nrhs + jj) * BS + lane]);
-                            if (grow < m) y[grow * ldy + jj] = tot;
-                        }
-                    }
-                    if (lane == 0) atomicExch(&counters[ta.y], 0);
-                }
+            __syncwarp();  // xt is rewritten by the next tile
+            if (tile + 1 < t1) {
+                ta = na;
+                tb = nb4;
             }
         }
-        tile = next;
+        const T s = reduce_rows<T, BS>(S.acc, lane);
+        __syncwarp();
+
+        // output: the unit holds the whole block row -> y; else the unit's
+        // sums go to the slot of its first tile, and the last unit to arrive
+        // adds the row's units (starting at its first tile, then every
+        // unit_tiles tiles) in order
+        const int64_t row0 = (int64_t)ta.y * BS;
+        const int64_t grow = row0 + lane;
+        const int64_t ntl = t1 - t0;
+        if (tb.y == 0xffffffffu || ntl == (int64_t)tb.w) {
+            if (lane < BS && grow < m) y[grow * ldy] = s;
+        } else {
+            const int64_t first = t1 - 1 - (int64_t)(tb.y - tb.z);
+            if (lane < BS) partials[(size_t)(tb.z + (t0 - first)) * BS + lane] = s;
+            __threadfence();
+            __syncwarp();
+            int last = 0;
+            if (lane == 0) {
+                const int old = atomicAdd(&counters[ta.y], (int)ntl);
+                last = old + (int)ntl == (int)tb.w;
+            }
+            last = __shfl_sync(kFull, last, 0);
+            if (last) {
+                __threadfence();
+                if (lane < BS) {
+                    T tot = T(0);
+                    for (uint32_t t = 0; t < tb.w; t += (uint32_t)unit_tiles)
+                        tot += __ldcg(&partials[(size_t)(tb.z + t) * BS + lane]);
+                    if (grow < m) y[grow * ldy] = tot;
+                }
+                if (lane == 0) atomicExch(&counters[ta.y], 0);
+            }
+        }
+        unit = next;
     }
     // this warp has made its last (failing) grab: count it out; the last warp
     // out resets the scheduler for the next launch
@@ -664,14 +668,14 @@ cudaError_t launch_chunk(const DevLayout &d, const void *x, void *y, int nrhs,
                                                       kWarps * 32, smem);
         if (resident < 1) resident = 1;
     }
-    int64_t grid = (d.ntiles + kWarps - 1) / kWarps;
+    if (nrhs != 1 || !d.dunit) return cudaErrorInvalidValue;
+    int64_t grid = (d.ndunits + kWarps - 1) / kWarps;
     grid = std::min<int64_t>(grid, (int64_t)sms * resident);
     if (grid == 0) return cudaSuccess;
     cb_spmv_tile_kernel<T, BS, CH><<<(unsigned)grid, kWarps * 32, smem, stream>>>(
-        static_cast<const uint4 *>(d.tiles), d.ntiles,
-        static_cast<const uint4 *>(d.blocks), d.payload, d.block_cols, d.gather,
-        static_cast<const T *>(x), static_cast<T *>(y), d.m, nrhs, ldx, ldy,
-        static_cast<T *>(d.partials), d.counters, d.sched);
+        static_cast<const uint4 *>(d.tiles), static_cast<const uint4 *>(d.blocks), d.payload,
+        d.block_cols, d.gather, static_cast<const T *>(x), static_cast<T *>(y), d.m, ldx, ldy,
+        static_cast<T *>(d.partials), d.counters, d.sched, d.dunit, d.ndunits, kDirectUnitTiles);
     note_launch();
     return cudaGetLastError();
 }
@@ -766,6 +770,19 @@ cudaError_t launch_tiles(const DevLayout &d, const void *x, void *y, int nrhs,
 }
 
 }  // namespace
+
+std::vector<uint32_t> direct_units(const uint32_t *tile8, int64_t ntiles) {
+    std::vector<uint32_t> us;
+    int64_t row_start = 0;
+    for (int64_t t = 0; t < ntiles; ++t) {
+        const uint32_t *d = tile8 + 8 * t;
+        const bool first = d[5] == 0xffffffffu || d[5] == d[6];  // slot == first slot
+        if (first) row_start = t;
+        if ((t - row_start) % kDirectUnitTiles == 0) us.push_back((uint32_t)t);
+    }
+    us.push_back((uint32_t)ntiles);
+    return us;
+}
 
 int64_t kernel_launches() { return g_kernel_launches.load(); }
 void note_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }

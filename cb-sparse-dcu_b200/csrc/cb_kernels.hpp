@@ -26,6 +26,9 @@ struct DevLayout {
     const uint32_t *wpart = nullptr;  // streaming: per-warp tile ranges
     int64_t nwarps = 0;               // streaming: warps of the launch
     uint32_t pay16_end = 0;           // payload size in 16-byte units
+    // direct kernel: units of one block row (kDirectUnitTiles tiles at most)
+    const uint32_t *dunit = nullptr;  // ndunits + 1 tile indices
+    int64_t ndunits = 0;
     // several right-hand sides: tile buffer bytes, scheduling units
     uint32_t mcap = 0;
     const int64_t *ustart = nullptr;  // nunits + 1 tile indices
@@ -84,6 +87,12 @@ cudaError_t launch_spmm(const DevLayout &d, const void *x, void *y, int nrhs, in
 cudaError_t launch_batch(int bs, int f32, MsClass c, const MatView *mats, int nmats,
                          const int64_t *toff, const int64_t *ustart, int64_t nunits,
                          uint32_t cap, uint32_t *sched, cudaStream_t stream);
+
+// The direct kernel's scheduling units: each block row's tiles in pieces of
+// at most kDirectUnitTiles, starting at the row's first tile; direct_units
+// returns the unit starts followed by the tile count.
+constexpr int kDirectUnitTiles = 16;
+std::vector<uint32_t> direct_units(const uint32_t *tile8, int64_t ntiles);
 
 // Warps of a streaming-kernel launch for this layout on the current device,
 // or 0 when the direct kernel is the one that runs.
