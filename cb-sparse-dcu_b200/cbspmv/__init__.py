@@ -90,6 +90,9 @@ def _load():
                                                    ctypes.POINTER(_P)]),
         "cbspmv_cb_spmv": (ctypes.c_int, [_P, _P, _P, ctypes.POINTER(Metrics)]),
         "cbspmv_upload": (ctypes.c_int, [_P, _P]),
+        "cbspmv_plan_save": (ctypes.c_int, [_P, ctypes.c_char_p]),
+        "cbspmv_plan_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_P)]),
+        "cbspmv_plan_opts": (ctypes.c_int, [_P, ctypes.POINTER(Opts)]),
         "cbspmv_spmv": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, _I64, _I64, _P]),
         "cbspmv_spmv_host": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, _P]),
         "cbspmv_spmv_host_async": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, _P]),
@@ -216,6 +219,29 @@ class Plan:
         self.bs = self.opts.block_size
         self.has_transpose = bool(self.opts.want_transpose)
         self._uploaded = False
+
+    # ---- plan files
+    def save(self, path) -> None:
+        """Writes the built plan to a .cbplan file (cbspmv_plan_save)."""
+        _check(_lib.cbspmv_plan_save(self._h, str(path).encode()))
+
+    @classmethod
+    def load(cls, path) -> "Plan":
+        """A plan read from a .cbplan file, without the COO input or the CB
+        build (cbspmv_plan_load)."""
+        h = ctypes.c_void_p()
+        _check(_lib.cbspmv_plan_load(str(path).encode(), ctypes.byref(h)))
+        self = cls.__new__(cls)
+        self._h = h
+        self.opts = Opts()
+        _check(_lib.cbspmv_plan_opts(h, ctypes.byref(self.opts)))
+        i = self.info()
+        self.m, self.n, self.nnz = int(i["m"]), int(i["n"]), int(i["nnz"])
+        self.f32 = self.opts.value_type == F32
+        self.bs = self.opts.block_size
+        self.has_transpose = bool(self.opts.want_transpose)
+        self._uploaded = False
+        return self
 
     # ---- lifetime
     def close(self):

@@ -15,6 +15,7 @@
 #include "cb_builder.hpp"
 #include "cb_kernels.hpp"
 #include "cb_layout.hpp"
+#include "cb_planfile.hpp"
 #include "cbspmv.h"
 
 namespace {
@@ -341,6 +342,72 @@ cbspmv_status cbspmv_coo2block_gather(const cbspmv_coo *coo,
     } catch (const std::bad_alloc &) {
         delete p;
         return fail(CBSPMV_ERR_ALLOC, "out of host memory while building");
+    }
+    *out = p;
+    return CBSPMV_OK;
+}
+
+cbspmv_status cbspmv_plan_save(const cbspmv_plan *p, const char *path) {
+    if (!p || !path) return fail(CBSPMV_ERR_INVALID, "null argument");
+    cb::PlanImage img;
+    const cbspmv_opts &o = p->opts;
+    const int32_t opts9[9] = {o.block_size,  o.row_owned,      o.waves_per_block,
+                              o.dense_sixteenths, o.force_coo64, o.value_type,
+                              o.want_transpose,   o.tile_entries, o.kernel};
+    std::memcpy(img.opts9, opts9, sizeof opts9);
+    img.has_t = p->has_t ? 1 : 0;
+    auto *q = const_cast<cbspmv_plan *>(p);  // visited, not modified, by the writer
+    img.host = &q->host;
+    img.host_t = &q->host_t;
+    img.A = &q->A.lay;
+    img.AT = &q->AT.lay;
+    const std::string err = cb::save_plan(img, path);
+    if (!err.empty()) return fail(CBSPMV_ERR_INVALID, err);
+    return CBSPMV_OK;
+}
+
+cbspmv_status cbspmv_plan_opts(const cbspmv_plan *p, cbspmv_opts *opts) {
+    if (!p || !opts) return fail(CBSPMV_ERR_INVALID, "null argument");
+    *opts = p->opts;
+    return CBSPMV_OK;
+}
+
+cbspmv_status cbspmv_plan_load(const char *path, cbspmv_plan **out) {
+    if (!path || !out) return fail(CBSPMV_ERR_INVALID, "null argument");
+    *out = nullptr;
+    cbspmv_plan *p = new (std::nothrow) cbspmv_plan;
+    if (!p) return fail(CBSPMV_ERR_ALLOC, "out of host memory");
+    cb::PlanImage img;
+    img.host = &p->host;
+    img.host_t = &p->host_t;
+    img.A = &p->A.lay;
+    img.AT = &p->AT.lay;
+    std::string err;
+    try {
+        err = cb::load_plan(path, img);
+    } catch (const std::bad_alloc &) {
+        err = "out of host memory while loading";
+    }
+    if (!err.empty()) {
+        delete p;
+        return fail(CBSPMV_ERR_INVALID, err);
+    }
+    cbspmv_opts &o = p->opts;
+    o.block_size = img.opts9[0];
+    o.row_owned = img.opts9[1];
+    o.waves_per_block = img.opts9[2];
+    o.dense_sixteenths = img.opts9[3];
+    o.force_coo64 = img.opts9[4];
+    o.value_type = img.opts9[5];
+    o.want_transpose = img.opts9[6];
+    o.tile_entries = img.opts9[7];
+    o.kernel = img.opts9[8];
+    p->has_t = img.has_t != 0;
+    if ((o.block_size != 16 && o.block_size != 32) ||
+        (o.value_type != CBSPMV_F64 && o.value_type != CBSPMV_F32) || o.kernel < 0 ||
+        o.kernel > 3 || p->A.lay.bs != o.block_size) {
+        delete p;
+        return fail(CBSPMV_ERR_INVALID, std::string(path) + " holds inconsistent options");
     }
     *out = p;
     return CBSPMV_OK;

@@ -1,0 +1,29 @@
+// Versioned binary plan files (.cbplan): a built plan's host CB structures
+// and device layouts, so a later process skips the CB build.  Host data only;
+// a loaded plan is uploaded like a freshly built one.
+#pragma once
+
+#include <cstdint>
+#include <string>
+
+#include "cb_builder.hpp"
+#include "cb_layout.hpp"
+
+namespace cb {
+
+// Everything a plan keeps on the host.  opts9: the nine int fields of
+// cbspmv_opts in declaration order.
+struct PlanImage {
+    int32_t opts9[9] = {};
+    int32_t has_t = 0;
+    HostCB *host = nullptr, *host_t = nullptr;
+    DeviceLayout *A = nullptr, *AT = nullptr;
+};
+
+// Return "" or an error message.
+std::string save_plan(const PlanImage &img, const std::string &path);
+std::string load_plan(const std::string &path, PlanImage &img);
+
+constexpr uint32_t kPlanFileVersion = 1;
+
+}  // namespace cb

@@ -118,6 +118,20 @@ cbspmv_status cbspmv_cb_spmv(cbspmv_plan *plan, const double *x, double *y,
 
 void cbspmv_default_opts(cbspmv_opts *opts);
 
+/* Plan files (.cbplan, versioned binary): save writes a built plan's host
+ * CB structures and device layouts (and the kernel chosen by
+ * cbspmv_autotune); load recreates the plan without the COO input or the CB
+ * build -- the reference rebuilds its structure on every run
+ * (main.hip.cpp:67-68).  A loaded plan is not uploaded yet.  A file of
+ * another format version, another byte order, or one that is truncated or
+ * fails its checksum is refused with CBSPMV_ERR_INVALID. */
+cbspmv_status cbspmv_plan_save(const cbspmv_plan *plan, const char *path);
+cbspmv_status cbspmv_plan_load(const char *path, cbspmv_plan **out);
+
+/* The options a plan was built (or loaded) with; `kernel` reflects
+ * cbspmv_autotune. */
+cbspmv_status cbspmv_plan_opts(const cbspmv_plan *plan, cbspmv_opts *opts);
+
 /* Copies the packed device layout to the current CUDA device. */
 cbspmv_status cbspmv_upload(cbspmv_plan *plan, void *stream);
 

@@ -189,6 +189,25 @@ def test_host_async_pipeline(cuda, nrhs):
     _check(yh.numpy().T, yref, ab, False, "async regrown")
 
 
+def test_loaded_plan_gives_the_same_y(cuda, tmp_path):
+    """A plan saved after autotuning and loaded back runs the same kernel on
+    the same layout: bit-identical y."""
+    import torch
+    import cbspmv
+    from cbspmv import gen
+    for coo in (dict(CASES)["pl8192"], dict(CASES)["st6"]):
+        p = cbspmv.Plan(coo)
+        p.autotune(1)
+        path = tmp_path / "p.cbplan"
+        p.save(path)
+        q = cbspmv.Plan.load(path)
+        assert q.opts.kernel == p.opts.kernel
+        x = torch.from_numpy(gen.uniform_x(coo.n, 8)).to(cuda)
+        y1, y2 = p.spmv(x), q.spmv(x)
+        torch.cuda.synchronize()
+        assert torch.equal(y1, y2)
+
+
 def test_empty_and_degenerate(cuda):
     import torch
     import cbspmv
