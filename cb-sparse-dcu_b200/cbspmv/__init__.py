@@ -39,7 +39,8 @@ class Opts(ctypes.Structure):
                 ("dense_sixteenths", ctypes.c_int),
                 ("force_coo64", ctypes.c_int), ("value_type", ctypes.c_int),
                 ("want_transpose", ctypes.c_int),
-                ("tile_entries", ctypes.c_int), ("kernel", ctypes.c_int)]
+                ("tile_entries", ctypes.c_int), ("kernel", ctypes.c_int),
+                ("keep_values", ctypes.c_int)]
 
 
 class CooDesc(ctypes.Structure):

@@ -9,6 +9,9 @@ caller's COO order) and X is (n,) or (n, k).  Backward:
   per stored value slot (``grad_vals``) and gathered back to input order
   through ``input_slots`` -- every input is summed into exactly one slot, so
   the slot's gradient is the input's gradient.
+
+Build the plan with ``keep_values=1`` when its initial values may all be 1:
+a unit-valued plan stores no values and cannot take new ones.
 """
 from __future__ import annotations
 

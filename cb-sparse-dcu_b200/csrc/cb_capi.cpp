@@ -167,6 +167,7 @@ cbspmv_status upload_side(DevSide &s, cudaStream_t st) {
     s.d.m = L.m;
     s.d.n = L.n;
     s.d.pay16_end = (uint32_t)(L.payload.size() / 16);
+    s.d.unit = L.unit;
     s.d.sched = reinterpret_cast<uint32_t *>(s.counters);
     s.d.counters = s.counters + 4;
     s.d.max_entries = L.max_entries;
@@ -276,6 +277,7 @@ void cbspmv_default_opts(cbspmv_opts *o) {
     o->want_transpose = 0;
     o->tile_entries = 0;
     o->kernel = 0;
+    o->keep_values = 0;
 }
 
 cbspmv_status cbspmv_coo2block_gather(const cbspmv_coo *coo,
@@ -302,7 +304,7 @@ cbspmv_status cbspmv_coo2block_gather(const cbspmv_coo *coo,
             return fail(code, err);
         }
         err = cb::build_layout(p->host, o.value_type == CBSPMV_F32, o.tile_entries, o.kernel,
-                               p->A.lay, &code);
+                               !o.keep_values, p->A.lay, &code);
         if (!err.empty()) {
             delete p;
             return fail(code, err);
@@ -327,7 +329,8 @@ cbspmv_status cbspmv_coo2block_gather(const cbspmv_coo *coo,
                                tv.data(), p->host_t, &code);
             if (err.empty())
                 err = cb::build_layout(p->host_t, o.value_type == CBSPMV_F32,
-                                       o.tile_entries, o.kernel, p->AT.lay, &code);
+                                       o.tile_entries, o.kernel, !o.keep_values, p->AT.lay,
+                                       &code);
             if (!err.empty()) {
                 delete p;
                 return fail(code, "transpose: " + err);
@@ -351,10 +354,10 @@ cbspmv_status cbspmv_plan_save(const cbspmv_plan *p, const char *path) {
     if (!p || !path) return fail(CBSPMV_ERR_INVALID, "null argument");
     cb::PlanImage img;
     const cbspmv_opts &o = p->opts;
-    const int32_t opts9[9] = {o.block_size,  o.row_owned,      o.waves_per_block,
+    const int32_t opts[10] = {o.block_size,  o.row_owned,      o.waves_per_block,
                               o.dense_sixteenths, o.force_coo64, o.value_type,
-                              o.want_transpose,   o.tile_entries, o.kernel};
-    std::memcpy(img.opts9, opts9, sizeof opts9);
+                              o.want_transpose,   o.tile_entries, o.kernel, o.keep_values};
+    std::memcpy(img.opts, opts, sizeof opts);
     img.has_t = p->has_t ? 1 : 0;
     auto *q = const_cast<cbspmv_plan *>(p);  // visited, not modified, by the writer
     img.host = &q->host;
@@ -393,15 +396,16 @@ cbspmv_status cbspmv_plan_load(const char *path, cbspmv_plan **out) {
         return fail(CBSPMV_ERR_INVALID, err);
     }
     cbspmv_opts &o = p->opts;
-    o.block_size = img.opts9[0];
-    o.row_owned = img.opts9[1];
-    o.waves_per_block = img.opts9[2];
-    o.dense_sixteenths = img.opts9[3];
-    o.force_coo64 = img.opts9[4];
-    o.value_type = img.opts9[5];
-    o.want_transpose = img.opts9[6];
-    o.tile_entries = img.opts9[7];
-    o.kernel = img.opts9[8];
+    o.block_size = img.opts[0];
+    o.row_owned = img.opts[1];
+    o.waves_per_block = img.opts[2];
+    o.dense_sixteenths = img.opts[3];
+    o.force_coo64 = img.opts[4];
+    o.value_type = img.opts[5];
+    o.want_transpose = img.opts[6];
+    o.tile_entries = img.opts[7];
+    o.kernel = img.opts[8];
+    o.keep_values = img.opts[9];
     p->has_t = img.has_t != 0;
     if ((o.block_size != 16 && o.block_size != 32) ||
         (o.value_type != CBSPMV_F64 && o.value_type != CBSPMV_F32) || o.kernel < 0 ||
@@ -685,6 +689,10 @@ cbspmv_status cbspmv_set_values(cbspmv_plan *p, const void *input_values,
                                 void *stream) {
     if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
     if (!p->uploaded) return fail(CBSPMV_ERR_STATE, "plan not uploaded");
+    if (p->A.lay.unit)
+        return fail(CBSPMV_ERR_UNSUPPORTED,
+                    "this plan stores no values (every value was 1); build it with "
+                    "keep_values = 1 to change them");
     cudaStream_t st = (cudaStream_t)stream;
     DevSide *sides[2] = {&p->A, p->has_t ? &p->AT : nullptr};
     for (DevSide *s : sides) {

@@ -46,6 +46,15 @@ __device__ __forceinline__ void add_entries(T *myacc, const uint32_t *w, const T
         if (f[u]) myacc[r[u] * 32] = a[u] + s[u];
 }
 
+// Element (r, c) of a DENSE block payload: bs*bs values, or for a unit-valued
+// plan a bs*bs-bit mask (bit r*bs + c) of the entries equal to 1.
+template <typename T, int BS>
+__device__ __forceinline__ T dense_at(const uint8_t *pb, int unit, int r, int c) {
+    const int i = r * BS + c;
+    if (unit) return T((pb[i >> 3] >> (i & 7)) & 1);
+    return reinterpret_cast<const T *>(pb)[i];
+}
+
 // ---- bulk asynchronous copies (TMA, no multicast) completing on mbarriers.
 // Every wait is bounded: after kWaitLimit polls it sets *err and gives up.
 constexpr uint32_t kWaitLimit = 1u << 22;

@@ -41,6 +41,7 @@ std::atomic<int64_t> g_kernel_launches{0};
 using dev::a16;
 using dev::add_entries;
 using dev::kColMask;
+using dev::dense_at;
 using dev::kFull;
 constexpr int kWarps = 8;
 
@@ -108,7 +109,7 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
                         int64_t ldx, int64_t ldy, T *__restrict__ partials,
                         int32_t *__restrict__ counters, uint32_t *__restrict__ sched,
                         const uint32_t *__restrict__ ustart, int64_t nunits,
-                        int unit_tiles) {
+                        int unit_tiles, int unit) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -122,10 +123,10 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
         if (lane == 0) t = atomicAdd(&sched[0], 1u);
         return (int64_t)__shfl_sync(kFull, t, 0);
     };
-    int64_t unit = grab();
-    while (unit < nunits) {
+    int64_t cur = grab();  // the unit being processed
+    while (cur < nunits) {
         const int64_t next = grab();
-        const int64_t t0 = __ldg(&ustart[unit]), t1 = __ldg(&ustart[unit + 1]);
+        const int64_t t0 = __ldg(&ustart[cur]), t1 = __ldg(&ustart[cur + 1]);
         uint4 ta = __ldg(&tiles[2 * t0]), tb = __ldg(&tiles[2 * t0 + 1]);
         for (int64_t tile = t0; tile < t1; ++tile) {
             uint4 na = ta, nb4 = tb;  // the next tile's descriptors, in flight
@@ -175,7 +176,7 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
                     v[u] = T(0);
                     if (e < E) {
                         w[u] = __ldg(&cidx[e]);
-                        v[u] = __ldg(&cval[e]);
+                        v[u] = unit ? T(1) : __ldg(&cval[e]);
                     }
                 }
 #pragma unroll
@@ -208,21 +209,20 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
                     const int kb = __ldg(&rp[row]), ke = __ldg(&rp[row + 1]);
                     T sum = T(0);
                     for (int q = kb + sub; q < ke; q += L)
-                        sum += __ldg(&vv[q]) * xt[__ldg(&ci[q])];
+                        sum += (unit ? T(1) : __ldg(&vv[q])) * xt[__ldg(&ci[q])];
                     myacc[row * 32] += sum;
                 } else {
-                    const T *vv = reinterpret_cast<const T *>(pb);
                     T sum = T(0);
                     if (BS == 16) {
                         const int row = lane >> 1, c0 = (lane & 1) * 8;
 #pragma unroll
                         for (int c = 0; c < 8; ++c)
-                            sum += __ldg(&vv[row * 16 + c0 + c]) * xt[c0 + c];
+                            sum += dense_at<T, BS>(pb, unit, row, c0 + c) * xt[c0 + c];
                         myacc[row * 32] += sum;
                     } else {
 #pragma unroll 8
                         for (int c = 0; c < BS; ++c)
-                            sum += __ldg(&vv[lane * BS + c]) * xt[c];
+                            sum += dense_at<T, BS>(pb, unit, lane, c) * xt[c];
                         myacc[lane * 32] += sum;
                     }
                 }
@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
                 if (lane == 0) atomicExch(&counters[ta.y], 0);
             }
         }
-        unit = next;
+        cur = next;
     }
     // this warp has made its last (failing) grab: count it out; the last warp
     // out resets the scheduler for the next launch
@@ -335,7 +335,7 @@ struct Staged {
 // Reads a staged COO section into registers and issues its x gathers (the
 // loads stay in flight until the values are used).
 template <typename T>
-__device__ __forceinline__ void gather_tile(const unsigned char *buf, int E,
+__device__ __forceinline__ void gather_tile(const unsigned char *buf, int E, int unit,
                                             const T *__restrict__ x, int lane,
                                             Staged<T> &g) {
     const uint32_t *sidx = reinterpret_cast<const uint32_t *>(buf);
@@ -344,7 +344,7 @@ __device__ __forceinline__ void gather_tile(const unsigned char *buf, int E,
     for (int u = 0; u < kStreamChunk; ++u) {
         const int e = u * 32 + lane;
         g.w[u] = e < E ? sidx[e] : 0u;
-        g.v[u] = e < E ? sval[e] : T(0);
+        g.v[u] = e < E ? (unit ? T(1) : sval[e]) : T(0);
     }
 #pragma unroll
     for (int u = 0; u < kStreamChunk; ++u) {
@@ -360,7 +360,7 @@ __device__ __forceinline__ void add_tile(const uint4 ta, const uint4 tb, const S
                                          T *acc, T *xts, const uint4 *__restrict__ blocks,
                                          const uint8_t *__restrict__ payload,
                                          const int32_t *__restrict__ block_cols, int gather,
-                                         const T *__restrict__ x, int lane) {
+                                         int unit, const T *__restrict__ x, int lane) {
     T *myacc = &acc[lane];  // row r at myacc[r * 32]
     const int E = (int)tb.x;
     add_entries<T, kStreamChunk>(myacc, g.w, g.v, g.x, lane, 32, E);
@@ -403,19 +403,20 @@ __device__ __forceinline__ void add_tile(const uint4 ta, const uint4 tb, const S
                 const int row = lane / L, sub = lane % L;
                 const int kb = __ldg(&rp[row]), ke = __ldg(&rp[row + 1]);
                 T sum = T(0);
-                for (int q = kb + sub; q < ke; q += L) sum += __ldg(&vv[q]) * xt[__ldg(&ci[q])];
+                for (int q = kb + sub; q < ke; q += L)
+                    sum += (unit ? T(1) : __ldg(&vv[q])) * xt[__ldg(&ci[q])];
                 myacc[row * 32] += sum;
             } else {
-                const T *vv = reinterpret_cast<const T *>(pb);
                 T sum = T(0);
                 if (BS == 16) {
                     const int row = lane >> 1, cc = (lane & 1) * 8;
 #pragma unroll
-                    for (int c = 0; c < 8; ++c) sum += __ldg(&vv[row * 16 + cc + c]) * xt[cc + c];
+                    for (int c = 0; c < 8; ++c)
+                        sum += dense_at<T, BS>(pb, unit, row, cc + c) * xt[cc + c];
                     myacc[row * 32] += sum;
                 } else {
 #pragma unroll 8
-                    for (int c = 0; c < BS; ++c) sum += __ldg(&vv[lane * BS + c]) * xt[c];
+                    for (int c = 0; c < BS; ++c) sum += dense_at<T, BS>(pb, unit, lane, c) * xt[c];
                     myacc[lane * 32] += sum;
                 }
             }
@@ -490,7 +491,7 @@ __global__ void __launch_bounds__(kStreamWarps * 32)
                           const T *__restrict__ x, T *__restrict__ y, int64_t m,
                           T *__restrict__ partials, int32_t *__restrict__ counters,
                           uint32_t *__restrict__ sched,
-                          const uint32_t *__restrict__ wpart, uint32_t cap) {
+                          const uint32_t *__restrict__ wpart, uint32_t cap, int unit) {
     using SL = StreamLayout<T, BS>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
@@ -523,7 +524,7 @@ __global__ void __launch_bounds__(kStreamWarps * 32)
     };
     auto stage = [&](const uint4 &a, const uint4 &b, int bi) {
         if (lane == 0) {
-            const uint32_t bytes = a16(4u * b.x) + a16(vsz * b.x);
+            const uint32_t bytes = a16(4u * b.x) + (unit ? 0u : a16(vsz * b.x));
             if (bytes == 0) {
                 mbar_arrive(&mbar[bi]);
             } else {
@@ -557,7 +558,7 @@ __global__ void __launch_bounds__(kStreamWarps * 32)
     }
     Staged<T> g0, g1;  // tile i's registers, tile i+1's registers
     bool ok = wait_buf(0);
-    if (ok) gather_tile(buf0, (int)b0.x, x, lane, g0);
+    if (ok) gather_tile(buf0, (int)b0.x, unit, x, lane, g0);
     __syncwarp();
     if (ok && nt > 2) {
         stage(a2, b2, 0);
@@ -569,14 +570,15 @@ __global__ void __launch_bounds__(kStreamWarps * 32)
         desc(i + 4, a4, b4);
         if (i + 1 < nt) {
             if (!wait_buf(nb)) break;
-            gather_tile(buf0 + nb * cap, (int)b1.x, x, lane, g1);
+            gather_tile(buf0 + nb * cap, (int)b1.x, unit, x, lane, g1);
             __syncwarp();
             if (i + 3 < nt) {
                 stage(a3, b3, nb);
                 inflight |= 1u << nb;
             }
         }
-        add_tile<T, BS>(a0, b0, g0, acc, xts, blocks, payload, block_cols, gather, x, lane);
+        add_tile<T, BS>(a0, b0, g0, acc, xts, blocks, payload, block_cols, gather, unit, x,
+                        lane);
         ++runlen;
         if (i + 1 >= nt || a1.y != a0.y) {  // the row's run in this warp ends here
             store_run<T, BS>(a0, b0, t0 + i, runlen, acc, y, m, partials, counters, wpart, gw,
@@ -675,7 +677,8 @@ cudaError_t launch_chunk(const DevLayout &d, const void *x, void *y, int nrhs,
     cb_spmv_tile_kernel<T, BS, CH><<<(unsigned)grid, kWarps * 32, smem, stream>>>(
         static_cast<const uint4 *>(d.tiles), static_cast<const uint4 *>(d.blocks), d.payload,
         d.block_cols, d.gather, static_cast<const T *>(x), static_cast<T *>(y), d.m, ldx, ldy,
-        static_cast<T *>(d.partials), d.counters, d.sched, d.dunit, d.ndunits, kDirectUnitTiles);
+        static_cast<T *>(d.partials), d.counters, d.sched, d.dunit, d.ndunits, kDirectUnitTiles,
+        d.unit);
     note_launch();
     return cudaGetLastError();
 }
@@ -741,7 +744,7 @@ cudaError_t launch_stream(const DevLayout &d, const void *x, void *y, cudaStream
             static_cast<const uint4 *>(d.tiles), d.ntiles,
             static_cast<const uint4 *>(d.blocks), d.payload, d.block_cols, d.gather,
             static_cast<const T *>(x), static_cast<T *>(y), d.m,
-            static_cast<T *>(d.partials), d.counters, d.sched, d.wpart, c.cap);
+            static_cast<T *>(d.partials), d.counters, d.sched, d.wpart, c.cap, d.unit);
     note_launch();
     return cudaGetLastError();
 }

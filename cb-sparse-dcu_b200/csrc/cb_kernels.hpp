@@ -16,6 +16,7 @@ struct DevLayout {
     const int32_t *block_cols = nullptr;
     int64_t ntiles = 0;
     int bs = 16, f32 = 0, gather = 0;
+    int unit = 0;                     // no stored values (all 1), DENSE as bitmasks
     int64_t m = 0, n = 0;
     void *partials = nullptr;         // slots * bs values (scratch)
     int32_t *counters = nullptr;      // gb_m arrival counters (scratch)
@@ -49,6 +50,7 @@ struct MatView {
     int64_t ntiles = 0, m = 0, ldx = 1, ldy = 1;
     int nrhs = 1, gather = 0;
     int xvec = 0;               // x rows allow vector loads of V values
+    int unit = 0;               // no stored values (all 1), DENSE as bitmasks
     uint32_t pay16_end = 0;     // payload size in 16-byte units
 };
 

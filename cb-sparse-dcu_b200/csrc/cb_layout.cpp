@@ -22,6 +22,7 @@ inline int64_t a16(int64_t x) { return (x + 15) & ~int64_t(15); }
 struct Ctx {
     const HostCB &g;
     int bs, bits, vsz, isz, emax, max_xt;
+    int unit = 0;       // values all 1: no value arrays, DENSE blocks as bitmasks
     int64_t max_bytes;  // tile payload cap (a larger single block is a tile alone)
     std::vector<int64_t> rowptr;  // device block order grouped by block row
     std::vector<int64_t> order;   // final block indices
@@ -31,16 +32,17 @@ struct Ctx {
     int type(int64_t i) const { return g.type_blk[i] & kTypeMask; }
     int64_t k(int64_t i) const { return g.nnz_blk[i]; }
     bool is_coo(int64_t i) const { return type(i) == kCOO; }
+    int64_t coo_bytes(int64_t E) const { return a16(E * 4) + (unit ? 0 : a16(E * vsz)); }
     int64_t payload_bytes(int64_t i) const {
         const int64_t kk = k(i);
-        if (type(i) == kCSR) return a16((bs + 1 + kk) * isz) + a16(kk * vsz);
-        return (int64_t)bs * bs * vsz;  // dense
+        if (type(i) == kCSR) return a16((bs + 1 + kk) * isz) + (unit ? 0 : a16(kk * vsz));
+        return unit ? (int64_t)bs * bs / 8 : (int64_t)bs * bs * vsz;  // dense
     }
     int64_t alg_payload(int64_t i) const {
         const int64_t kk = k(i);
-        if (type(i) == kCOO) return kk * (4 + vsz);
-        if (type(i) == kCSR) return (bs + 1 + kk) * isz + kk * vsz;
-        return (int64_t)bs * bs * vsz;
+        if (type(i) == kCOO) return kk * (4 + (unit ? 0 : vsz));
+        if (type(i) == kCSR) return (bs + 1 + kk) * isz + (unit ? 0 : kk * vsz);
+        return unit ? (int64_t)bs * bs / 8 : (int64_t)bs * bs * vsz;
     }
     int64_t nvals(int64_t i) const {
         return type(i) == kDENSE ? (int64_t)bs * bs : k(i);
@@ -66,7 +68,7 @@ struct Ctx {
 template <class Fn>
 void split_row(const Ctx &c, int64_t b0, int64_t b1, Fn fn) {
     int64_t s = b0, nb = 0, e = 0, nxt = 0, xbytes = 0;
-    auto bytes = [&](int64_t ee, int64_t xb) { return a16(ee * 4) + a16(ee * c.vsz) + xb; };
+    auto bytes = [&](int64_t ee, int64_t xb) { return c.coo_bytes(ee) + xb; };
     for (int64_t p = b0; p < b1; ++p) {
         const int64_t i = c.order[p];
         const bool coo = c.is_coo(i);
@@ -98,7 +100,7 @@ struct RowTotals {
 
 }  // namespace
 
-std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
+std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel, int unit,
                          DeviceLayout &L, int *code) {
     *code = CBSPMV_ERR_UNSUPPORTED;
     if (g.n > kMaxCols)
@@ -109,6 +111,7 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
     c.bs = g.o.bs;
     c.bits = c.bs == 16 ? 4 : 5;
     c.vsz = f32 ? 4 : 8;
+    c.unit = unit && g.unit_values ? 1 : 0;
     c.isz = c.bs == 16 ? 1 : 2;
     int64_t auto_emax = kTileEntries;
     if (kernel != 2) {
@@ -164,7 +167,7 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
                     if (g.gather_flag) t.bcols += c.valid_cols(i);
                 }
             }
-            t.bytes += a16(E * 4) + a16(E * vsz);
+            t.bytes += c.coo_bytes(E);
         });
         tot[R] = t;
     }
@@ -197,6 +200,7 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
     L = DeviceLayout();
     L.bs = bs;
     L.f32 = f32;
+    L.unit = c.unit;
     L.gather = g.gather_flag;
     L.m = g.m;
     L.n = g.n;
@@ -262,7 +266,7 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
             uint8_t *base = L.payload.data() + byte;
             uint32_t *idx = (uint32_t *)base;
             const int64_t vals_at = a16(E * 4);
-            int64_t xoff = a16(E * 4) + a16(E * vsz);  // CSR/dense payloads
+            int64_t xoff = c.coo_bytes(E);  // CSR/dense payloads
             int64_t e0 = 0;
             for (size_t q = 0; q < tb.size(); ++q) {
                 const int64_t i = tb[q];
@@ -342,6 +346,10 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
                 for (int64_t q2 = 0; q2 < E; ++q2) {
                     const int64_t from = (int64_t)(key[q2] & 0xffff);
                     idx[q2] = (uint32_t)(key[q2] >> 16);
+                    if (c.unit) {  // no value arrays: nothing to place
+                        L.val_off[val + from] = 0;
+                        continue;
+                    }
                     const int64_t at = byte + vals_at + q2 * vsz;
                     put_tile_val(at, sorted_val[from]);
                     L.val_off[val + from] = (uint64_t)at;
@@ -349,7 +357,7 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
             }
             // value slots of CSR/DENSE blocks come after the tile's COO values
             int64_t v = val + E;
-            int64_t xo = a16(E * 4) + a16(E * vsz);
+            int64_t xo = c.coo_bytes(E);
             for (size_t q = ncoo; q < tb.size(); ++q) {
                 const int64_t i = tb[q];
                 const int32_t o = c.origin(i);
@@ -363,13 +371,18 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
                 for (int64_t q2 = 0; q2 < nv; ++q2) {
                     const int64_t at = byte + xo + vals_here + q2 * vsz;
                     const double x = pf[q2];
-                    if (f32) {
+                    if (c.unit) {  // CSR: no values; DENSE: bit q2 of the bitmask
+                        if (ty != kCSR && x == 1.0)
+                            L.payload[byte + xo + q2 / 8] |= (uint8_t)(1u << (q2 % 8));
+                        L.val_off[v + q2] = 0;
+                    } else if (f32) {
                         const float f = (float)x;
                         std::memcpy(L.payload.data() + at, &f, 4);
+                        L.val_off[v + q2] = (uint64_t)at;
                     } else {
                         std::memcpy(L.payload.data() + at, &x, 8);
+                        L.val_off[v + q2] = (uint64_t)at;
                     }
-                    L.val_off[v + q2] = (uint64_t)at;
                     int64_t r, col;
                     if (ty == kCSR) {
                         r = 0;
@@ -404,7 +417,7 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
             }
             val = vv;
             blk += (int64_t)tb.size();
-            byte += a16(E * 4) + a16(E * vsz);
+            byte += c.coo_bytes(E);
             for (size_t q = ncoo; q < tb.size(); ++q) byte += c.payload_bytes(tb[q]);
             ++tile;
             ++t_in_row;

@@ -64,6 +64,7 @@ inline uint32_t meta_nnz(uint32_t m) { return (m >> 3) & 2047u; }
 struct DeviceLayout {
     int bs = 16;
     int f32 = 0;  // value type of the payload
+    int unit = 0;  // every value is 1: no value arrays, DENSE blocks as bitmasks
     int gather = 0;
     int64_t m = 0, n = 0, gb_m = 0;
     std::vector<TileDesc> tiles;
@@ -91,7 +92,10 @@ struct DeviceLayout {
 // kernel: 0 auto, 1 streaming, 2 direct -- the default tile size follows the
 // kernel family (256 COO entries for the streaming kernel, 512 otherwise; the
 // automatic choice is streaming when most stored entries are in COO blocks).
-std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
+// unit = 1: when every stored value is 1 (g.unit_values), store no values and
+// DENSE blocks as bs*bs-bit masks (the reference's UNIT_VALUES,
+// cb-spmv-dcu.hpp:1105-1127).
+std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel, int unit,
                          DeviceLayout &L, int *code);
 
 // Cost-balanced contiguous split of the tiles over `warps` warps (the

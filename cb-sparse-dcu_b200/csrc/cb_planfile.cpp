@@ -127,7 +127,7 @@ void visit(Ar &ar, HostCB &g) {
 
 template <class Ar>
 void visit(Ar &ar, DeviceLayout &L) {
-    ar(L.bs), ar(L.f32), ar(L.gather), ar(L.m), ar(L.n), ar(L.gb_m);
+    ar(L.bs), ar(L.f32), ar(L.unit), ar(L.gather), ar(L.m), ar(L.n), ar(L.gb_m);
     ar(L.tiles), ar(L.blocks), ar(L.payload), ar(L.block_cols);
     ar(L.slots), ar(L.split_rows), ar(L.max_row_tiles), ar(L.max_entries);
     ar(L.max_tile_bytes), ar(L.coo_share), ar(L.nvals);
@@ -137,7 +137,7 @@ void visit(Ar &ar, DeviceLayout &L) {
 
 template <class Ar>
 void visit_body(Ar &ar, PlanImage &img) {
-    for (int32_t &v : img.opts9) ar(v);
+    for (int32_t &v : img.opts) ar(v);
     ar(img.has_t);
     visit(ar, *img.host);
     visit(ar, *img.A);

@@ -11,10 +11,10 @@
 
 namespace cb {
 
-// Everything a plan keeps on the host.  opts9: the nine int fields of
+// Everything a plan keeps on the host.  opts: the ten int fields of
 // cbspmv_opts in declaration order.
 struct PlanImage {
-    int32_t opts9[9] = {};
+    int32_t opts[10] = {};
     int32_t has_t = 0;
     HostCB *host = nullptr, *host_t = nullptr;
     DeviceLayout *A = nullptr, *AT = nullptr;
@@ -24,6 +24,6 @@ struct PlanImage {
 std::string save_plan(const PlanImage &img, const std::string &path);
 std::string load_plan(const std::string &path, PlanImage &img);
 
-constexpr uint32_t kPlanFileVersion = 1;
+constexpr uint32_t kPlanFileVersion = 2;
 
 }  // namespace cb

@@ -42,6 +42,7 @@ namespace {
 using dev::a16;
 using dev::add_entries;
 using dev::bulk_g2s;
+using dev::dense_at;
 using dev::fence_mbar_init;
 using dev::fence_proxy_async;
 using dev::kColMask;
@@ -154,7 +155,7 @@ __device__ __forceinline__ void ms_add(const MatView &M, const uint4 ta, const u
         for (int u = 0; u < KC; ++u) {
             const int e = c0 + u * G + es;
             w_[u] = e < E ? sidx[e] : 0u;
-            a_[u] = e < E ? sval[e] : T(0);
+            a_[u] = e < E ? (M.unit ? T(1) : sval[e]) : T(0);
         }
 #pragma unroll
         for (int u = 0; u < KC; ++u) {
@@ -264,7 +265,7 @@ __device__ __forceinline__ void ms_add(const MatView &M, const uint4 ta, const u
 #pragma unroll
                     for (int v = 0; v < V; ++v) sum[v] = T(0);
                     for (int t = rp[row] + (G >= BS ? es % L : 0); t < rp[row + 1]; t += L) {
-                        const T av = vv[t];
+                        const T av = M.unit ? T(1) : vv[t];
                         lds_v<T, V>(xq + ci[t] * RV, xx);
 #pragma unroll
                         for (int v = 0; v < V; ++v) sum[v] = fma(av, xx[v], sum[v]);
@@ -273,7 +274,6 @@ __device__ __forceinline__ void ms_add(const MatView &M, const uint4 ta, const u
                     if (G >= BS) break;
                 }
             } else {  // DENSE, row-major bs x bs; columns in a rotated order
-                const T *vv = reinterpret_cast<const T *>(pb);
                 constexpr int L = G >= BS ? G / BS : 1;
                 constexpr int RS = G >= BS ? BS : G;
                 constexpr int W = BS / L;  // columns per lane
@@ -285,7 +285,7 @@ __device__ __forceinline__ void ms_add(const MatView &M, const uint4 ta, const u
 #pragma unroll 4
                     for (int c = 0; c < W; ++c) {
                         const int cc = cb0 + ((c + row) % W);
-                        const T av = vv[row * BS + cc];
+                        const T av = dense_at<T, BS>(pb, M.unit, row, cc);
                         lds_v<T, V>(xq + cc * RV, xx);
 #pragma unroll
                         for (int v = 0; v < V; ++v) sum[v] = fma(av, xx[v], sum[v]);
@@ -731,6 +731,7 @@ MatView mat_view(const DevLayout &d, const void *x, void *y, int nrhs, int64_t l
     M.nrhs = nrhs;
     M.gather = d.gather;
     M.pay16_end = d.pay16_end;
+    M.unit = d.unit;
     // vector x loads: rows aligned to V values and every V-group a lane reads
     // inside its row (ldx a multiple of V, and the last group within ldx)
     const MsClass c = ms_class(nrhs, d.f32);

@@ -62,6 +62,11 @@ typedef struct cbspmv_opts {
                              2 direct (high occupancy, for CSR/dense-heavy
                              ones), 3 staged (the several-right-hand-side
                              kernel, one vector); see cbspmv_autotune      */
+    int keep_values;      /* 0 (default): when every stored value is 1, store
+                             no values and DENSE blocks as bitmasks, as the
+                             reference does (UNIT_VALUES,
+                             cb-spmv-dcu.hpp:1105-1127); such a plan refuses
+                             cbspmv_set_values.  1: always store values    */
 } cbspmv_opts;
 
 /* Host COO, 0-based, rows in non-decreasing order (the order the reference's

@@ -34,6 +34,8 @@ def decode_spmv(plan, x: np.ndarray, transpose: bool = False) -> np.ndarray:
     isz = 1 if bs == 16 else 2
     it = np.uint8 if bs == 16 else np.uint16
     gather = d["gather_flag"]
+    # unit-valued layouts store no values and DENSE blocks as bitmasks
+    unit = bool(plan.info()["unit_values"]) and not plan.opts.keep_values
     bcols = d["block_cols"]
     m = d["m"]
     y = np.zeros(m, np.longdouble)
@@ -44,7 +46,8 @@ def decode_spmv(plan, x: np.ndarray, transpose: bool = False) -> np.ndarray:
         assert nb == ncoo + nxt and nb <= 32 and E <= 512
         base = p16 * 16
         idx = pay[base:base + 4 * E].view(np.uint32)
-        cv = pay[base + _a16(4 * E):base + _a16(4 * E) + vsz * E].view(vt)
+        cv = (np.ones(E, vt) if unit else
+              pay[base + _a16(4 * E):base + _a16(4 * E) + vsz * E].view(vt))
         r0 = brow * bs
         rows = np.arange(r0, min(r0 + bs, m))
         seen_rows[rows] = True
@@ -71,13 +74,17 @@ def decode_spmv(plan, x: np.ndarray, transpose: bool = False) -> np.ndarray:
                 rp = pay[pb:pb + (bs + 1) * isz].view(it)
                 ci = pay[pb + (bs + 1) * isz:pb + (bs + 1 + k) * isz].view(it)
                 vo = pb + _a16((bs + 1 + k) * isz)
-                vv = pay[vo:vo + k * vsz].view(vt)
+                vv = np.ones(k, vt) if unit else pay[vo:vo + k * vsz].view(vt)
                 for r in range(bs):
                     for kk in range(int(rp[r]), int(rp[r + 1])):
                         y[r0 + r] += np.longdouble(vv[kk]) * x[xcol(int(ci[kk]))]
             else:
                 assert typ == 3
-                vv = pay[pb:pb + bs * bs * vsz].view(vt)
+                if unit:
+                    vv = np.unpackbits(pay[pb:pb + bs * bs // 8],
+                                       bitorder="little").astype(vt)
+                else:
+                    vv = pay[pb:pb + bs * bs * vsz].view(vt)
                 for r in range(bs):
                     if r0 + r >= m:
                         continue

@@ -187,3 +187,39 @@ def test_info_counts():
     assert i["coo_blocks"] == np.sum(t == 0) and i["csr_blocks"] == np.sum(t == 1)
     assert i["dense_blocks"] == np.sum(t == 3)
     assert i["algorithmic_bytes"] > 0 and i["tiles"] >= 1
+
+
+def _unit_cases():
+    from cbspmv import gen
+    rng = np.random.default_rng(77)
+    band = gen.banded(rng, 700, 20)
+    return [("coo", gen.random_small(rng, 1500, 1200, 20000, unit=True)),
+            ("dense", gen.random_small(rng, 128, 128, 15000, unit=True)),
+            ("banded", gen.Coo(band.m, band.n, band.row, band.col, np.ones(band.nnz)))]
+
+
+UNIT_CASES = _unit_cases()
+
+
+@pytest.mark.parametrize("name,coo", UNIT_CASES, ids=[c[0] for c in UNIT_CASES])
+@pytest.mark.parametrize("bs", [16, 32])
+@pytest.mark.parametrize("f32", [0, 1])
+def test_unit_layout_reads_back(name, coo, bs, f32):
+    """Unit-valued matrices (the reference's UNIT_VALUES, cb-spmv-dcu.hpp:
+    1105-1127): the layout stores no values and DENSE blocks as bitmasks,
+    evaluates to the oracle's y, and is smaller than the valued layout."""
+    import cbspmv
+    from cbspmv import gen
+    p = cbspmv.Plan(coo, block_size=bs, value_type=f32, tile_entries=64, want_transpose=1)
+    k = cbspmv.Plan(coo, block_size=bs, value_type=f32, tile_entries=64, keep_values=1)
+    assert p.info()["unit_values"] == 1
+    assert p.info()["device_bytes"] < k.info()["device_bytes"]
+    assert p.info()["algorithmic_bytes"] < k.info()["algorithmic_bytes"]
+    tol = 1e-6 if f32 else 1e-13
+    x = gen.uniform_x(coo.n, 3)
+    yref, ab = cd.oracle_spmm_ld(coo, x[None, :])
+    for plan in (p, k):
+        assert np.all(np.abs(ld.decode_spmv(plan, x) - yref[0]) <= tol * ab[0] + 1e-300)
+    g = gen.uniform_x(coo.m, 4)
+    gref, gab = cd.oracle_spmm_ld(coo, g[None, :], transpose=True)
+    assert np.all(np.abs(ld.decode_spmv(p, g, transpose=True) - gref[0]) <= tol * gab[0] + 1e-300)

@@ -228,3 +228,46 @@ def test_empty_and_degenerate(cuda):
     y = p.spmv(x, torch.full((1000,), 7.0, dtype=torch.float64, device=cuda))
     yy = y.cpu().numpy()
     assert yy[999] == 2.5 and not yy[:999].any()
+
+
+def _unit_cases():
+    from cbspmv import gen
+    rng = np.random.default_rng(78)
+    band = gen.banded(rng, 3000, 40)
+    return [("coo", gen.random_small(rng, 4000, 3000, 60000, unit=True)),
+            ("dense", gen.random_small(rng, 256, 256, 60000, unit=True)),
+            ("banded", gen.Coo(band.m, band.n, band.row, band.col, np.ones(band.nnz)))]
+
+
+UNIT = _unit_cases()
+
+
+@pytest.mark.parametrize("name,coo", UNIT, ids=[c[0] for c in UNIT])
+@pytest.mark.parametrize("bs", [16, 32])
+@pytest.mark.parametrize("f32", [False, True])
+@pytest.mark.parametrize("kernel", [1, 2, 3])
+@pytest.mark.parametrize("nrhs", [1, 4])
+def test_unit_valued_plans(cuda, name, coo, bs, f32, kernel, nrhs):
+    """Unit-valued matrices run without stored values (DENSE blocks as
+    bitmasks) in every kernel, and refuse set_values."""
+    import torch
+    import cbspmv
+    import cbdump as cd
+    from cbspmv import gen
+    dt = torch.float32 if f32 else torch.float64
+    plan = cbspmv.Plan(coo, block_size=bs, value_type=int(f32), kernel=kernel, tile_entries=128)
+    assert plan.info()["unit_values"] == 1
+    X = gen.uniform_x(coo.n, 6, nrhs=max(nrhs, 2))[:nrhs]
+    if f32:
+        X = X.astype(np.float32).astype(np.float64)
+    yref, ab = cd.oracle_spmm_ld(coo, X)
+    xd = torch.from_numpy(np.ascontiguousarray(X.T)).to(cuda, dt)
+    if nrhs == 1:
+        xd = xd[:, 0].contiguous()
+    for _ in range(2):
+        y = plan.spmv(xd)
+        torch.cuda.synchronize()
+        _check(y.cpu().numpy().reshape(coo.m, nrhs).T, yref, ab, f32, f"unit {name}")
+    with pytest.raises(cbspmv.CBSpMVError) as e:
+        plan.set_values(torch.ones(coo.nnz, dtype=dt, device=cuda))
+    assert e.value.status == "UNSUPPORTED"
