@@ -170,7 +170,9 @@ def _timed(fn, reps: int, warmup: int, flush=None):
 def secondary_configs(dev, peak: float, want=("lap", "pl32", "st", "diff", "bat"),
                       bat_count: int = 512) -> dict:
     """The other workloads of the benchmark suite, each timed on the device:
-    LAP (5-point Laplacian 256^2, FP64), PL in FP32, ST (27-point x 3 dof
+    LAP (5-point Laplacian 256^2, FP64), PL in FP32, PL with unit values (the
+    value-free payload the reference uses for its unit-valued inputs), ST
+    (27-point x 3 dof
     stencil on 64^3, FP64 and FP32), DIFF (power-law n = 2^18, 8 right-hand
     sides, FP32: forward, adjoint A^T G and the value gradient) and BAT (512
     uneven FP32 matrices with 1-16 right-hand sides: one batched launch per
@@ -206,6 +208,11 @@ def secondary_configs(dev, peak: float, want=("lap", "pl32", "st", "diff", "bat"
         single("LAP fp64 (256^2 5-point)", gen.laplacian_2d(), False)
     if "pl32" in want:
         single("PL fp32 (n=2^20)", gen.power_law(), True)
+    if "unit" in want:  # the reference's own matrices are unit-valued (its reader sets 1.0)
+        pl = gen.power_law()
+        single("PL fp64 unit values (value-free payload)",
+               gen.Coo(pl.m, pl.n, pl.row, pl.col, np.ones(pl.nnz)), False)
+        del pl
     if "st" in want:
         st = gen.stencil_27pt()
         single("ST fp64 (64^3 x 3 dof 27-point)", st, False, reps=20)
@@ -371,7 +378,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--configs", default="all",
                     help="other workloads to time (rank 0, N=1 only): all, none, or a "
-                         "comma list of lap,pl32,st,diff,bat")
+                         "comma list of lap,pl32,unit,st,diff,bat")
     ap.add_argument("--bat-count", type=int, default=512,
                     help="matrices in the BAT batch (512 is the workload; fewer for "
                          "profiling captures)")
@@ -491,7 +498,7 @@ def main():
     line = None
     configs = None
     if rank == 0 and world == 1 and args.configs != "none":
-        want = {"lap", "pl32", "st", "diff", "bat"} if args.configs == "all" \
+        want = {"lap", "pl32", "unit", "st", "diff", "bat"} if args.configs == "all" \
             else set(args.configs.split(","))
         configs = secondary_configs(dev, peak, want, args.bat_count)
     if rank == 0:
