@@ -246,7 +246,7 @@ def diff_config(dev, peak, flush, out):
     fwd_bytes = info["algorithmic_bytes"] + xy
     adj_bytes = fwd_bytes + plan.num_values() * (8 + 4) + 4 * (coo.n + coo.m) * k
     t_f = _timed(lambda: plan.spmv(X, Y), 30, 5, flush)
-    t_a = _timed(lambda: (plan.spmv_t(G, GX), plan.grad_vals(G, X, GV)), 30, 5, flush)
+    t_a = _timed(lambda: plan.adjoint(G, X, GX, GV), 30, 5, flush)
     out["DIFF fp32 (n=2^18, 8 rhs)"] = {
         "nnz": coo.nnz, "fwd_ms": round(t_f, 4), "adj_ms": round(t_a, 4),
         "fwd_plus_adj_over_fwd": round((t_f + t_a) / t_f, 3),

@@ -100,6 +100,8 @@ def _load():
         "cbspmv_spmv_t": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, _I64, _I64, _P]),
         "cbspmv_grad_vals": (ctypes.c_int, [_P, _P, _P, _P, ctypes.c_int, _I64,
                                             _I64, _P]),
+        "cbspmv_adjoint": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int, _I64, _I64,
+                                          _I64, _P]),
         "cbspmv_num_values": (_I64, [_P]),
         "cbspmv_set_values": (ctypes.c_int, [_P, _P, _P]),
         "cbspmv_value_coords": (ctypes.c_int, [_P, _P, _P, _P]),
@@ -361,6 +363,31 @@ class Plan:
         _check(_lib.cbspmv_grad_vals(self._h, _dptr(g), _dptr(x), _dptr(out), k,
                                      k, k, _stream(stream)))
         return out
+
+    def adjoint(self, g, x, gx=None, gvals=None, want_gx=True, want_gvals=True,
+                stream=None):
+        """(A^T g, value gradient) in one call, the value gradient on a
+        second stream of the plan's (needs want_transpose=1 for A^T g);
+        returns (gx, gvals), None for an output not wanted."""
+        import torch
+        self.upload(stream)
+        self._check_dev(g, x)
+        k = 1 if g.dim() == 1 else g.shape[1]
+        if want_gx and gx is None:
+            gx = torch.empty((self.n,) if g.dim() == 1 else (self.n, k),
+                             dtype=g.dtype, device=g.device)
+        if want_gvals and gvals is None:
+            gvals = torch.empty(self.num_values(), dtype=g.dtype, device=g.device)
+        gx = gx if want_gx else None
+        gvals = gvals if want_gvals else None
+        for t in (gx, gvals):
+            if t is not None:
+                self._check_dev(t)
+        _check(_lib.cbspmv_adjoint(self._h, _dptr(g), _dptr(x),
+                                   _dptr(gx) if gx is not None else None,
+                                   _dptr(gvals) if gvals is not None else None,
+                                   k, k, k, k, _stream(stream)))
+        return gx, gvals
 
     def set_values(self, vals, stream=None):
         """Re-pack A (and A^T) from new input values (nnz, caller order)."""

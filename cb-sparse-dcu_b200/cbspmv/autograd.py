@@ -32,15 +32,18 @@ class CBSpMVFunction(torch.autograd.Function):
         plan = ctx.plan
         (x,) = ctx.saved_tensors
         gy = gy.contiguous()
-        gx = gvals = None
-        if ctx.needs_input_grad[1]:
-            gx = plan.spmv_t(gy)
-        if ctx.needs_input_grad[0]:
+        want_gx, want_v = ctx.needs_input_grad[1], ctx.needs_input_grad[0]
+        if not (want_gx or want_v):
+            return None, None, None
+        # both in one call: the value gradient overlaps A^T g on a second stream
+        gx, gslots = plan.adjoint(gy, x.contiguous(), want_gx=want_gx, want_gvals=want_v)
+        gvals = None
+        if want_v:
             slots = getattr(plan, "_slots_dev", None)
             if slots is None or slots.device != gy.device:
                 slots = torch.from_numpy(plan.input_slots()).to(gy.device)
                 plan._slots_dev = slots
-            gvals = plan.grad_vals(gy, x.contiguous())[slots]
+            gvals = gslots[slots]
         return gvals, gx, None
 
 

@@ -123,9 +123,15 @@ struct cbspmv_plan {
     void *hx = nullptr, *hy = nullptr;
     size_t hx_bytes = 0, hy_bytes = 0;
     HostPipe pipe;
+    // cbspmv_adjoint: the value gradient's stream and its fork/join events
+    cudaStream_t adj = nullptr;
+    cudaEvent_t adj_fork = nullptr, adj_join = nullptr;
     ~cbspmv_plan() {
         if (pipe.comp) cudaStreamSynchronize(pipe.out ? pipe.out : pipe.comp);
         pipe.release();
+        if (adj) cudaStreamSynchronize(adj), cudaStreamDestroy(adj);
+        if (adj_fork) cudaEventDestroy(adj_fork);
+        if (adj_join) cudaEventDestroy(adj_join);
         A.release();
         AT.release();
         if (hx) cudaFree(hx);
@@ -681,6 +687,42 @@ cbspmv_status cbspmv_grad_vals(cbspmv_plan *p, const void *g, const void *x,
                                  ldg, x, ldx, nrhs, gvals, (cudaStream_t)stream),
             "grad_vals launch");
     return CBSPMV_OK;
+}
+
+cbspmv_status cbspmv_adjoint(cbspmv_plan *p, const void *g, const void *x, void *gx,
+                             void *gvals, int nrhs, int64_t ldg, int64_t ldx, int64_t ldgx,
+                             void *stream) {
+    if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
+    if (!gx && !gvals) return fail(CBSPMV_ERR_INVALID, "neither gx nor gvals given");
+    if (gx && !p->has_t) return fail(CBSPMV_ERR_STATE, "plan built without want_transpose");
+    if (!gx) return cbspmv_grad_vals(p, g, x, gvals, nrhs, ldg, ldx, stream);
+    if (!gvals) return cbspmv_spmv_t(p, g, gx, nrhs, ldg, ldgx, stream);
+    if (!p->uploaded) return fail(CBSPMV_ERR_STATE, "plan not uploaded");
+    if (nrhs < 1) return fail(CBSPMV_ERR_INVALID, "nrhs must be >= 1");
+    const int64_t lg = ldg ? ldg : nrhs, lx = ldx ? ldx : nrhs;
+    if (lg < nrhs || lx < nrhs)
+        return fail(CBSPMV_ERR_INVALID, "leading dimension smaller than nrhs");
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev != p->device)
+        return fail(CBSPMV_ERR_STATE, "plan was uploaded to another device");
+    if (!p->adj) {
+        CB_CUDA(cudaStreamCreateWithFlags(&p->adj, cudaStreamNonBlocking), "adjoint stream");
+        CB_CUDA(cudaEventCreateWithFlags(&p->adj_fork, cudaEventDisableTiming), "adjoint event");
+        CB_CUDA(cudaEventCreateWithFlags(&p->adj_join, cudaEventDisableTiming), "adjoint event");
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    CB_CUDA(cudaEventRecord(p->adj_fork, st), "adjoint fork");
+    CB_CUDA(cudaStreamWaitEvent(p->adj, p->adj_fork, 0), "adjoint fork");
+    DevSide &s = p->A;
+    CB_CUDA(cb::launch_grad_vals(s.lay.f32, s.lay.nvals, s.val_row, s.val_col, g, lg, x, lx,
+                                 nrhs, gvals, p->adj),
+            "grad_vals launch");
+    const cbspmv_status rc = run_side(p, p->AT, g, gx, nrhs, lg, ldgx, st);
+    // join even when A^T g failed, so no work is left unordered on `stream`
+    CB_CUDA(cudaEventRecord(p->adj_join, p->adj), "adjoint join");
+    CB_CUDA(cudaStreamWaitEvent(st, p->adj_join, 0), "adjoint join");
+    return rc;
 }
 
 int64_t cbspmv_num_values(const cbspmv_plan *p) { return p ? p->A.lay.nvals : -1; }

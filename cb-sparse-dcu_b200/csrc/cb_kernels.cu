@@ -610,46 +610,74 @@ __global__ void cb_set_values_kernel(int64_t nvals, const int64_t *__restrict__ 
     *reinterpret_cast<T *>(payload + off[v]) = s;
 }
 
-// VEC right-hand sides per load (16-byte vectors) when both rows are aligned
-// to them and nrhs is a multiple of VEC; VEC = 1 otherwise.
-template <typename T, int VEC>
-__global__ void cb_grad_vals_kernel(int64_t nvals, const int32_t *__restrict__ vrow,
-                                    const int32_t *__restrict__ vcol,
-                                    const T *__restrict__ g, int64_t ldg,
-                                    const T *__restrict__ x, int64_t ldx, int nrhs,
-                                    T *__restrict__ out) {
-    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (v >= nvals) return;
-    const int32_t r = __ldg(&vrow[v]), c = __ldg(&vcol[v]);
-    T s = T(0);
-    if (r >= 0 && c >= 0) {
-        const T *gr = g + (int64_t)r * ldg;
-        const T *xr = x + (int64_t)c * ldx;
-        if constexpr (VEC == 1) {
-            for (int j = 0; j < nrhs; ++j) s += __ldg(&gr[j]) * __ldg(&xr[j]);
-        } else if constexpr (sizeof(T) == 4) {
-            T s2 = T(0);
-            for (int j = 0; j < nrhs; j += 4) {
-                const float4 a = __ldg(reinterpret_cast<const float4 *>(gr + j));
-                const float4 b = __ldg(reinterpret_cast<const float4 *>(xr + j));
-                s = fma(a.x, b.x, s);
-                s2 = fma(a.y, b.y, s2);
-                s = fma(a.z, b.z, s);
-                s2 = fma(a.w, b.w, s2);
+// LP lanes per value slot (a power of two): lane `sub` of a slot takes the
+// VEC-wide pieces sub, sub + LP, ... of the nrhs right-hand sides (one 16-byte
+// vector load per piece when both rows are aligned to it, VEC = 1 otherwise),
+// and the LP partial sums meet by shuffles.  With LP * VEC covering a 32-byte
+// row, one warp instruction reads whole sectors of g and x.  Each thread
+// carries U slots (a block step covers U runs of 256 / LP consecutive slots)
+// so that U times as many g and x rows are in flight, and the grid holds only
+// as many blocks as are resident at once, striding over the slots: the kernel
+// is bound by the latency of its gathers and, with one short block per few
+// slots, by block launches.
+template <typename T, int VEC, int LP, int U>
+__global__ void __launch_bounds__(256)
+    cb_grad_vals_kernel(int64_t nvals, const int32_t *__restrict__ vrow,
+                        const int32_t *__restrict__ vcol, const T *__restrict__ g,
+                        int64_t ldg, const T *__restrict__ x, int64_t ldx, int nrhs,
+                        T *__restrict__ out) {
+    constexpr int VPB = 256 / LP;  // slots per block and step
+    const int sub = (int)threadIdx.x % LP;
+    for (int64_t step = blockIdx.x; step * VPB * U < nvals; step += gridDim.x) {
+        const int64_t v0 = step * VPB * U + threadIdx.x / LP;
+        int32_t r[U], c[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int64_t v = v0 + (int64_t)u * VPB;
+            r[u] = v < nvals ? __ldg(&vrow[v]) : -1;
+            c[u] = v < nvals ? __ldg(&vcol[v]) : -1;
+            if (c[u] < 0) r[u] = -1;  // dense padding: gradient 0
+        }
+        T s[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) s[u] = T(0);
+        for (int j = sub * VEC; j < nrhs; j += LP * VEC) {
+            T a[U][VEC], b[U][VEC];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const T *gr = g + (int64_t)max(r[u], 0) * ldg + j;
+                const T *xr = x + (int64_t)max(c[u], 0) * ldx + j;
+                if (r[u] < 0) {
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) a[u][q] = b[u][q] = T(0);
+                } else if constexpr (VEC == 1) {
+                    a[u][0] = __ldg(gr);
+                    b[u][0] = __ldg(xr);
+                } else if constexpr (sizeof(T) == 4) {
+                    const float4 fa = __ldg(reinterpret_cast<const float4 *>(gr));
+                    const float4 fb = __ldg(reinterpret_cast<const float4 *>(xr));
+                    a[u][0] = fa.x, a[u][1] = fa.y, a[u][2] = fa.z, a[u][3] = fa.w;
+                    b[u][0] = fb.x, b[u][1] = fb.y, b[u][2] = fb.z, b[u][3] = fb.w;
+                } else {
+                    const double2 da = __ldg(reinterpret_cast<const double2 *>(gr));
+                    const double2 db = __ldg(reinterpret_cast<const double2 *>(xr));
+                    a[u][0] = da.x, a[u][1] = da.y;
+                    b[u][0] = db.x, b[u][1] = db.y;
+                }
             }
-            s += s2;
-        } else {
-            T s2 = T(0);
-            for (int j = 0; j < nrhs; j += 2) {
-                const double2 a = __ldg(reinterpret_cast<const double2 *>(gr + j));
-                const double2 b = __ldg(reinterpret_cast<const double2 *>(xr + j));
-                s = fma(a.x, b.x, s);
-                s2 = fma(a.y, b.y, s2);
-            }
-            s += s2;
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) s[u] = fma(a[u][q], b[u][q], s[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+#pragma unroll
+            for (int o = LP / 2; o > 0; o >>= 1) s[u] += __shfl_xor_sync(kFull, s[u], o);
+            const int64_t v = v0 + (int64_t)u * VPB;
+            if (sub == 0 && v < nvals) out[v] = s[u];
         }
     }
-    out[v] = s;
 }
 
 template <typename T, int BS, int CH>
@@ -888,34 +916,53 @@ cudaError_t launch_set_values(int f32, int64_t nvals, const int64_t *vsrc_ptr,
     return cudaGetLastError();
 }
 
+template <typename T, int V>
+void grad_vals_go(int lp, int64_t nvals, const int32_t *vrow, const int32_t *vcol,
+                  const void *g, int64_t ldg, const void *x, int64_t ldx, int nrhs,
+                  void *gvals, cudaStream_t st) {
+    constexpr int U = 4;
+    const T *gp = static_cast<const T *>(g), *xp = static_cast<const T *>(x);
+    T *op = static_cast<T *>(gvals);
+    const int li = lp == 1 ? 0 : lp == 2 ? 1 : lp == 4 ? 2 : 3;
+    void (*const kerns[4])(int64_t, const int32_t *, const int32_t *, const T *, int64_t,
+                           const T *, int64_t, int, T *) = {
+        cb_grad_vals_kernel<T, V, 1, U>, cb_grad_vals_kernel<T, V, 2, U>,
+        cb_grad_vals_kernel<T, V, 4, U>, cb_grad_vals_kernel<T, V, 8, U>};
+    auto kern = kerns[li];
+    static int resident[4] = {0, 0, 0, 0};  // blocks per SM, per instantiation
+    static int sms = 0;
+    if (!resident[li]) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        int r = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, kern, 256, 0);
+        resident[li] = r < 1 ? 1 : r;
+    }
+    const int64_t per_block = 256 / lp * U;
+    const int64_t grid = std::min<int64_t>((nvals + per_block - 1) / per_block,
+                                           (int64_t)sms * resident[li]);
+    kern<<<(unsigned)grid, 256, 0, st>>>(nvals, vrow, vcol, gp, ldg, xp, ldx, nrhs, op);
+}
+
 cudaError_t launch_grad_vals(int f32, int64_t nvals, const int32_t *vrow,
                              const int32_t *vcol, const void *g, int64_t ldg,
                              const void *x, int64_t ldx, int nrhs, void *gvals,
                              cudaStream_t stream) {
     if (nvals == 0) return cudaSuccess;
-    const unsigned grid = (unsigned)((nvals + 255) / 256);
     const int vec = f32 ? 4 : 2;
     const bool vok = nrhs % vec == 0 && ldg % vec == 0 && ldx % vec == 0 &&
                      reinterpret_cast<uintptr_t>(g) % 16 == 0 &&
                      reinterpret_cast<uintptr_t>(x) % 16 == 0;
+    const int pieces = vok ? nrhs / vec : nrhs;
+    int lp = 1;  // lanes per value slot
+    while (lp < pieces && lp < 8) lp *= 2;
     if (f32) {
-        const float *gp = static_cast<const float *>(g), *xp = static_cast<const float *>(x);
-        float *op = static_cast<float *>(gvals);
-        if (vok)
-            cb_grad_vals_kernel<float, 4><<<grid, 256, 0, stream>>>(nvals, vrow, vcol, gp, ldg, xp,
-                                                                   ldx, nrhs, op);
-        else
-            cb_grad_vals_kernel<float, 1><<<grid, 256, 0, stream>>>(nvals, vrow, vcol, gp, ldg, xp,
-                                                                   ldx, nrhs, op);
+        (vok ? grad_vals_go<float, 4> : grad_vals_go<float, 1>)(lp, nvals, vrow, vcol, g, ldg,
+                                                                x, ldx, nrhs, gvals, stream);
     } else {
-        const double *gp = static_cast<const double *>(g), *xp = static_cast<const double *>(x);
-        double *op = static_cast<double *>(gvals);
-        if (vok)
-            cb_grad_vals_kernel<double, 2><<<grid, 256, 0, stream>>>(nvals, vrow, vcol, gp, ldg,
-                                                                    xp, ldx, nrhs, op);
-        else
-            cb_grad_vals_kernel<double, 1><<<grid, 256, 0, stream>>>(nvals, vrow, vcol, gp, ldg,
-                                                                    xp, ldx, nrhs, op);
+        (vok ? grad_vals_go<double, 2> : grad_vals_go<double, 1>)(lp, nvals, vrow, vcol, g, ldg,
+                                                                  x, ldx, nrhs, gvals, stream);
     }
     note_launch();
     return cudaGetLastError();

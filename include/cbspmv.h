@@ -197,6 +197,18 @@ cbspmv_status cbspmv_grad_vals(cbspmv_plan *plan, const void *g,
                                const void *x, void *gvals, int nrhs,
                                int64_t ldg, int64_t ldx, void *stream);
 
+/* The whole backward pass of Y = A X for one upstream gradient g: gx = A^T g
+ * (when gx is not NULL; needs want_transpose) and the value gradient gvals
+ * (when gvals is not NULL), as cbspmv_spmv_t and cbspmv_grad_vals compute
+ * them.  The two are independent, so the value gradient runs on a second
+ * stream of the plan's own, forked from and joined back to `stream` by
+ * events: work issued to `stream` afterwards sees both results, and the call
+ * can be captured in a CUDA graph.  The first call with both outputs creates
+ * that stream and its events. */
+cbspmv_status cbspmv_adjoint(cbspmv_plan *plan, const void *g, const void *x,
+                             void *gx, void *gvals, int nrhs, int64_t ldg,
+                             int64_t ldx, int64_t ldgx, void *stream);
+
 /* Stored values: the plan's packed value slots, in device (tile) order.
  * Dense blocks store all bs*bs values, so there can be more slots than input
  * nonzeros; COO blocks merge duplicates (coo2block.h:249-255), so there can

@@ -14,7 +14,7 @@ def _plan(coo, f32=False, **kw):
 
 @pytest.mark.parametrize("bs", [16, 32])
 @pytest.mark.parametrize("f32", [False, True])
-@pytest.mark.parametrize("nrhs", [1, 4])
+@pytest.mark.parametrize("nrhs", [1, 3, 4, 8, 16, 33])
 def test_transpose_and_value_gradient(cuda, bs, f32, nrhs):
     import torch
     import cbdump as cd
@@ -40,6 +40,57 @@ def test_transpose_and_value_gradient(cuda, bs, f32, nrhs):
     want = cd.oracle_grad_vals(coo, G, X)
     scale = np.sum(np.abs(G[:, coo.row] * X[:, coo.col]), axis=0)
     assert np.all(np.abs(gin - want) <= tol * scale + 1e-300)
+    # the combined call runs the same kernels: identical results
+    gx2, gv2 = plan.adjoint(gd, xd)
+    torch.cuda.synchronize()
+    assert np.array_equal(gx2.cpu().numpy().reshape(coo.n, nrhs).T, gx)
+    assert np.array_equal(gv2.cpu().numpy().astype(np.float64), gv)
+
+
+def test_adjoint_streams_graph_and_errors(cuda):
+    """cbspmv_adjoint: the value gradient's second stream joins back before
+    work issued later on the caller's stream; captured in a CUDA graph it
+    replays with new inputs; bad calls return statuses."""
+    import torch
+    import cbspmv
+    from cbspmv import gen
+    coo = gen.power_law(20000, kmax=4000, band=512, seed=8, mean=20)
+    plan = _plan(coo, True)
+    k = 8
+    g = torch.rand(coo.m, k, device=cuda)
+    x = torch.rand(coo.n, k, device=cuda)
+    gx_ref, gv_ref = plan.spmv_t(g), plan.grad_vals(g, x)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        gx, gv = plan.adjoint(g, x, stream=s)
+        both = torch.cat([gx.flatten(), gv])  # ordered after both outputs
+    s.synchronize()
+    assert torch.equal(both, torch.cat([gx_ref.flatten(), gv_ref]))
+    gx.zero_()
+    gv.zero_()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        plan.adjoint(g, x, gx, gv)
+    for seed in range(2):
+        torch.manual_seed(seed)
+        g.copy_(torch.rand_like(g))
+        x.copy_(torch.rand_like(x))
+        graph.replay()
+        torch.cuda.synchronize()
+        assert torch.equal(gx, plan.spmv_t(g))
+        assert torch.equal(gv, plan.grad_vals(g, x))
+    del graph
+    only_v = plan.adjoint(g, x, want_gx=False)
+    assert only_v[0] is None and torch.equal(only_v[1], plan.grad_vals(g, x))
+    with pytest.raises(cbspmv.CBSpMVError) as e:
+        plan.adjoint(g, x, want_gx=False, want_gvals=False)
+    assert e.value.status == "INVALID"
+    no_t = cbspmv.Plan(coo, value_type=1)
+    with pytest.raises(cbspmv.CBSpMVError) as e:
+        no_t.adjoint(g, x)
+    assert e.value.status == "STATE"
+    assert no_t.adjoint(g, x, want_gx=False)[1].shape == (no_t.num_values(),)
 
 
 def test_gradcheck_small(cuda):
