@@ -47,6 +47,32 @@ def test_transpose_and_value_gradient(cuda, bs, f32, nrhs):
     assert np.array_equal(gv2.cpu().numpy().astype(np.float64), gv)
 
 
+@pytest.mark.parametrize("f32", [False, True])
+@pytest.mark.parametrize("nrhs", [1, 8, 33])
+def test_value_gradient_sparse_rows(cuda, f32, nrhs):
+    """About one stored value per row: a block of the value-gradient kernel
+    sees more g rows than it stages in shared memory and reads g directly."""
+    import torch
+    import cbdump as cd
+    from cbspmv import gen
+    rng = np.random.default_rng(12)
+    coo = gen.random_small(rng, 5000, 4000, 5000)
+    plan = _plan(coo, f32)
+    dt = torch.float32 if f32 else torch.float64
+    tol = 1e-5 if f32 else 1e-12
+    G = gen.uniform_x(coo.m, 31, nrhs=max(nrhs, 2))[:nrhs]
+    X = gen.uniform_x(coo.n, 32, nrhs=max(nrhs, 2))[:nrhs]
+    if f32:
+        G = G.astype(np.float32).astype(np.float64)
+        X = X.astype(np.float32).astype(np.float64)
+    gd = torch.from_numpy(np.ascontiguousarray(G.T)).to(cuda, dt)
+    xd = torch.from_numpy(np.ascontiguousarray(X.T)).to(cuda, dt)
+    gv = plan.grad_vals(gd, xd).cpu().numpy().astype(np.float64)
+    want = cd.oracle_grad_vals(coo, G, X)
+    scale = np.sum(np.abs(G[:, coo.row] * X[:, coo.col]), axis=0)
+    assert np.all(np.abs(gv[plan.input_slots()] - want) <= tol * scale + 1e-300)
+
+
 def test_adjoint_streams_graph_and_errors(cuda):
     """cbspmv_adjoint: the value gradient's second stream joins back before
     work issued later on the caller's stream; captured in a CUDA graph it
