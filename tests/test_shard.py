@@ -1,0 +1,138 @@
+"""Block-row sharding of one matrix (cbspmv.shard): the cuts, the split of a
+rank's rows into own and halo columns, and the padded all-gather layout,
+checked on CPU against the oracle's SpMV (tests/cbdump.py); the exchange
+itself between two gloo ranks; the per-rank plans on the GPU with the ranks
+run one after another in one process (their all-gathered x laid out by
+hand, no collective)."""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+
+def _cases():
+    from cbspmv import gen
+    rng = np.random.default_rng(9)
+    return [("pl", gen.power_law(6000, kmax=3000, band=300, seed=5, mean=12)),
+            ("lap", gen.laplacian_2d(40, 50)),
+            ("rect", gen.random_small(rng, 700, 1300, 9000)),
+            ("tiny", gen.random_small(rng, 20, 20, 60))]
+
+
+CASES = _cases()
+
+
+def _x_all(coo, cb, x):
+    """The padded all-gather layout of x (ranges of length L end to end)."""
+    L = int(np.max(np.diff(cb)))
+    out = np.zeros((len(cb) - 1) * L)
+    for s in range(len(cb) - 1):
+        out[s * L: s * L + cb[s + 1] - cb[s]] = x[cb[s]:cb[s + 1]]
+    return out
+
+
+@pytest.mark.parametrize("name,coo", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("world", [1, 2, 3, 8])
+@pytest.mark.parametrize("bs", [16, 32])
+def test_cuts_split_and_layout(name, coo, world, bs):
+    import cbdump as cd
+    from cbspmv import shard
+    rb = shard.block_row_bounds(coo, world, bs)
+    assert rb[0] == 0 and rb[-1] == coo.m and np.all(np.diff(rb) >= 0)
+    assert all(c % bs == 0 or c == coo.m for c in rb)
+    # balance: each part within one block row's stored values of nnz / world
+    per_br = np.bincount(coo.row // bs, minlength=(coo.m + bs - 1) // bs)
+    counts = np.diff(np.searchsorted(coo.row, rb))
+    assert np.all(np.abs(counts - coo.nnz / world) <= per_br.max() + 1)
+    cb = rb if coo.m == coo.n else shard.even_bounds(coo.n, world, bs)
+    assert cb[0] == 0 and cb[-1] == coo.n and np.all(np.diff(cb) >= 0)
+    x = np.random.default_rng(1).uniform(-1, 1, coo.n)
+    xa = _x_all(coo, cb, x)
+    yref = cd.oracle_spmv(coo, x)
+    for r in range(world):
+        rows = shard.rows_of(coo, rb[r], rb[r + 1])
+        own, halo = shard.split_columns(rows, cb, r)
+        assert own.nnz + halo.nnz == rows.nnz
+        assert np.all(np.diff(own.row) >= 0) and np.all(np.diff(halo.row) >= 0)
+        y = cd.oracle_spmv(own, x[cb[r]:cb[r + 1]]) + cd.oracle_spmv(halo, xa)
+        assert np.allclose(y, yref[rb[r]:rb[r + 1]], rtol=1e-12, atol=1e-12)
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _rank(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port),
+                      WORLD_SIZE=str(world), RANK=str(rank), LOCAL_RANK=str(rank))
+    import sys
+    import pathlib
+    repo = pathlib.Path(__file__).resolve().parent.parent
+    sys.path.insert(0, str(repo / "cb-sparse-dcu_b200"))
+    sys.path.insert(0, str(repo / "tests"))
+    import torch
+    import torch.distributed as dist
+    import cbdump as cd
+    from cbspmv import gen, shard
+    dist.init_process_group("gloo", timeout=__import__("datetime").timedelta(seconds=60))
+    coo = gen.power_law(5000, kmax=2500, band=200, seed=6, mean=10)
+    sh = shard.RowShard(coo, world, rank)  # builds both plans on the host
+    x = np.random.default_rng(2).uniform(-1, 1, coo.n)
+    piece = sh.pad(torch.from_numpy(x[sh.c0:sh.c1].copy()))
+    x_all = torch.empty(world * sh.L, dtype=piece.dtype)
+    dist.all_gather_into_tensor(x_all, piece)
+    y = cd.oracle_spmv(sh.own_coo, x[sh.c0:sh.c1])
+    if sh.halo is not None:
+        y = y + cd.oracle_spmv(sh.halo_coo, x_all.numpy())
+    ok = np.allclose(y, cd.oracle_spmv(coo, x)[sh.r0:sh.r1], rtol=1e-12, atol=1e-12)
+    dist.barrier()
+    dist.destroy_process_group()
+    out.put((rank, bool(ok), sh.halo is not None))
+
+
+@pytest.mark.timeout(180)
+def test_two_ranks_exchange_x():
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=150) for _ in procs)
+    for p in procs:
+        p.join(timeout=30)
+        assert p.exitcode == 0
+    assert [r[1] for r in res] == [True, True]
+    assert any(r[2] for r in res)  # the halo part was exercised
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,coo", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("world", [1, 3])
+@pytest.mark.parametrize("f32", [False, True])
+@pytest.mark.parametrize("nrhs", [1, 4])
+def test_row_shards_on_gpu(cuda, name, coo, world, f32, nrhs):
+    import torch
+    import cbdump as cd
+    from cbspmv import gen, shard
+    dt = torch.float32 if f32 else torch.float64
+    X = gen.uniform_x(coo.n, 3, nrhs=max(nrhs, 2))[:nrhs]
+    if f32:
+        X = X.astype(np.float32).astype(np.float64)
+    yref, ab = cd.oracle_spmm_ld(coo, X)
+    shards = [shard.RowShard(coo, world, r, value_type=int(f32)) for r in range(world)]
+    xd = torch.from_numpy(np.ascontiguousarray(X.T)).to(cuda, dt)
+    if nrhs == 1:
+        xd = xd[:, 0].contiguous()
+    x_all = torch.cat([s.pad(xd[s.c0:s.c1]) for s in shards]) if world > 1 else None
+    ys = [s.spmv(xd[s.c0:s.c1].contiguous(), x_all=x_all) for s in shards]
+    torch.cuda.synchronize()
+    y = torch.cat(ys).cpu().numpy().reshape(coo.m, nrhs).T
+    tol = 1e-5 if f32 else 1e-12
+    assert np.all(np.abs(y - yref) <= tol * ab + 1e-300)
