@@ -4,17 +4,23 @@ Rank r owns rows [rb[r], rb[r+1]) of A, cut on block-row boundaries so that
 every rank holds about the same number of stored values, and the entries
 [cb[r], cb[r+1]) of x (the same cuts when A is square).  y = A x on rank r
 needs x at the columns its rows use: its own entries plus a halo held by the
-other ranks.  Its rows' matrix is split into
+other ranks.  x travels by one all-gather (NCCL over NVLink on GPUs, gloo on
+CPUs) of each rank's x range padded to the longest range (equal pieces), so
+x_all holds range s at s * L.  Two ways to run a rank's rows:
 
-* A_own: the columns it owns, renumbered to its x range, and
-* A_halo: every other column, renumbered into the all-gathered x (each rank's
-  x range padded to the longest range, so the all-gather moves equal pieces).
+* one plan (default): every column renumbered into x_all; the all-gather,
+  then one SpMV.  The CB build gathers each block row's columns, so the
+  scattered columns of other ranks cost no more than they do unsharded.
+* own + halo (overlap=True): A_own (the rank's own columns, renumbered to its
+  x range) runs while the all-gather is in flight, then A_halo (every other
+  column, renumbered into x_all) is added.  The overlap pays only when the
+  halo is a small, clustered part of the rows: widely scattered halo columns
+  make a plan of nearly one-value blocks, and the second launch and the sum
+  cost more than the exchange they hide.
 
-A step starts the all-gather of x (asynchronous; NCCL over NVLink on GPUs,
-gloo on CPUs), computes y = A_own x_own while it is in flight, waits for it,
-and adds A_halo x_all.  No reduction on y is needed: each rank's rows are its
-own.  Both parts are ordinary CB plans (the reference's coo2block_gather +
-cb_spmv per rank), so each rank keeps the single-GPU kernels unchanged.
+No reduction on y is needed: each rank's rows are its own.  Every part is an
+ordinary CB plan (the reference's coo2block_gather + cb_spmv per rank), so a
+rank runs the single-GPU kernels unchanged.
 """
 from __future__ import annotations
 
@@ -75,16 +81,27 @@ def split_columns(rows: Coo, cb: np.ndarray, rank: int):
     return a, h
 
 
+def padded_columns(rows: Coo, cb: np.ndarray) -> Coo:
+    """One rank's rows with every column renumbered into the padded
+    all-gather layout (range s at s * L)."""
+    L = int(np.max(np.diff(cb)))
+    col = rows.col.astype(np.int64)
+    s = np.searchsorted(cb, col, side="right") - 1
+    return Coo(rows.m, (len(cb) - 1) * L, rows.row.copy(),
+               (s * L + (col - cb[s])).astype(np.int32), rows.val.copy())
+
+
 class RowShard:
     """One rank's share of y = A x: plans for A_own and A_halo.
 
     coo: the whole matrix (every rank passes the same one and keeps its own
     rows); bounds: row cuts (default: block_row_bounds); cbounds: x cuts
-    (default: the row cuts when A is square, else even_bounds).  Plan
-    options (block_size, value_type, ...) pass through to both plans."""
+    (default: the row cuts when A is square, else even_bounds); overlap:
+    own + halo plans instead of one.  Plan options (block_size, value_type,
+    ...) pass through to the plans."""
 
     def __init__(self, coo: Coo, world: int, rank: int, bounds=None, cbounds=None,
-                 **plan_opts):
+                 overlap: bool = False, **plan_opts):
         from . import Plan
         bs = int(plan_opts.get("block_size", 16) or 16)
         self.world, self.rank = world, rank
@@ -97,11 +114,19 @@ class RowShard:
         self.c0, self.c1 = int(self.cbounds[rank]), int(self.cbounds[rank + 1])
         self.L = int(np.max(np.diff(self.cbounds)))
         self.m, self.n = coo.m, coo.n
-        own, halo = split_columns(rows_of(coo, self.r0, self.r1), self.cbounds, rank)
-        self.own_coo, self.halo_coo = own, halo
-        self.own = Plan(own, **plan_opts)
-        self.halo = Plan(halo, **plan_opts) if halo.nnz else None
-        self.f32 = self.own.f32
+        self.overlap = bool(overlap) and world > 1
+        rows = rows_of(coo, self.r0, self.r1)
+        self.own = self.halo = self.full = None
+        if self.overlap:
+            own, halo = split_columns(rows, self.cbounds, rank)
+            self.own_coo, self.halo_coo = own, halo
+            self.own = Plan(own, **plan_opts)
+            self.halo = Plan(halo, **plan_opts) if halo.nnz else None
+            self.f32 = self.own.f32
+        else:
+            self.full_coo = padded_columns(rows, self.cbounds) if world > 1 else rows
+            self.full = Plan(self.full_coo, **plan_opts)
+            self.f32 = self.full.f32
 
     def pad(self, x_own):
         """This rank's x range padded to L rows (the all-gather piece)."""
@@ -132,9 +157,13 @@ class RowShard:
             x_all = torch.empty((self.world * self.L,) + tuple(piece.shape[1:]),
                                 dtype=piece.dtype, device=piece.device)
             work = dist.all_gather_into_tensor(x_all, piece, group=group, async_op=True)
+        if self.full is not None:
+            if work is not None:
+                work.wait()  # the current stream waits for the gathered x
+            return self.full.spmv(x_own if self.world == 1 else x_all, y)
         self.own.spmv(x_own, y)
         if work is not None:
-            work.wait()  # the current stream waits for the gathered x
+            work.wait()
         if self.halo is not None:
             y.add_(self.halo.spmv(x_all))
         return y

@@ -57,6 +57,9 @@ def test_cuts_split_and_layout(name, coo, world, bs):
         assert np.all(np.diff(own.row) >= 0) and np.all(np.diff(halo.row) >= 0)
         y = cd.oracle_spmv(own, x[cb[r]:cb[r + 1]]) + cd.oracle_spmv(halo, xa)
         assert np.allclose(y, yref[rb[r]:rb[r + 1]], rtol=1e-12, atol=1e-12)
+        full = shard.padded_columns(rows, cb)
+        assert np.allclose(cd.oracle_spmv(full, xa), yref[rb[r]:rb[r + 1]],
+                           rtol=1e-12, atol=1e-12)
 
 
 def _free_port():
@@ -81,15 +84,21 @@ def _rank(rank, world, port, out):
     from cbspmv import gen, shard
     dist.init_process_group("gloo", timeout=__import__("datetime").timedelta(seconds=60))
     coo = gen.power_law(5000, kmax=2500, band=200, seed=6, mean=10)
-    sh = shard.RowShard(coo, world, rank)  # builds both plans on the host
     x = np.random.default_rng(2).uniform(-1, 1, coo.n)
-    piece = sh.pad(torch.from_numpy(x[sh.c0:sh.c1].copy()))
-    x_all = torch.empty(world * sh.L, dtype=piece.dtype)
-    dist.all_gather_into_tensor(x_all, piece)
-    y = cd.oracle_spmv(sh.own_coo, x[sh.c0:sh.c1])
-    if sh.halo is not None:
-        y = y + cd.oracle_spmv(sh.halo_coo, x_all.numpy())
-    ok = np.allclose(y, cd.oracle_spmv(coo, x)[sh.r0:sh.r1], rtol=1e-12, atol=1e-12)
+    want = cd.oracle_spmv(coo, x)
+    ok = True
+    for overlap in (False, True):  # the plans are built on the host
+        sh = shard.RowShard(coo, world, rank, overlap=overlap)
+        piece = sh.pad(torch.from_numpy(x[sh.c0:sh.c1].copy()))
+        x_all = torch.empty(world * sh.L, dtype=piece.dtype)
+        dist.all_gather_into_tensor(x_all, piece)
+        if overlap:
+            y = cd.oracle_spmv(sh.own_coo, x[sh.c0:sh.c1])
+            if sh.halo is not None:
+                y = y + cd.oracle_spmv(sh.halo_coo, x_all.numpy())
+        else:
+            y = cd.oracle_spmv(sh.full_coo, x_all.numpy())
+        ok = ok and np.allclose(y, want[sh.r0:sh.r1], rtol=1e-12, atol=1e-12)
     dist.barrier()
     dist.destroy_process_group()
     out.put((rank, bool(ok), sh.halo is not None))
@@ -117,7 +126,8 @@ def test_two_ranks_exchange_x():
 @pytest.mark.parametrize("world", [1, 3])
 @pytest.mark.parametrize("f32", [False, True])
 @pytest.mark.parametrize("nrhs", [1, 4])
-def test_row_shards_on_gpu(cuda, name, coo, world, f32, nrhs):
+@pytest.mark.parametrize("overlap", [False, True])
+def test_row_shards_on_gpu(cuda, name, coo, world, f32, nrhs, overlap):
     import torch
     import cbdump as cd
     from cbspmv import gen, shard
@@ -126,7 +136,8 @@ def test_row_shards_on_gpu(cuda, name, coo, world, f32, nrhs):
     if f32:
         X = X.astype(np.float32).astype(np.float64)
     yref, ab = cd.oracle_spmm_ld(coo, X)
-    shards = [shard.RowShard(coo, world, r, value_type=int(f32)) for r in range(world)]
+    shards = [shard.RowShard(coo, world, r, overlap=overlap, value_type=int(f32))
+              for r in range(world)]
     xd = torch.from_numpy(np.ascontiguousarray(X.T)).to(cuda, dt)
     if nrhs == 1:
         xd = xd[:, 0].contiguous()
