@@ -191,8 +191,41 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
                 }
             }
 
-            // CSR and DENSE blocks
-            for (int jb = 0; jb < nxt; ++jb) {
+            // CSR and DENSE blocks.  bs = 16: each half-warp takes a block,
+            // one lane per row, so two blocks' dependent load chains (row
+            // pointers, then columns and values) are in flight at a time.
+            if (BS == 16) {
+                for (int jb = 0; jb < nxt; jb += 2) {
+                    const int j = jb + (lane >> 4);
+                    const int jc = min(j, nxt - 1);
+                    const uint32_t off = __shfl_sync(kFull, bd.x, jc);
+                    const uint32_t mb = __shfl_sync(kFull, bd.y, jc);
+                    if (j < nxt) {
+                        const int k = (mb >> 3) & 2047;
+                        const uint8_t *pb = base + off;
+                        const T *xt = &S.xt[j * BS];
+                        const int row = lane & 15;
+                        T sum = T(0);
+                        if ((mb & 3) == 1) {
+                            const uint8_t *rp = pb;
+                            const uint8_t *ci = rp + BS + 1;
+                            const T *vv = reinterpret_cast<const T *>(
+                                pb + a16((uint32_t)(BS + 1 + k)));
+                            const int kb = __ldg(&rp[row]), ke = __ldg(&rp[row + 1]);
+#pragma unroll 4
+                            for (int q = kb; q < ke; ++q)
+                                sum += (unit ? T(1) : __ldg(&vv[q])) * xt[__ldg(&ci[q])];
+                        } else {
+#pragma unroll
+                            for (int c = 0; c < BS; ++c)
+                                sum += dense_at<T, BS>(pb, unit, row, (c + row) & 15) *
+                                       xt[(c + row) & 15];
+                        }
+                        myacc[row * 32] += sum;
+                    }
+                }
+            }
+            for (int jb = 0; BS != 16 && jb < nxt; ++jb) {
                 const uint32_t off = __shfl_sync(kFull, bd.x, jb);
                 const uint32_t mb = __shfl_sync(kFull, bd.y, jb);
                 const int k = (mb >> 3) & 2047;
@@ -711,14 +744,17 @@ cudaError_t launch_chunk(const DevLayout &d, const void *x, void *y, int nrhs,
     return cudaGetLastError();
 }
 
-int chunk_choice(int vsz) {
+// COO entries per lane in flight in the direct kernel: 4 for both value
+// types (measured fastest on CSR-heavy matrices; 6 and 8 also spill in
+// FP64); CBSPMV_CHUNK=4|6|8 overrides it for tuning.
+int chunk_choice() {
     static int forced = -1;
     if (forced < 0) {
         const char *e = std::getenv("CBSPMV_CHUNK");
         forced = e ? std::atoi(e) : 0;
     }
     if (forced == 4 || forced == 6 || forced == 8) return forced;
-    return vsz == 8 ? 6 : 8;
+    return 4;
 }
 
 template <typename T, int BS>
@@ -793,7 +829,7 @@ cudaError_t launch_tiles(const DevLayout &d, const void *x, void *y, int nrhs,
     if (nrhs == 1 && ldx == 1 && ldy == 1 && use_stream(d))
         return launch_stream<T, BS>(d, x, y, stream);
     if (nrhs > 1 || d.kernel == 3) return launch_spmm(d, x, y, nrhs, ldx, ldy, stream);
-    switch (chunk_choice(sizeof(T))) {
+    switch (chunk_choice()) {
         case 4: return launch_chunk<T, BS, 4>(d, x, y, nrhs, ldx, ldy, stream);
         case 6: return launch_chunk<T, BS, 6>(d, x, y, nrhs, ldx, ldy, stream);
         default: return launch_chunk<T, BS, 8>(d, x, y, nrhs, ldx, ldy, stream);
