@@ -195,7 +195,24 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
             // one lane per row, so two blocks' dependent load chains (row
             // pointers, then columns and values) are in flight at a time.
             if (BS == 16) {
+                // the blocks of pair jb2 into L1, one 128-byte line per lane of
+                // a block's half-warp, a pair ahead of their reads
+                auto prefetch = [&](int jb2) {
+                    const int j2 = jb2 + (lane >> 4);
+                    const int j2c = min(j2, nxt - 1);
+                    const uint32_t off2 = __shfl_sync(kFull, bd.x, j2c);
+                    const uint32_t mb2 = __shfl_sync(kFull, bd.y, j2c);
+                    if (j2 >= nxt) return;
+                    const uint32_t k2 = (mb2 >> 3) & 2047;
+                    const uint32_t bytes = (mb2 & 3) == 1
+                        ? a16(BS + 1 + k2) + (unit ? 0u : k2 * (uint32_t)sizeof(T))
+                        : (unit ? BS * BS / 8u : BS * BS * (uint32_t)sizeof(T));
+                    for (uint32_t b = (uint32_t)(lane & 15) * 128u; b < bytes; b += 16u * 128u)
+                        asm volatile("prefetch.global.L1 [%0];" ::"l"(base + off2 + b));
+                };
+                prefetch(0);
                 for (int jb = 0; jb < nxt; jb += 2) {
+                    prefetch(jb + 2);
                     const int j = jb + (lane >> 4);
                     const int jc = min(j, nxt - 1);
                     const uint32_t off = __shfl_sync(kFull, bd.x, jc);
