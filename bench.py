@@ -254,6 +254,24 @@ def diff_config(dev, peak, flush, out):
         "adj_gbs": round(adj_bytes / t_a / 1e6, 1),
         "gflops_fwd": round(2 * coo.nnz * k / t_f / 1e6, 1), "l2": "flushed before each step"}
     del plan
+    # library comparator for the forward: cuSPARSE SpMM (CSR, int32 indices)
+    try:
+        import warnings
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")
+            idx = torch.from_numpy(np.stack([coo.row, coo.col]).astype(np.int64))
+            A = torch.sparse_coo_tensor(idx, torch.from_numpy(coo.val.astype(np.float32)),
+                                        (coo.m, coo.n)).coalesce().to_sparse_csr()
+            A = torch.sparse_csr_tensor(A.crow_indices().to(torch.int32),
+                                        A.col_indices().to(torch.int32), A.values(),
+                                        A.shape).to(dev)
+            t_c = _timed(lambda: torch.mm(A, X), 30, 5, flush)
+        out["DIFF fp32 (n=2^18, 8 rhs)"]["comparator"] = {
+            "library": "cuSPARSE SpMM via torch.mm (CSR, FP32, int32 indices)",
+            "fwd_ms": round(t_c, 4), "this_library_speedup": round(t_c / t_f, 2)}
+        del A
+    except Exception as exc:  # informative only
+        out["DIFF fp32 (n=2^18, 8 rhs)"]["comparator"] = {"unavailable": str(exc)[:200]}
 
 
 def bat_config(dev, peak, count, out):
