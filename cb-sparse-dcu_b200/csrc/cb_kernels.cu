@@ -39,6 +39,7 @@ namespace {
 std::atomic<int64_t> g_kernel_launches{0};
 
 using dev::a16;
+using dev::add_csr_dense;
 using dev::add_entries;
 using dev::kColMask;
 using dev::dense_at;
@@ -191,83 +192,7 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
                 }
             }
 
-            // CSR and DENSE blocks.  bs = 16: each half-warp takes a block,
-            // one lane per row, so two blocks' dependent load chains (row
-            // pointers, then columns and values) are in flight at a time;
-            // bs = 32: a block at a time.  prefetch(jb2) brings the blocks of
-            // step jb2 into L1, one 128-byte line per lane of a block's
-            // lanes, a step ahead of their reads.
-            auto prefetch = [&](int jb2) {
-                const int j2 = jb2 + lane / BS;
-                const int j2c = min(j2, nxt - 1);
-                const uint32_t off2 = __shfl_sync(kFull, bd.x, j2c);
-                const uint32_t mb2 = __shfl_sync(kFull, bd.y, j2c);
-                if (j2 >= nxt) return;
-                const uint32_t k2 = (mb2 >> 3) & 2047;
-                constexpr uint32_t isz = BS == 16 ? 1u : 2u;
-                const uint32_t bytes = (mb2 & 3) == 1
-                    ? a16((BS + 1 + k2) * isz) + (unit ? 0u : k2 * (uint32_t)sizeof(T))
-                    : (unit ? BS * BS / 8u : BS * BS * (uint32_t)sizeof(T));
-                for (uint32_t b = (uint32_t)(lane % BS) * 128u; b < bytes; b += BS * 128u)
-                    asm volatile("prefetch.global.L1 [%0];" ::"l"(base + off2 + b));
-            };
-            if (nxt) prefetch(0);
-            if (BS == 16) {
-                for (int jb = 0; jb < nxt; jb += 2) {
-                    prefetch(jb + 2);
-                    const int j = jb + (lane >> 4);
-                    const int jc = min(j, nxt - 1);
-                    const uint32_t off = __shfl_sync(kFull, bd.x, jc);
-                    const uint32_t mb = __shfl_sync(kFull, bd.y, jc);
-                    if (j < nxt) {
-                        const int k = (mb >> 3) & 2047;
-                        const uint8_t *pb = base + off;
-                        const T *xt = &S.xt[j * BS];
-                        const int row = lane & 15;
-                        T sum = T(0);
-                        if ((mb & 3) == 1) {
-                            const uint8_t *rp = pb;
-                            const uint8_t *ci = rp + BS + 1;
-                            const T *vv = reinterpret_cast<const T *>(
-                                pb + a16((uint32_t)(BS + 1 + k)));
-                            const int kb = __ldg(&rp[row]), ke = __ldg(&rp[row + 1]);
-#pragma unroll 4
-                            for (int q = kb; q < ke; ++q)
-                                sum += (unit ? T(1) : __ldg(&vv[q])) * xt[__ldg(&ci[q])];
-                        } else {
-#pragma unroll
-                            for (int c = 0; c < BS; ++c)
-                                sum += dense_at<T, BS>(pb, unit, row, (c + row) & 15) *
-                                       xt[(c + row) & 15];
-                        }
-                        myacc[row * 32] += sum;
-                    }
-                }
-            }
-            // bs = 32: a block at a time, one lane per row
-            for (int jb = 0; BS == 32 && jb < nxt; ++jb) {
-                prefetch(jb + 1);
-                const uint32_t off = __shfl_sync(kFull, bd.x, jb);
-                const uint32_t mb = __shfl_sync(kFull, bd.y, jb);
-                const int k = (mb >> 3) & 2047;
-                const uint8_t *pb = base + off;
-                const T *xt = &S.xt[jb * BS];
-                T sum = T(0);
-                if ((mb & 3) == 1) {
-                    const uint16_t *rp = reinterpret_cast<const uint16_t *>(pb);
-                    const uint16_t *ci = rp + BS + 1;
-                    const T *vv = reinterpret_cast<const T *>(
-                        pb + a16((uint32_t)((BS + 1 + k) * sizeof(uint16_t))));
-                    const int kb = __ldg(&rp[lane]), ke = __ldg(&rp[lane + 1]);
-#pragma unroll 4
-                    for (int q = kb; q < ke; ++q)
-                        sum += (unit ? T(1) : __ldg(&vv[q])) * xt[__ldg(&ci[q])];
-                } else {
-#pragma unroll 8
-                    for (int c = 0; c < BS; ++c) sum += dense_at<T, BS>(pb, unit, lane, c) * xt[c];
-                }
-                myacc[lane * 32] += sum;
-            }
+            add_csr_dense<T, BS>(base, bd, nxt, S.xt, myacc, unit, lane);
             __syncwarp();  // xt is rewritten by the next tile
             if (tile + 1 < t1) {
                 ta = na;
