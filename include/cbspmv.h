@@ -204,7 +204,7 @@ cbspmv_status cbspmv_grad_vals(cbspmv_plan *plan, const void *g,
  * stream of the plan's own, forked from and joined back to `stream` by
  * events: work issued to `stream` afterwards sees both results, and the call
  * can be captured in a CUDA graph.  The first call with both outputs creates
- * that stream and its events. */
+ * that stream and its events, so make it before capturing one. */
 cbspmv_status cbspmv_adjoint(cbspmv_plan *plan, const void *g, const void *x,
                              void *gx, void *gvals, int nrhs, int64_t ldg,
                              int64_t ldx, int64_t ldgx, void *stream);
