@@ -7,6 +7,7 @@
 #include <atomic>
 #include <chrono>
 #include <cstring>
+#include <future>
 #include <new>
 #include <numeric>
 #include <string>
@@ -302,28 +303,33 @@ cbspmv_status cbspmv_coo2block_gather(const cbspmv_coo *coo,
     if (!p) return fail(CBSPMV_ERR_ALLOC, "out of host memory");
     p->opts = o;
     try {
-        int code = 0;
-        std::string err = cb::build_cb(to_build(o), coo->m, coo->n, coo->nnz,
-                                       coo->row, coo->col, coo->val, p->host, &code);
-        if (!err.empty()) {
-            delete p;
-            return fail(code, err);
-        }
-        err = cb::build_layout(p->host, o.value_type == CBSPMV_F32, o.tile_entries, o.kernel,
-                               !o.keep_values, p->A.lay, &code);
-        if (!err.empty()) {
-            delete p;
-            return fail(code, err);
-        }
-        if (o.want_transpose) {
+        // A^T (when wanted) is built on a second host thread while A is built
+        // here: the two builds share nothing but the caller's COO, read-only.
+        const int64_t nnz = coo->nnz;
+        std::vector<int32_t> tr, tc, perm;
+        std::vector<double> tv;
+        std::future<std::pair<std::string, int>> side;
+        // (a COO that fails these checks is refused by A's build below)
+        if (o.want_transpose && coo->m >= 0 && coo->n >= 0 && nnz >= 0 &&
+            (nnz == 0 || (coo->row && coo->col && coo->val))) {
             // A^T as a row-sorted COO: a stable counting sort by column keeps
-            // each column's entries in row order.
-            const int64_t nnz = coo->nnz, n = coo->n;
+            // each column's entries in row order.  The input is checked here
+            // (columns in range) before it indexes anything; build_cb checks
+            // the rest of it for A.
+            const int64_t n = coo->n;
+            for (int64_t i = 0; i < nnz; ++i)
+                if (coo->col[i] < 0 || coo->col[i] >= n || coo->row[i] < 0 ||
+                    coo->row[i] >= coo->m) {
+                    delete p;
+                    return fail(CBSPMV_ERR_BOUNDS, "COO index out of range");
+                }
             std::vector<int64_t> cnt(n + 1, 0);
             for (int64_t i = 0; i < nnz; ++i) cnt[coo->col[i] + 1]++;
             for (int64_t c = 0; c < n; ++c) cnt[c + 1] += cnt[c];
-            std::vector<int32_t> tr(nnz), tc(nnz), perm(nnz);
-            std::vector<double> tv(nnz);
+            tr.resize(nnz);
+            tc.resize(nnz);
+            perm.resize(nnz);
+            tv.resize(nnz);
             for (int64_t i = 0; i < nnz; ++i) {
                 const int64_t d = cnt[coo->col[i]]++;
                 tr[d] = coo->col[i];
@@ -331,15 +337,37 @@ cbspmv_status cbspmv_coo2block_gather(const cbspmv_coo *coo,
                 tv[d] = coo->val[i];
                 perm[d] = (int32_t)i;
             }
-            err = cb::build_cb(to_build(o), coo->n, coo->m, nnz, tr.data(), tc.data(),
-                               tv.data(), p->host_t, &code);
-            if (err.empty())
-                err = cb::build_layout(p->host_t, o.value_type == CBSPMV_F32,
-                                       o.tile_entries, o.kernel, !o.keep_values, p->AT.lay,
-                                       &code);
-            if (!err.empty()) {
+            side = std::async(std::launch::async, [&]() -> std::pair<std::string, int> {
+                int c = 0;
+                std::string e = cb::build_cb(to_build(o), coo->n, coo->m, nnz, tr.data(),
+                                             tc.data(), tv.data(), p->host_t, &c);
+                if (e.empty())
+                    e = cb::build_layout(p->host_t, o.value_type == CBSPMV_F32, o.tile_entries,
+                                         o.kernel, !o.keep_values, p->AT.lay, &c);
+                return {e, c};
+            });
+        }
+        int code = 0;
+        std::string err = cb::build_cb(to_build(o), coo->m, coo->n, coo->nnz,
+                                       coo->row, coo->col, coo->val, p->host, &code);
+        if (err.empty())
+            err = cb::build_layout(p->host, o.value_type == CBSPMV_F32, o.tile_entries,
+                                   o.kernel, !o.keep_values, p->A.lay, &code);
+        std::pair<std::string, int> terr;
+        const bool have_t = side.valid();
+        if (have_t) terr = side.get();  // joined before any return
+        if (!err.empty()) {
+            delete p;
+            return fail(code, err);
+        }
+        if (o.want_transpose) {
+            if (!have_t) {  // not reached: A's build refuses such input
                 delete p;
-                return fail(code, "transpose: " + err);
+                return fail(CBSPMV_ERR_INVALID, "transpose: invalid COO");
+            }
+            if (!terr.first.empty()) {
+                delete p;
+                return fail(terr.second, "transpose: " + terr.first);
             }
             // value sources of A^T refer to the caller's nonzero order
             for (int32_t &s : p->AT.lay.vsrc) s = perm[s];

@@ -100,17 +100,16 @@ def test_input_validation():
     from cbspmv.gen import Coo
     bad_order = Coo(4, 4, np.array([1, 0], np.int32), np.array([0, 0], np.int32),
                     np.ones(2))
-    with pytest.raises(cbspmv.CBSpMVError) as e:
-        cbspmv.Plan(bad_order)
-    assert e.value.status == "UNSORTED"
     oob = Coo(4, 4, np.array([0, 4], np.int32), np.array([0, 0], np.int32), np.ones(2))
-    with pytest.raises(cbspmv.CBSpMVError) as e:
-        cbspmv.Plan(oob)
-    assert e.value.status == "BOUNDS"
     neg = Coo(4, 4, np.array([0, 1], np.int32), np.array([-1, 0], np.int32), np.ones(2))
-    with pytest.raises(cbspmv.CBSpMVError) as e:
-        cbspmv.Plan(neg)
-    assert e.value.status == "BOUNDS"
+    big_col = Coo(4, 4, np.array([0, 1], np.int32), np.array([0, 9], np.int32), np.ones(2))
+    # the same answers with A^T built alongside (on its own host thread)
+    for t in (0, 1):
+        for coo, status in ((bad_order, "UNSORTED"), (oob, "BOUNDS"), (neg, "BOUNDS"),
+                            (big_col, "BOUNDS")):
+            with pytest.raises(cbspmv.CBSpMVError) as e:
+                cbspmv.Plan(coo, want_transpose=t)
+            assert e.value.status == status, (t, status)
     ok = Coo(4, 4, np.array([0], np.int32), np.array([0], np.int32), np.ones(1))
     for opt in (dict(block_size=8), dict(block_size=64), dict(dense_sixteenths=0),
                 dict(waves_per_block=0), dict(value_type=2)):
