@@ -27,6 +27,9 @@ configs     the other workloads (LAP, PL FP32, ST FP64/FP32, DIFF forward and
 
 Multi-GPU: every rank runs its own copy of the workload (replicas; SpMV of
 one matrix needs no exchange), weak scaling, timed as the max over ranks.
+--mode shard instead splits the one matrix over the ranks by block rows
+(cbspmv.shard.RowShard, x all-gathered over NCCL inside every step), strong
+scaling: the whole matrix's algorithmic bytes over the slowest rank's time.
 """
 from __future__ import annotations
 
@@ -386,12 +389,83 @@ def reference_arm(args, budget_s: float = 150.0):
     print(json.dumps(line), flush=True)
 
 
+def shard_arm(args):
+    """--mode shard: the headline matrix split over the N ranks by block rows
+    (cbspmv.shard.RowShard: each rank its rows' plan, x all-gathered over
+    NCCL inside every step), strong scaling: value = the whole matrix's
+    algorithmic bytes / the slowest rank's step time."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import cbspmv
+    from cbspmv import gen, shard
+    from cbspmv.dist import Group
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = Group("nccl", dev)
+    coo = gen.power_law()
+    x_host = gen.uniform_x(coo.n, 0)
+    sh = shard.RowShard(coo, world, rank)
+    plans = [p for p in (sh.full, sh.own, sh.halo) if p is not None]
+    alg_rank = sum(p.info()["algorithmic_bytes"] for p in plans)
+    x_own = torch.from_numpy(x_host[sh.c0:sh.c1].copy()).to(dev)
+    y = torch.empty(sh.r1 - sh.r0, dtype=torch.float64, device=dev)
+    sh.spmv(x_own, y)  # correctness gate: this rank's rows
+    torch.cuda.synchronize()
+    sys.path.insert(0, str(REPO / "tests"))
+    import cbdump as cd
+    yref, ab = cd.oracle_spmm_ld(coo, x_host[None, :])
+    err = float(np.max(np.abs(y.cpu().numpy() - yref[0][sh.r0:sh.r1]) /
+                       (ab[0][sh.r0:sh.r1] + 1e-300))) if sh.r1 > sh.r0 else 0.0
+    if pg.max(err) > 1e-12:
+        raise SystemExit(f"bench: sharded SpMV error {err:.3g} above 1e-12")
+    alg = alg_rank
+    if world > 1:
+        t = torch.tensor([float(alg_rank)], dtype=torch.float64, device=dev)
+        dist.all_reduce(t)
+        alg = int(t.item())
+    for _ in range(args.warmup):
+        sh.spmv(x_own, y)
+    launches0 = cbspmv.launch_count()
+    pg.barrier()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        sh.spmv(x_own, y)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = cbspmv.launch_count() - launches0
+    ms = pg.max(ev0.elapsed_time(ev1) / args.steps)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(alg / (ms * 1e-3) / 1e9, 2), "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 5), "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "mode": "shard",
+            "config": {"workload": WORKLOAD, "nnz": coo.nnz, "algorithmic_bytes": alg,
+                       "parallelism": f"block-row shards x{world}, x all-gathered (NCCL)",
+                       "x_piece_bytes": sh.L * 8, "l2": "inputs larger than L2 at N=1"},
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    pg.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10000)
     ap.add_argument("--warmup", type=int, default=50)
     ap.add_argument("--impl", default="cbspmv", choices=["cbspmv", "reference"])
+    ap.add_argument("--mode", default="replicas", choices=["replicas", "shard"],
+                    help="N > 1: every rank its own copy of the headline SpMV (replicas, "
+                         "weak scaling; the default) or one matrix split by block rows "
+                         "(shard, strong scaling)")
     ap.add_argument("--e2e-steps", type=int, default=300)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--configs", default="all",
@@ -405,6 +479,9 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         reference_arm(args)
+        return
+    if args.mode == "shard":
+        shard_arm(args)
         return
 
     import numpy as np
