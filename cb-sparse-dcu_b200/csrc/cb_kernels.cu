@@ -6,15 +6,18 @@
 //     per-warp bulk-async (TMA) double-buffered tiles, host-balanced
 //     contiguous tile ranges, x gathers of the next tile in flight while the
 //     current one is added up;
-//   * cb_spmv_tile_kernel ("direct"; CSR/DENSE-heavy matrices and several
-//     right-hand sides): one warp per tile, tiles taken from a global counter.
+//   * cb_spmv_tile_kernel ("direct"; CSR/DENSE-heavy matrices, one
+//     right-hand side): persistent warps take block-row units from a global
+//     counter.
 // Both add each COO entry's val * x[col] into its row (the reference's
 // per-entry accumulate_output, cb-spmv-dcu.hpp:423-426) in a lane-private
 // shared accumulator -- no atomics, a fixed order, bitwise reproducible -- and
-// reduce the 32 copies of a row once per tile (direct) or once per run of a
-// block row's tiles (streaming).  CSR blocks use 32/bs lanes per row (the
-// reference's LANES_PER_ROW, macros.h:84, re-derived for 32 lanes), DENSE
-// blocks 2 lanes per row (bs = 16) or 1 (bs = 32).  A block row split over
+// reduce the 32 copies of a row once per unit (direct) or once per run of a
+// block row's tiles (streaming).  CSR blocks: the streaming kernel uses 32/bs
+// lanes per row (the reference's LANES_PER_ROW, macros.h:84, re-derived for
+// 32 lanes), the direct kernel one lane per row and a half-warp per block
+// (bs = 16); DENSE blocks 2 lanes per row (streaming, bs = 16) or 1.  Several
+// right-hand sides run in the staged kernel (cb_spmm.cu).  A block row split over
 // several tiles (or warps) leaves partial sums; the last tile (or warp) to
 // arrive on the row's counter adds them in a fixed order and stores y.  No
 // tile waits on another (the reference spins on a row epoch,
