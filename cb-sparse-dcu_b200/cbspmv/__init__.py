@@ -92,6 +92,7 @@ def _load():
         "cbspmv_cb_spmv": (ctypes.c_int, [_P, _P, _P, ctypes.POINTER(Metrics)]),
         "cbspmv_upload": (ctypes.c_int, [_P, _P]),
         "cbspmv_plan_save": (ctypes.c_int, [_P, ctypes.c_char_p]),
+        "cbspmv_plan_save_ex": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_int]),
         "cbspmv_plan_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_P)]),
         "cbspmv_plan_opts": (ctypes.c_int, [_P, ctypes.POINTER(Opts)]),
         "cbspmv_spmv": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, _I64, _I64, _P]),
@@ -224,9 +225,12 @@ class Plan:
         self._uploaded = False
 
     # ---- plan files
-    def save(self, path) -> None:
-        """Writes the built plan to a .cbplan file (cbspmv_plan_save)."""
-        _check(_lib.cbspmv_plan_save(self._h, str(path).encode()))
+    def save(self, path, spmv_only: bool = False) -> None:
+        """Writes the built plan to a .cbplan file (cbspmv_plan_save_ex);
+        spmv_only: without the host block arrays and the per-value arrays
+        (a plan loaded from it multiplies but cannot take new values or give
+        value gradients)."""
+        _check(_lib.cbspmv_plan_save_ex(self._h, str(path).encode(), 1 if spmv_only else 0))
 
     @classmethod
     def load(cls, path) -> "Plan":

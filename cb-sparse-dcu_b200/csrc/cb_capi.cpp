@@ -124,6 +124,10 @@ struct cbspmv_plan {
     void *hx = nullptr, *hy = nullptr;
     size_t hx_bytes = 0, hy_bytes = 0;
     HostPipe pipe;
+    // loaded from an SpMV-only plan file: no per-value arrays, no host block
+    // arrays; counts = the block counts the plan's info reports
+    bool spmv_only = false;
+    int64_t counts[6] = {};
     // cbspmv_adjoint: the value gradient's stream and its fork/join events
     cudaStream_t adj = nullptr;
     cudaEvent_t adj_fork = nullptr, adj_join = nullptr;
@@ -141,6 +145,34 @@ struct cbspmv_plan {
 };
 
 namespace {
+
+// A's COO, CSR, DENSE and uniform blocks, segments and row patterns.
+void block_counts(const cbspmv_plan *p, int64_t out[6]) {
+    if (p->spmv_only) {
+        std::memcpy(out, p->counts, sizeof p->counts);
+        return;
+    }
+    const cb::HostCB &g = p->host;
+    for (int q = 0; q < 6; ++q) out[q] = 0;
+    for (int64_t i = 0; i < g.nnzb; ++i) {
+        if (g.nnz_blk[i] <= 0) continue;
+        const int t = g.type_blk[i] & cb::kTypeMask;
+        out[0] += t == cb::kCOO;
+        out[1] += t == cb::kCSR;
+        out[2] += t == cb::kDENSE;
+        out[3] += (g.type_blk[i] & cb::kUniform) != 0;
+    }
+    out[4] = (int64_t)g.seg_rows.size();
+    out[5] = g.pat_row_ptr.empty() ? 0 : (int64_t)g.pat_row_ptr.size() - 1;
+}
+
+// Calls that need the per-value arrays an SpMV-only plan file leaves out.
+cbspmv_status refuse_spmv_only(const cbspmv_plan *p) {
+    return p->spmv_only
+        ? fail(CBSPMV_ERR_STATE, "plan loaded from an SpMV-only plan file holds no "
+                                 "per-value data")
+        : CBSPMV_OK;
+}
 
 size_t vsize(const cbspmv_plan *p) {
     return p->opts.value_type == CBSPMV_F32 ? 4 : 8;
@@ -385,8 +417,17 @@ cbspmv_status cbspmv_coo2block_gather(const cbspmv_coo *coo,
 }
 
 cbspmv_status cbspmv_plan_save(const cbspmv_plan *p, const char *path) {
+    return cbspmv_plan_save_ex(p, path, 0);
+}
+
+cbspmv_status cbspmv_plan_save_ex(const cbspmv_plan *p, const char *path, int flags) {
     if (!p || !path) return fail(CBSPMV_ERR_INVALID, "null argument");
+    if (flags & ~CBSPMV_PLAN_SPMV_ONLY) return fail(CBSPMV_ERR_INVALID, "unknown flags");
+    if (p->spmv_only && !(flags & CBSPMV_PLAN_SPMV_ONLY))
+        return fail(CBSPMV_ERR_STATE, "an SpMV-only plan can only be saved SpMV-only");
     cb::PlanImage img;
+    img.flags = (flags & CBSPMV_PLAN_SPMV_ONLY) ? cb::kPlanSpmvOnly : 0;
+    block_counts(p, img.counts);
     const cbspmv_opts &o = p->opts;
     const int32_t opts[10] = {o.block_size,  o.row_owned,      o.waves_per_block,
                               o.dense_sixteenths, o.force_coo64, o.value_type,
@@ -429,6 +470,8 @@ cbspmv_status cbspmv_plan_load(const char *path, cbspmv_plan **out) {
         delete p;
         return fail(CBSPMV_ERR_INVALID, err);
     }
+    p->spmv_only = (img.flags & cb::kPlanSpmvOnly) != 0;
+    std::memcpy(p->counts, img.counts, sizeof p->counts);
     cbspmv_opts &o = p->opts;
     o.block_size = img.opts[0];
     o.row_owned = img.opts[1];
@@ -704,6 +747,7 @@ cbspmv_status cbspmv_grad_vals(cbspmv_plan *p, const void *g, const void *x,
                                void *gvals, int nrhs, int64_t ldg, int64_t ldx,
                                void *stream) {
     if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
+    if (cbspmv_status rc = refuse_spmv_only(p)) return rc;
     if (!p->uploaded) return fail(CBSPMV_ERR_STATE, "plan not uploaded");
     if (nrhs < 1) return fail(CBSPMV_ERR_INVALID, "nrhs must be >= 1");
     if (ldg == 0) ldg = nrhs;
@@ -725,6 +769,7 @@ cbspmv_status cbspmv_adjoint(cbspmv_plan *p, const void *g, const void *x, void 
     if (gx && !p->has_t) return fail(CBSPMV_ERR_STATE, "plan built without want_transpose");
     if (!gx) return cbspmv_grad_vals(p, g, x, gvals, nrhs, ldg, ldx, stream);
     if (!gvals) return cbspmv_spmv_t(p, g, gx, nrhs, ldg, ldgx, stream);
+    if (cbspmv_status rc = refuse_spmv_only(p)) return rc;
     if (!p->uploaded) return fail(CBSPMV_ERR_STATE, "plan not uploaded");
     if (nrhs < 1) return fail(CBSPMV_ERR_INVALID, "nrhs must be >= 1");
     const int64_t lg = ldg ? ldg : nrhs, lx = ldx ? ldx : nrhs;
@@ -758,6 +803,7 @@ int64_t cbspmv_num_values(const cbspmv_plan *p) { return p ? p->A.lay.nvals : -1
 cbspmv_status cbspmv_set_values(cbspmv_plan *p, const void *input_values,
                                 void *stream) {
     if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
+    if (cbspmv_status rc = refuse_spmv_only(p)) return rc;
     if (!p->uploaded) return fail(CBSPMV_ERR_STATE, "plan not uploaded");
     if (p->A.lay.unit)
         return fail(CBSPMV_ERR_UNSUPPORTED,
@@ -777,6 +823,7 @@ cbspmv_status cbspmv_set_values(cbspmv_plan *p, const void *input_values,
 cbspmv_status cbspmv_value_coords(const cbspmv_plan *p, int32_t *row, int32_t *col,
                                   int64_t *first_input) {
     if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
+    if (cbspmv_status rc = refuse_spmv_only(p)) return rc;
     const cb::DeviceLayout &L = p->A.lay;
     if (row) std::memcpy(row, L.val_row.data(), L.nvals * 4);
     if (col) std::memcpy(col, L.val_col.data(), L.nvals * 4);
@@ -788,6 +835,7 @@ cbspmv_status cbspmv_value_coords(const cbspmv_plan *p, int32_t *row, int32_t *c
 
 cbspmv_status cbspmv_input_slots(const cbspmv_plan *p, int64_t *slot) {
     if (!p || !slot) return fail(CBSPMV_ERR_INVALID, "null argument");
+    if (cbspmv_status rc = refuse_spmv_only(p)) return rc;
     std::memcpy(slot, p->A.lay.input_slot.data(), p->host.nnz * sizeof(int64_t));
     return CBSPMV_OK;
 }
@@ -813,16 +861,14 @@ cbspmv_status cbspmv_info_get(const cbspmv_plan *p, cbspmv_info *info) {
     I.super_sparse_ratio = g.ratio;
     I.load_stddev_before = g.sd_before;
     I.load_stddev_after = g.sd_after;
-    for (int64_t i = 0; i < g.nnzb; ++i) {
-        if (g.nnz_blk[i] <= 0) continue;
-        const int t = g.type_blk[i] & cb::kTypeMask;
-        I.coo_blocks += t == cb::kCOO;
-        I.csr_blocks += t == cb::kCSR;
-        I.dense_blocks += t == cb::kDENSE;
-        I.uniform_blocks += (g.type_blk[i] & cb::kUniform) != 0;
-    }
-    I.segments = (int64_t)g.seg_rows.size();
-    I.patterns = g.pat_row_ptr.empty() ? 0 : (int64_t)g.pat_row_ptr.size() - 1;
+    int64_t c[6];
+    block_counts(p, c);
+    I.coo_blocks = c[0];
+    I.csr_blocks = c[1];
+    I.dense_blocks = c[2];
+    I.uniform_blocks = c[3];
+    I.segments = c[4];
+    I.patterns = c[5];
     I.stored_values = p->A.lay.nvals;
     I.tiles = (int64_t)p->A.lay.tiles.size();
     I.split_rows = p->A.lay.split_rows;
@@ -869,9 +915,19 @@ int64_t export_device(const cb::DeviceLayout &L, const std::string &k, void *out
 }
 }  // namespace
 
+// An SpMV-only plan has the device layout's geometry and payload but no host
+// block arrays and no per-value arrays: those names give -1.
+bool exportable(const cbspmv_plan *p, const std::string &k) {
+    if (!p->spmv_only) return true;
+    const bool ok = k == "dev_tiles" || k == "dev_blocks" || k == "dev_payload";
+    if (!ok) fail(CBSPMV_ERR_STATE, "plan loaded from an SpMV-only plan file: no " + k);
+    return ok;
+}
+
 int64_t cbspmv_export(const cbspmv_plan *p, const char *name, void *out) {
     if (!p || !name) return -1;
     const std::string k(name);
+    if (!exportable(p, k)) return -1;
     if (k.rfind("dev_", 0) == 0) return export_device(p->A.lay, k, out);
     return cb::export_array(p->host, k, out);
 }
@@ -879,6 +935,7 @@ int64_t cbspmv_export(const cbspmv_plan *p, const char *name, void *out) {
 int64_t cbspmv_export_t(const cbspmv_plan *p, const char *name, void *out) {
     if (!p || !name || !p->has_t) return -1;
     const std::string k(name);
+    if (!exportable(p, k)) return -1;
     if (k.rfind("dev_", 0) == 0) return export_device(p->AT.lay, k, out);
     return cb::export_array(p->host_t, k, out);
 }

@@ -110,40 +110,47 @@ struct Reader {
     }
 };
 
+// lean: scalars only (an SpMV-only file)
 template <class Ar>
-void visit(Ar &ar, HostCB &g) {
+void visit(Ar &ar, HostCB &g, bool lean) {
     ar(g.o.bs), ar(g.o.row_owned), ar(g.o.waves), ar(g.o.dense_sixteenths), ar(g.o.force_coo64);
     ar(g.m), ar(g.n), ar(g.nnz), ar(g.gb_m), ar(g.gb_n), ar(g.nnzb);
     ar(g.gather_flag), ar(g.direct), ar(g.compact), ar(g.balanced);
     ar(g.super_sparse), ar(g.analyzed), ar(g.ratio), ar(g.sd_before), ar(g.sd_after);
+    ar(g.unit_values);
+    if (lean) return;
     ar(g.gb_row), ar(g.gb_col), ar(g.nnz_blk), ar(g.type_blk), ar(g.gb_row_ptr);
     ar(g.seg_rows), ar(g.seg_begin), ar(g.seg_end), ar(g.seg_direct), ar(g.seg_uniform);
     ar(g.row_uniform), ar(g.flat_row_ptr), ar(g.flat_col), ar(g.pat_row_ptr), ar(g.pat_col);
     ar(g.pat_out_ptr), ar(g.pat_out_rows), ar(g.block_cols_offset), ar(g.block_cols);
     ar(g.bidx_origin), ar(g.bidx_end), ar(g.bidx_nnz), ar(g.nnzb_orig);
     ar(g.u32_off), ar(g.f64_off), ar(g.pay_u32), ar(g.pay_f64), ar(g.src_ptr), ar(g.src);
-    ar(g.unit_values);
 }
 
+// lean: no per-value arrays (value offsets, coordinates, sources, slots)
 template <class Ar>
-void visit(Ar &ar, DeviceLayout &L) {
+void visit(Ar &ar, DeviceLayout &L, bool lean) {
     ar(L.bs), ar(L.f32), ar(L.unit), ar(L.gather), ar(L.m), ar(L.n), ar(L.gb_m);
     ar(L.tiles), ar(L.blocks), ar(L.payload), ar(L.block_cols);
     ar(L.slots), ar(L.split_rows), ar(L.max_row_tiles), ar(L.max_entries);
-    ar(L.max_tile_bytes), ar(L.coo_share), ar(L.nvals);
+    ar(L.max_tile_bytes), ar(L.coo_share), ar(L.nvals), ar(L.alg_bytes);
+    if (lean) return;
     ar(L.val_off), ar(L.val_row), ar(L.val_col), ar(L.vsrc_ptr), ar(L.vsrc);
-    ar(L.input_slot), ar(L.alg_bytes);
+    ar(L.input_slot);
 }
 
 template <class Ar>
 void visit_body(Ar &ar, PlanImage &img) {
+    ar(img.flags);
+    const bool lean = (img.flags & kPlanSpmvOnly) != 0;
     for (int32_t &v : img.opts) ar(v);
     ar(img.has_t);
-    visit(ar, *img.host);
-    visit(ar, *img.A);
+    for (int64_t &c : img.counts) ar(c);
+    visit(ar, *img.host, lean);
+    visit(ar, *img.A, lean);
     if (img.has_t) {
-        visit(ar, *img.host_t);
-        visit(ar, *img.AT);
+        visit(ar, *img.host_t, lean);
+        visit(ar, *img.AT, lean);
     }
 }
 

@@ -12,10 +12,17 @@
 namespace cb {
 
 // Everything a plan keeps on the host.  opts: the ten int fields of
-// cbspmv_opts in declaration order.
+// cbspmv_opts in declaration order.  flags & kPlanSpmvOnly: the file holds
+// the host structures' scalars and the device layouts without their
+// per-value arrays (enough to upload and multiply); counts: A's COO, CSR,
+// DENSE and uniform blocks, segments and row patterns (what the plan's info
+// reports), kept because such a file has no block arrays to count.
+constexpr int32_t kPlanSpmvOnly = 1;
 struct PlanImage {
+    int32_t flags = 0;
     int32_t opts[10] = {};
     int32_t has_t = 0;
+    int64_t counts[6] = {};
     HostCB *host = nullptr, *host_t = nullptr;
     DeviceLayout *A = nullptr, *AT = nullptr;
 };
@@ -24,6 +31,6 @@ struct PlanImage {
 std::string save_plan(const PlanImage &img, const std::string &path);
 std::string load_plan(const std::string &path, PlanImage &img);
 
-constexpr uint32_t kPlanFileVersion = 2;
+constexpr uint32_t kPlanFileVersion = 3;
 
 }  // namespace cb

@@ -133,6 +133,20 @@ void cbspmv_default_opts(cbspmv_opts *opts);
 cbspmv_status cbspmv_plan_save(const cbspmv_plan *plan, const char *path);
 cbspmv_status cbspmv_plan_load(const char *path, cbspmv_plan **out);
 
+/* cbspmv_plan_save with flags.  CBSPMV_PLAN_SPMV_ONLY writes what products
+ * need -- the options, the host structures' scalars, the block counts and
+ * the device layouts' tiles, blocks and payload -- and leaves out the host
+ * GLOBAL_BLOCK arrays and the per-value arrays (PL: 0.22 GB instead of 1.5
+ * GB).  A plan loaded from such a file uploads, multiplies (cbspmv_spmv,
+ * cbspmv_spmv_t, host and batch calls), autotunes and saves SpMV-only; the
+ * calls that need per-value data (cbspmv_set_values, cbspmv_grad_vals, the
+ * value gradient of cbspmv_adjoint, cbspmv_value_coords,
+ * cbspmv_input_slots) return CBSPMV_ERR_STATE, and cbspmv_export returns -1
+ * for every name but dev_tiles, dev_blocks and dev_payload. */
+#define CBSPMV_PLAN_SPMV_ONLY 1
+cbspmv_status cbspmv_plan_save_ex(const cbspmv_plan *plan, const char *path,
+                                  int flags);
+
 /* The options a plan was built (or loaded) with; `kernel` reflects
  * cbspmv_autotune. */
 cbspmv_status cbspmv_plan_opts(const cbspmv_plan *plan, cbspmv_opts *opts);

@@ -195,17 +195,29 @@ def test_loaded_plan_gives_the_same_y(cuda, tmp_path):
     import torch
     import cbspmv
     from cbspmv import gen
-    for coo in (dict(CASES)["pl8192"], dict(CASES)["st6"]):
-        p = cbspmv.Plan(coo)
+    for coo, spmv_only in ((dict(CASES)["pl8192"], False), (dict(CASES)["st6"], False),
+                           (dict(CASES)["pl8192"], True), (dict(CASES)["st6"], True)):
+        p = cbspmv.Plan(coo, want_transpose=1)
         p.autotune(1)
         path = tmp_path / "p.cbplan"
-        p.save(path)
+        p.save(path, spmv_only=spmv_only)
         q = cbspmv.Plan.load(path)
         assert q.opts.kernel == p.opts.kernel
         x = torch.from_numpy(gen.uniform_x(coo.n, 8)).to(cuda)
+        X = torch.from_numpy(gen.uniform_x(coo.n, 9, nrhs=4).T.copy()).to(cuda)
+        g = torch.from_numpy(gen.uniform_x(coo.m, 10)).to(cuda)
         y1, y2 = p.spmv(x), q.spmv(x)
+        Y1, Y2 = p.spmv(X), q.spmv(X)
+        t1, t2 = p.spmv_t(g), q.spmv_t(g)
         torch.cuda.synchronize()
-        assert torch.equal(y1, y2)
+        assert torch.equal(y1, y2) and torch.equal(Y1, Y2) and torch.equal(t1, t2)
+        if spmv_only:  # no per-value data: value updates and gradients refused
+            for call in (lambda: q.set_values(torch.ones(coo.nnz, dtype=torch.float64,
+                                                         device=cuda)),
+                         lambda: q.grad_vals(g, x)):
+                with pytest.raises(cbspmv.CBSpMVError) as e:
+                    call()
+                assert e.value.status == "STATE"
 
 
 def test_empty_and_degenerate(cuda):

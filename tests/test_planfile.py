@@ -60,6 +60,47 @@ def test_save_load_round_trip(tmp_path, name, coo, opts):
         assert np.array_equal(ld.decode_spmv(p, x), ld.decode_spmv(q, x))
 
 
+@pytest.mark.parametrize("name,coo", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("opts", [dict(), dict(block_size=32, value_type=1, want_transpose=1)])
+def test_spmv_only_files(tmp_path, name, coo, opts):
+    """An SpMV-only file: the same device layout (tiles, blocks, payload),
+    info and scalars, a fraction of the size; calls needing per-value data or
+    host block arrays are refused; it saves again only SpMV-only."""
+    import cbspmv
+    p = cbspmv.Plan(coo, **opts)
+    full, lean = tmp_path / "full.cbplan", tmp_path / "lean.cbplan"
+    p.save(full)
+    p.save(lean, spmv_only=True)
+    if coo.nnz:
+        assert lean.stat().st_size < full.stat().st_size / 2
+    q = cbspmv.Plan.load(lean)
+    assert q.info() == p.info()
+    for f in ("block_size", "value_type", "want_transpose", "tile_entries", "kernel"):
+        assert getattr(q.opts, f) == getattr(p.opts, f), f
+    sp, sq = np.zeros(12, np.int64), np.zeros(12, np.int64)
+    fp, fq = np.zeros(3), np.zeros(3)
+    lib = cbspmv.lib()
+    for t in ((0, 1) if opts.get("want_transpose") else (0,)):
+        lib.cbspmv_export_scalars(p._h, t, sp.ctypes.data_as(cbspmv.ctypes.c_void_p),
+                                  fp.ctypes.data_as(cbspmv.ctypes.c_void_p))
+        lib.cbspmv_export_scalars(q._h, t, sq.ctypes.data_as(cbspmv.ctypes.c_void_p),
+                                  fq.ctypes.data_as(cbspmv.ctypes.c_void_p))
+        assert np.array_equal(sp, sq) and np.array_equal(fp, fq)
+        for dn in ("dev_tiles", "dev_blocks", "dev_payload"):
+            assert np.array_equal(_raw(p, dn, bool(t)), _raw(q, dn, bool(t))), dn
+        fn = lib.cbspmv_export_t if t else lib.cbspmv_export
+        for dn in ("dev_values", "gb_row_idx", "block_cols"):
+            assert fn(q._h, dn.encode(), None) == -1, dn
+    with pytest.raises(cbspmv.CBSpMVError) as e:
+        q.input_slots()
+    assert e.value.status == "STATE"
+    with pytest.raises(cbspmv.CBSpMVError) as e:
+        q.save(tmp_path / "again.cbplan")
+    assert e.value.status == "STATE"
+    q.save(tmp_path / "again.cbplan", spmv_only=True)
+    assert (tmp_path / "again.cbplan").read_bytes() == lean.read_bytes()
+
+
 def test_damaged_files_are_refused(tmp_path):
     import cbspmv
     p = cbspmv.Plan(CASES[0][1])
