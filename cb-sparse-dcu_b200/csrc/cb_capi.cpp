@@ -995,7 +995,17 @@ struct cbspmv_batch {
     cudaStream_t cap[8] = {};
     cudaEvent_t ev[9] = {};
     cudaGraphExec_t exec[2] = {};
+    // cbspmv_batch_run: groups after the first run on streams of their own,
+    // forked from and joined back to the caller's stream
+    std::vector<cudaStream_t> side;
+    std::vector<cudaEvent_t> side_done;
+    cudaEvent_t fork = nullptr;
     ~cbspmv_batch() {
+        for (cudaStream_t s : side)
+            if (s) cudaStreamSynchronize(s), cudaStreamDestroy(s);
+        for (cudaEvent_t e : side_done)
+            if (e) cudaEventDestroy(e);
+        if (fork) cudaEventDestroy(fork);
         for (cudaGraphExec_t &g : exec)
             if (g) cudaGraphExecDestroy(g);
         for (cudaEvent_t &e : ev)
@@ -1032,12 +1042,32 @@ cbspmv_status batch_each(cbspmv_batch *b, cudaStream_t st) {
     return CBSPMV_OK;
 }
 
+// One persistent launch per lane class.  The classes' launches are
+// independent (own tiles, units and counters), so all but the first run on
+// side streams forked from `st` and joined back to it: one class's tail
+// overlaps the next class's start.
 cbspmv_status batch_one(cbspmv_batch *b, cudaStream_t st) {
-    for (const BatchGroup &g : b->groups)
-        CB_CUDA(cb::launch_batch(b->bs, b->f32, g.c, b->d_views + g.first, g.count, g.d_toff,
-                                 g.d_ustart, g.nunits, b->tile_cap, g.d_sched, st),
-                "batch launch");
-    return CBSPMV_OK;
+    const size_t ng = b->groups.size();
+    if (ng > 1) {
+        CB_CUDA(cudaEventRecord(b->fork, st), "batch fork");
+        for (size_t q = 1; q < ng; ++q)
+            CB_CUDA(cudaStreamWaitEvent(b->side[q - 1], b->fork, 0), "batch fork");
+    }
+    cbspmv_status rc = CBSPMV_OK;
+    for (size_t q = 0; q < ng && !rc; ++q) {
+        const BatchGroup &g = b->groups[q];
+        const cudaError_t e =
+            cb::launch_batch(b->bs, b->f32, g.c, b->d_views + g.first, g.count, g.d_toff,
+                             g.d_ustart, g.nunits, b->tile_cap, g.d_sched,
+                             q ? b->side[q - 1] : st);
+        if (e != cudaSuccess) rc = cuda_fail(e, "batch launch");
+    }
+    // join every side stream, also after a failed launch
+    for (size_t q = 1; q < ng; ++q) {
+        CB_CUDA(cudaEventRecord(b->side_done[q - 1], b->side[q - 1]), "batch join");
+        CB_CUDA(cudaStreamWaitEvent(st, b->side_done[q - 1], 0), "batch join");
+    }
+    return rc;
 }
 
 }  // namespace
@@ -1124,6 +1154,16 @@ cbspmv_status cbspmv_batch_create(cbspmv_plan *const *plans, int count, const in
         b->groups.push_back(g);
     }
     if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_views, count * sizeof(cb::MatView));
+    for (size_t q = 1; q < b->groups.size() && e == cudaSuccess; ++q) {
+        cudaStream_t s = nullptr;
+        cudaEvent_t d = nullptr;
+        e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+        if (e == cudaSuccess) b->side.push_back(s);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&d, cudaEventDisableTiming);
+        if (e == cudaSuccess) b->side_done.push_back(d);
+    }
+    if (e == cudaSuccess && b->groups.size() > 1)
+        e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         delete b;
         return cuda_fail(e, "allocate batch tables");
