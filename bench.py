@@ -42,12 +42,19 @@ import re
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 REPO = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO / "cb-sparse-dcu_b200"))
 
 METRIC = "SpMV GB/s (algorithmic CB bytes / t), plain CB-SpMV FP64, power-law n=2^20"
+# Algorithmic bytes of one SpMV of the headline workload in this library's
+# layout (cbspmv_info.algorithmic_bytes: tile descriptors, COO indices and
+# values without padding, x once, y once).  The reference arm divides by the
+# same count without loading the product library; a CPU test checks that the
+# library reports this number.
+PL_FP64_ALG_BYTES = 221776532
 UNIT = "GB/s"
 WORKLOAD = ("power-law n=2^20, alpha 2.1, lengths [1,20000], mean 16 nnz/row, "
             "70% within +-4096 of diagonal, N(0,1) values, seed 1; FP64; 16x16 blocks")
@@ -77,8 +84,9 @@ class Clocks:
     def __init__(self, index: int):
         self.index = index
         self.proc = None
-        self.path = REPO / "gpurun_out" / f"clocks_rank{index}.csv"
-        self.err = REPO / "gpurun_out" / f"clocks_rank{index}.err"
+        tmp = pathlib.Path(tempfile.mkdtemp(prefix="cbspmv_clocks_"))
+        self.path = tmp / f"clocks_rank{index}.csv"
+        self.err = tmp / f"clocks_rank{index}.err"
         self.gpu = str(index)
         try:  # the device as nvidia-smi names it (CUDA_VISIBLE_DEVICES may remap)
             import torch
@@ -170,22 +178,52 @@ def _timed(fn, reps: int, warmup: int, flush=None):
     return total / reps
 
 
+def _oracle():
+    """The CPU oracle (test infrastructure: the checker of every result the
+    bench reports, never the thing timed)."""
+    sys.path.insert(0, str(REPO / "tests"))
+    import cbdump as cd
+    return cd
+
+
+def _parity(y, yref, ab, f32) -> dict:
+    """Error of a result against the long-double oracle.  y, yref, ab:
+    (nrhs, rows); ab = sum_k |a_ik x_kj| per row.  max_err_rowscaled =
+    max |y - yref| / ab (the tests' bound: <= 1e-12 FP64, <= 1e-5 FP32);
+    for FP32 the plain errors against the FP64 oracle are stated too."""
+    import numpy as np
+    y = np.asarray(y, np.float64)
+    d = np.abs(y - yref)
+    tol = 1e-5 if f32 else 1e-12
+    err = float(np.max(d / (ab + 1e-300))) if d.size else 0.0
+    out = {"max_err_rowscaled": float(f"{err:.3g}"), "tol": tol, "pass": bool(err <= tol)}
+    if f32:
+        ymax = float(np.max(np.abs(yref))) if yref.size else 0.0
+        dmax = float(np.max(d)) if d.size else 0.0
+        out["fp32_vs_fp64_oracle"] = {
+            "max_abs_err": float(f"{dmax:.3g}"),
+            "max_abs_err_over_max_abs_y": float(f"{(dmax / ymax) if ymax else 0.0:.3g}")}
+    return out
+
+
 def secondary_configs(dev, peak: float, want=("lap", "pl32", "st", "diff", "bat"),
                       bat_count: int = 512) -> dict:
-    """The other workloads of the benchmark suite, each timed on the device:
-    LAP (5-point Laplacian 256^2, FP64), PL in FP32, PL with unit values (the
-    value-free payload the reference uses for its unit-valued inputs), ST
-    (27-point x 3 dof
-    stencil on 64^3, FP64 and FP32), DIFF (power-law n = 2^18, 8 right-hand
-    sides, FP32: forward, adjoint A^T G and the value gradient) and BAT (512
-    uneven FP32 matrices with 1-16 right-hand sides: one batched launch per
-    lane class, its CUDA graph, one launch per matrix, and a graph of those).
-    Every plan is autotuned first (cbspmv_autotune).  Algorithmic bytes: the
-    packed matrix the kernel must read, x and y once per right-hand side."""
+    """The other workloads of the benchmark suite, each timed on the device
+    and each result checked against the oracle at its full size (outside the
+    timed region): LAP (5-point Laplacian 256^2, FP64), PL in FP32, PL with
+    unit values (the value-free payload the reference uses for its
+    unit-valued inputs), ST (27-point x 3 dof stencil on 64^3, FP64 and FP32),
+    DIFF (power-law n = 2^18, 8 right-hand sides, FP32: forward, adjoint A^T G
+    and the value gradient) and BAT (512 uneven FP32 matrices with 1-16
+    right-hand sides: the batched launch, its CUDA graph, one launch per
+    matrix, and a graph of those).  Every plan is autotuned first
+    (cbspmv_autotune).  Algorithmic bytes: the packed matrix the kernel must
+    read, x and y once per right-hand side."""
     import numpy as np
     import torch
     import cbspmv
     from cbspmv import gen
+    cd = _oracle()
 
     l2_flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     flush = lambda: l2_flush.zero_()  # noqa: E731
@@ -195,15 +233,21 @@ def secondary_configs(dev, peak: float, want=("lap", "pl32", "st", "diff", "bat"
         plan = cbspmv.Plan(coo, value_type=int(f32))
         kernel, _ = plan.autotune(1)
         dt = torch.float32 if f32 else torch.float64
-        x = torch.from_numpy(gen.uniform_x(coo.n, 0)).to(dev, dt)
+        xh = gen.uniform_x(coo.n, 0)
+        if f32:
+            xh = xh.astype(np.float32).astype(np.float64)  # the x the GPU sees
+        x = torch.from_numpy(xh).to(dev, dt)
         y = torch.empty(coo.m, dtype=dt, device=dev)
         info = plan.info()
         small = info["device_bytes"] < (200 << 20)
         ms = _timed(lambda: plan.spmv(x, y), reps, 5, flush if small else None)
+        plan.check()
+        yref, ab = cd.oracle_spmm_ld(coo, xh[None, :])
         alg = info["algorithmic_bytes"]
         out[name] = {"nnz": coo.nnz, "kernel": kernel, "ms": round(ms, 4),
                      "gbs": round(alg / ms / 1e6, 1), "gflops": round(2 * coo.nnz / ms / 1e6, 1),
                      "frac": round(alg / ms / 1e6 / peak, 4),
+                     "parity": _parity(y.cpu().numpy()[None, :], yref, ab, f32),
                      "l2": "flushed before each step" if small else "inputs larger than L2"}
         del plan
 
@@ -229,18 +273,22 @@ def secondary_configs(dev, peak: float, want=("lap", "pl32", "st", "diff", "bat"
 
 
 def diff_config(dev, peak, flush, out):
-    """DIFF: Y = A X, then G -> A^T G and the value gradient."""
+    """DIFF: Y = A X, then G -> A^T G and the value gradient; every output
+    checked against the oracle at full size."""
     import numpy as np
     import torch
     import cbspmv
     from cbspmv import gen
+    cd = _oracle()
 
     coo = gen.power_law(1 << 18, seed=3, mean=24)
     k = 8
     plan = cbspmv.Plan(coo, value_type=1, want_transpose=1)
-    plan.autotune(k)
-    X = torch.from_numpy(np.ascontiguousarray(gen.uniform_x(coo.n, 1, nrhs=k).T)).to(dev, torch.float32)
-    G = torch.from_numpy(np.ascontiguousarray(gen.uniform_x(coo.m, 2, nrhs=k).T)).to(dev, torch.float32)
+    kernel, _ = plan.autotune(k)
+    Xh = gen.uniform_x(coo.n, 1, nrhs=k).astype(np.float32).astype(np.float64)
+    Gh = gen.uniform_x(coo.m, 2, nrhs=k).astype(np.float32).astype(np.float64)
+    X = torch.from_numpy(np.ascontiguousarray(Xh.T)).to(dev, torch.float32)
+    G = torch.from_numpy(np.ascontiguousarray(Gh.T)).to(dev, torch.float32)
     Y = torch.empty(coo.m, k, device=dev)
     GX = torch.empty(coo.n, k, device=dev)
     GV = torch.empty(plan.num_values(), device=dev)
@@ -250,12 +298,21 @@ def diff_config(dev, peak, flush, out):
     adj_bytes = fwd_bytes + plan.num_values() * (8 + 4) + 4 * (coo.n + coo.m) * k
     t_f = _timed(lambda: plan.spmv(X, Y), 30, 5, flush)
     t_a = _timed(lambda: plan.adjoint(G, X, GX, GV), 30, 5, flush)
+    plan.check()
+    yref, ab = cd.oracle_spmm_ld(coo, Xh)
+    gref, gab = cd.oracle_spmm_ld(coo, Gh, transpose=True)
+    vref = cd.oracle_grad_vals(coo, Gh, Xh)
+    vscale = np.sum(np.abs(Gh[:, coo.row] * Xh[:, coo.col]), axis=0)[None, :]
+    gv = GV.cpu().numpy().astype(np.float64)[plan.input_slots()][None, :]
     out["DIFF fp32 (n=2^18, 8 rhs)"] = {
-        "nnz": coo.nnz, "fwd_ms": round(t_f, 4), "adj_ms": round(t_a, 4),
+        "nnz": coo.nnz, "kernel": kernel, "fwd_ms": round(t_f, 4), "adj_ms": round(t_a, 4),
         "fwd_plus_adj_over_fwd": round((t_f + t_a) / t_f, 3),
         "fwd_gbs": round(fwd_bytes / t_f / 1e6, 1), "fwd_frac": round(fwd_bytes / t_f / 1e6 / peak, 4),
         "adj_gbs": round(adj_bytes / t_a / 1e6, 1),
-        "gflops_fwd": round(2 * coo.nnz * k / t_f / 1e6, 1), "l2": "flushed before each step"}
+        "gflops_fwd": round(2 * coo.nnz * k / t_f / 1e6, 1), "l2": "flushed before each step",
+        "parity": {"forward": _parity(Y.cpu().numpy().T, yref, ab, True),
+                   "adjoint_gx": _parity(GX.cpu().numpy().T, gref, gab, True),
+                   "value_gradient": _parity(gv, vref[None, :], vscale, True)}}
     del plan
     # library comparator for the forward: cuSPARSE SpMM (CSR, int32 indices)
     try:
@@ -277,26 +334,59 @@ def diff_config(dev, peak, flush, out):
         out["DIFF fp32 (n=2^18, 8 rhs)"]["comparator"] = {"unavailable": str(exc)[:200]}
 
 
+def _check_batch(cd, items, xs_h, ys, threads=16) -> dict:
+    """Every matrix of a batch against the oracle, on host threads (the
+    oracle's C calls release the GIL); the worst matrix's figures."""
+    from concurrent.futures import ThreadPoolExecutor
+    yh = [y.cpu().numpy() for y in ys]
+
+    def one(k):
+        it = items[k]
+        yref, ab = cd.oracle_spmm_ld(it.coo, xs_h[k].T)
+        return _parity(yh[k].reshape(it.coo.m, it.nrhs).T, yref, ab, True)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(threads, os.cpu_count() or 1))) as ex:
+        res = list(ex.map(one, range(len(items))))
+    worst = max(range(len(res)), key=lambda k: res[k]["max_err_rowscaled"])
+    out = dict(res[worst])
+    out["checked_matrices"] = len(res)
+    out["pass"] = all(r["pass"] for r in res)
+    out["worst_matrix"] = worst
+    return out
+
+
 def bat_config(dev, peak, count, out):
-    """BAT: `count` uneven FP32 matrices (512 is the workload)."""
+    """BAT: `count` uneven FP32 matrices (512 is the workload); each mode's
+    results checked against the oracle, every matrix."""
+    import numpy as np
     import torch
     import cbspmv
     from cbspmv import gen
+    cd = _oracle()
     items = gen.batch_uneven(count=count)
     plans = [cbspmv.Plan(it.coo, value_type=1) for it in items]
-    xs = [torch.rand(it.coo.n, it.nrhs, device=dev) for it in items]
+    rng = np.random.default_rng(40)
+    xs_h = [rng.uniform(-1, 1, (it.coo.n, it.nrhs)).astype(np.float32).astype(np.float64)
+            for it in items]
+    xs = [torch.from_numpy(x).to(dev, torch.float32) for x in xs_h]
     ys = [torch.empty(it.coo.m, it.nrhs, device=dev) for it in items]
     b = cbspmv.Batch(plans, [it.nrhs for it in items]).bind(xs, ys)
     alg = sum(p.info()["algorithmic_bytes"] + 4 * (it.coo.n + it.coo.m) * (it.nrhs - 1)
               for p, it in zip(plans, items))
-    r = {"matrices": len(items), "nnz": sum(it.coo.nnz for it in items), "algorithmic_bytes": alg}
+    r = {"matrices": len(items), "nnz": sum(it.coo.nnz for it in items), "algorithmic_bytes": alg,
+         "parity": {}}
     for name, fn in (("batched", b.run), ("batched_graph", lambda: b.graph_launch(False)),
                      ("per_matrix", b.run_each), ("per_matrix_graph", lambda: b.graph_launch(True))):
+        for y in ys:
+            y.fill_(float("nan"))
         ms = _timed(fn, 5, 3)
+        torch.cuda.synchronize()
         r[name + "_ms"] = round(ms, 3)
         r[name + "_gbs"] = round(alg / ms / 1e6, 1)
+        r["parity"][name] = _check_batch(cd, items, xs_h, ys)
     r["batched_frac"] = round(r["batched_gbs"] / peak, 4)
     r["batched_over_per_matrix"] = round(r["per_matrix_ms"] / r["batched_ms"], 2)
+    r["batched_graph_over_per_matrix"] = round(r["per_matrix_ms"] / r["batched_graph_ms"], 2)
     r["l2"] = "inputs larger than L2"
     out[f"BAT fp32 ({len(items)} matrices, 1-16 rhs)"] = r
     b.close()
@@ -345,22 +435,21 @@ def _row_prefix(coo, nnz_target: int):
     """The first rows of coo holding about nnz_target nonzeros (a bounded
     sample with the workload's row distribution)."""
     import numpy as np
-    from cbspmv.gen import Coo
     k = int(min(coo.nnz, max(1, nnz_target)))
     rows = int(coo.row[k - 1]) + 1
     k = int(np.searchsorted(coo.row, rows))
-    return Coo(rows, coo.n, coo.row[:k], coo.col[:k], coo.val[:k])
+    return type(coo)(rows, coo.n, coo.row[:k], coo.col[:k], coo.val[:k])
 
 
 def reference_arm(args, budget_s: float = 150.0):
     world, rank, _ = _dist()
     if rank != 0:
         return
-    from cbspmv import gen
-    import cbspmv
+    sys.path.insert(0, str(REPO / "cb-sparse-dcu_b200" / "cbspmv"))
+    import gen  # the workload generator alone (numpy), not the product library
     coo = gen.power_law()
     x = gen.uniform_x(coo.n, 0)
-    alg = cbspmv.Plan(coo).info()["algorithmic_bytes"]
+    alg = PL_FP64_ALG_BYTES  # the same metric's byte count as the GPU arm
     # size each step so that warm-up + timed steps fit the time budget
     t_full, kind, _ = _ref_cpu(coo, x, 0.0, 1)
     frac = min(1.0, budget_s / max(1, args.steps + args.warmup) / t_full)
@@ -599,8 +688,10 @@ def main():
     if rank == 0:
         cpu_dt, kind, reps = _ref_cpu(coo, x_host, args.cpu_seconds, 400)
         cpu = {"value": round(alg / cpu_dt / 1e9, 3), "unit": UNIT, "cores": 1, "kind": kind,
+               "host_cores": os.cpu_count(),
                "sample": f"{reps} full SpMVs of the workload on 1 host thread "
-                         "(check_results_consistency, utils.h:85-136)",
+                         "(check_results_consistency, utils.h:85-136, serial as written) "
+                         f"on a host with {os.cpu_count()} cores",
                "ms_per_spmv": round(cpu_dt * 1e3, 3)}
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": world,
@@ -625,6 +716,17 @@ def main():
         }
         if configs is not None:
             line["configs"] = configs
+            flags = []
+
+            def collect(d):
+                if isinstance(d, dict):
+                    if "pass" in d and "max_err_rowscaled" in d:
+                        flags.append(bool(d["pass"]))
+                    for v in d.values():
+                        collect(v)
+            collect(configs)
+            line["parity"] = {"headline_max_err_rowscaled": float(f"{err:.3g}"),
+                              "configs_checked": len(flags), "all_pass": all(flags)}
     pg.close()
     if line:
         print(json.dumps(line), flush=True)

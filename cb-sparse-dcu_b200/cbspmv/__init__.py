@@ -23,7 +23,7 @@ LIB_PATH = pathlib.Path(os.environ.get("CBSPMV_LIB", _HERE / "libcbspmv.so"))
 
 F64, F32 = 0, 1
 STATUS = {0: "OK", 1: "INVALID", 2: "UNSORTED", 3: "BOUNDS", 4: "ALLOC",
-          5: "CUDA", 6: "STATE", 7: "UNSUPPORTED"}
+          5: "CUDA", 6: "STATE", 7: "UNSUPPORTED", 8: "DEVICE"}
 
 
 class CBSpMVError(RuntimeError):
@@ -115,6 +115,8 @@ def _load():
         "cbspmv_last_error": (ctypes.c_size_t, [ctypes.c_char_p, ctypes.c_size_t]),
         "cbspmv_launch_count": (_I64, []),
         "cbspmv_autotune": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _P]),
+        "cbspmv_check": (ctypes.c_int, [_P, _P]),
+        "cbspmv_debug_wait_polls": (None, [_I64]),
         "cbspmv_batch_create": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.POINTER(_P)]),
         "cbspmv_batch_bind": (ctypes.c_int, [_P, _P, _P, _P]),
         "cbspmv_batch_run": (ctypes.c_int, [_P, _P]),
@@ -149,6 +151,12 @@ def _check(code: int) -> None:
 
 def launch_count() -> int:
     return int(_lib.cbspmv_launch_count())
+
+
+def debug_wait_polls(polls: int) -> None:
+    """Polls each device wait makes before giving up (0: at once); -1
+    restores the default.  For tests of the give-up path."""
+    _lib.cbspmv_debug_wait_polls(int(polls))
 
 
 def default_opts(**kw) -> Opts:
@@ -330,6 +338,11 @@ class Plan:
         _check(_lib.cbspmv_spmv(self._h, _dptr(x), _dptr(y), k, k, k,
                                 _stream(stream)))
         return y
+
+    def check(self, stream=None) -> None:
+        """Synchronizes and raises CBSpMVError (status DEVICE) if a launch on
+        this plan gave up a bounded device wait since the last report."""
+        _check(_lib.cbspmv_check(self._h, _stream(stream)))
 
     def autotune(self, nrhs: int = 1, stream=None):
         """Times the kernels that can run this plan for nrhs right-hand sides

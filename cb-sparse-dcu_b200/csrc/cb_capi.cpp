@@ -131,6 +131,10 @@ struct cbspmv_plan {
     // cbspmv_adjoint: the value gradient's stream and its fork/join events
     cudaStream_t adj = nullptr;
     cudaEvent_t adj_fork = nullptr, adj_join = nullptr;
+    // error words of A's and A^T's launches (host-mapped pinned memory, so the
+    // host reads them without a copy): set by a kernel whose bounded wait gave
+    // up; herr is the host view, derr the device view
+    uint32_t *herr = nullptr, *derr = nullptr;
     ~cbspmv_plan() {
         if (pipe.comp) cudaStreamSynchronize(pipe.out ? pipe.out : pipe.comp);
         pipe.release();
@@ -141,6 +145,7 @@ struct cbspmv_plan {
         AT.release();
         if (hx) cudaFree(hx);
         if (hy) cudaFree(hy);
+        if (herr) cudaFreeHost(herr);
     }
 };
 
@@ -211,6 +216,12 @@ cbspmv_status upload_side(DevSide &s, cudaStream_t st) {
     s.d.counters = s.counters + 4;
     s.d.max_entries = L.max_entries;
     s.d.coo_share = L.coo_share;
+    s.d.has_x = 0;
+    for (const cb::TileDesc &t : L.tiles)
+        if ((t.counts >> 16) & 0xffu) {
+            s.d.has_x = 1;
+            break;
+        }
     return CBSPMV_OK;
 }
 
@@ -271,9 +282,36 @@ cbspmv_status ensure_partials(DevSide &s, int nrhs, size_t vsz) {
     return CBSPMV_OK;
 }
 
+// Reports (once) that a launch on side s (0 = A, 1 = A^T) of the plan gave up
+// a bounded device wait, and resets the side's scheduler words and arrival
+// counters on `st` so that later launches start clean.
+cbspmv_status take_device_error(cbspmv_plan *p, int side, cudaStream_t st) {
+    if (!p->herr) return CBSPMV_OK;
+    volatile uint32_t *w = p->herr + side;
+    if (*w == 0) return CBSPMV_OK;
+    *w = 0;
+    DevSide &s = side ? p->AT : p->A;
+    if (s.counters) {
+        const cudaError_t e =
+            cudaMemsetAsync(s.counters, 0, (s.lay.gb_m + 4) * sizeof(int32_t), st);
+        if (e != cudaSuccess) return cuda_fail(e, "reset scratch after a device error");
+    }
+    return fail(CBSPMV_ERR_DEVICE,
+                std::string("a bounded device wait gave up in an earlier launch on this plan (") +
+                    (side ? "A^T" : "A") +
+                    "): that launch's output is incomplete; the plan's scratch was reset");
+}
+
+cbspmv_status device_errors(cbspmv_plan *p, cudaStream_t st) {
+    cbspmv_status rc = take_device_error(p, 0, st);
+    const cbspmv_status rt = take_device_error(p, 1, st);
+    return rc ? rc : rt;
+}
+
 cbspmv_status run_side(cbspmv_plan *p, DevSide &s, const void *x, void *y,
                        int nrhs, int64_t ldx, int64_t ldy, cudaStream_t st) {
     if (!p->uploaded) return fail(CBSPMV_ERR_STATE, "plan not uploaded");
+    if (cbspmv_status rc = take_device_error(p, &s == &p->AT ? 1 : 0, st)) return rc;
     if (nrhs < 1) return fail(CBSPMV_ERR_INVALID, "nrhs must be >= 1");
     if (ldx == 0) ldx = nrhs;
     if (ldy == 0) ldy = nrhs;
@@ -499,10 +537,17 @@ cbspmv_status cbspmv_upload(cbspmv_plan *p, void *stream) {
     if (p->uploaded) return CBSPMV_OK;
     cudaStream_t st = (cudaStream_t)stream;
     CB_CUDA(cudaGetDevice(&p->device), "cudaGetDevice");
+    if (!p->herr) {
+        CB_CUDA(cudaHostAlloc((void **)&p->herr, 16, cudaHostAllocMapped), "allocate error words");
+        std::memset(p->herr, 0, 16);
+        CB_CUDA(cudaHostGetDevicePointer((void **)&p->derr, p->herr, 0), "map error words");
+    }
     cbspmv_status rc = upload_side(p->A, st);
     if (!rc) rc = upload_partition(p->A, p->opts.kernel, st);
     if (!rc && p->has_t) rc = upload_side(p->AT, st);
     if (!rc && p->has_t) rc = upload_partition(p->AT, p->opts.kernel, st);
+    p->A.d.err = p->derr;
+    p->AT.d.err = p->derr + 1;
     if (rc) {
         p->A.release();
         p->AT.release();
@@ -535,6 +580,7 @@ cbspmv_status cbspmv_spmv_noalloc(cbspmv_plan *p, const void *x, void *y, int nr
     cudaGetDevice(&dev);
     if (dev != p->device)
         return fail(CBSPMV_ERR_STATE, "plan was uploaded to another device");
+    if (cbspmv_status rc = take_device_error(p, 0, (cudaStream_t)stream)) return rc;
     const size_t need = cb::fixed_scratch_need(s.lay.gb_m, s.lay.slots, nrhs, s.lay.bs,
                                                s.lay.f32);
     if (need > cb::kFixedScratchBytes)
@@ -549,6 +595,18 @@ cbspmv_status cbspmv_spmv_noalloc(cbspmv_plan *p, const void *x, void *y, int nr
             "spmv_noalloc launch");
     return CBSPMV_OK;
 }
+
+cbspmv_status cbspmv_check(cbspmv_plan *p, void *stream) {
+    if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
+    if (!p->uploaded) return CBSPMV_OK;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    CB_CUDA(cudaStreamSynchronize(st), "check: synchronize");
+    if (p->pipe.comp) CB_CUDA(cudaStreamSynchronize(p->pipe.comp), "check: synchronize");
+    if (p->adj) CB_CUDA(cudaStreamSynchronize(p->adj), "check: synchronize");
+    return device_errors(p, st);
+}
+
+void cbspmv_debug_wait_polls(int64_t polls) { cb::set_wait_polls(polls); }
 
 cbspmv_status cbspmv_autotune(cbspmv_plan *p, int nrhs, void *stream, int *kernel, double *ms) {
     if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
@@ -651,7 +709,7 @@ cbspmv_status cbspmv_spmv_host(cbspmv_plan *p, const void *x_host, void *y_host,
     if (rc) return rc;
     if (yb) CB_CUDA(cudaMemcpyAsync(y_host, p->hy, yb, cudaMemcpyDeviceToHost, st), "copy y");
     CB_CUDA(cudaStreamSynchronize(st), "spmv_host");
-    return CBSPMV_OK;
+    return take_device_error(p, 0, st);
 }
 
 cbspmv_status cbspmv_spmv_host_async(cbspmv_plan *p, const void *x_host, void *y_host,
@@ -735,6 +793,7 @@ cbspmv_status cbspmv_cb_spmv(cbspmv_plan *p, const double *x, double *y,
     cudaEventDestroy(b);
     if (rc) return rc;
     if (e != cudaSuccess) return cuda_fail(e, "timing");
+    if ((rc = take_device_error(p, 0, nullptr))) return rc;
     if (metrics) {
         metrics->runtime_ms = ms / 1000.0;
         if (metrics->runtime_ms > 0)

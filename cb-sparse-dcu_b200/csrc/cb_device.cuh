@@ -46,6 +46,33 @@ __device__ __forceinline__ void add_entries(T *myacc, const uint32_t *w, const T
         if (f[u]) myacc[r[u] * 32] = a[u] + s[u];
 }
 
+// One 32-entry step of a row-sorted COO section: lane l holds one entry, its
+// row r (rows never decrease across the lanes; r >= BS marks a lane with no
+// entry, and such lanes come last) and its product p.  The entries of one row
+// are a run of lanes: an inclusive segmented scan -- shuffle levels 1, 2, 4,
+// ... up to the longest run -- leaves each run's sum in its last lane, which
+// adds it into the row's accumulator acc[r] (one per row, shared by the
+// warp).  Distinct runs are distinct rows, so no two lanes of one step touch
+// the same accumulator; the closing __syncwarp orders this step's updates
+// before the next step's, whose run of a row may end in another lane.  The
+// sum's order is fixed by the layout, so results are bitwise reproducible.
+template <typename T, int BS>
+__device__ __forceinline__ void seg_add(T *acc, uint32_t r, T p, int lane) {
+    const uint32_t rprev = __shfl_up_sync(kFull, r, 1);
+    const uint32_t heads = __ballot_sync(kFull, lane == 0 || rprev != r);
+    const int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+    const uint32_t longest = __reduce_max_sync(kFull, (uint32_t)(lane - start + 1));
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        if ((uint32_t)d >= longest) break;
+        const T t = __shfl_up_sync(kFull, p, d);
+        if (lane - d >= start) p += t;
+    }
+    const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+    if (tail && r < (uint32_t)BS) acc[r] += p;
+    __syncwarp();
+}
+
 // Element (r, c) of a DENSE block payload: bs*bs values, or for a unit-valued
 // plan a bs*bs-bit mask (bit r*bs + c) of the entries equal to 1.
 template <typename T, int BS>
@@ -193,10 +220,15 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
         "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
         : "memory");
 }
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t *err) {
-    for (uint32_t i = 0; i < kWaitLimit; ++i)
+// Waits for the phase `parity` of `bar` to complete, polling at most `limit`
+// times; on give-up sets *err (the launch's error word: host-mapped memory the
+// host reads without a copy, or device memory) and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t *err,
+                                          uint32_t limit = kWaitLimit) {
+    for (uint32_t i = 0; i < limit; ++i)
         if (mbar_try_wait(bar, parity)) return true;
-    atomicExch(err, 1u);
+    *reinterpret_cast<volatile uint32_t *>(err) = 1u;
+    __threadfence_system();
     return false;
 }
 

@@ -28,7 +28,9 @@
 #include <atomic>
 #include <cstdint>
 #include <cstdlib>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <type_traits>
 #include <vector>
 
@@ -258,17 +260,20 @@ __global__ void __launch_bounds__(kWarps * 32, 4)
 //     multicast), so the HBM stream runs a tile ahead of the compute;
 //   * each warp owns a contiguous, cost-balanced range of tiles computed on
 //     the host for the launch's grid (no shared counter: same-address atomics
-//     on one counter cannot keep up with ~10^5 tiles per launch), and loads
-//     tile descriptors two tiles ahead of use;
-//   * the x gathers of a chunk are the only global loads on the entry path;
+//     on one counter cannot keep up with ~10^5 tiles per launch);
+//   * a tile's COO entries are stored sorted by (row, column) and taken 32 at
+//     a time, one per lane, so the rows of a step never decrease across the
+//     lanes: the products of one row are a run of lanes, summed by a
+//     segmented shuffle scan, and the run's last lane adds the sum into the
+//     warp's single accumulator of that row (bs values in shared memory);
 //   * consecutive tiles of one block row in a warp's range keep adding into
 //     the same accumulators; only a block row that crosses a warp boundary
 //     leaves one partial sum per warp, and the last of those warps to arrive
 //     on the row's counter adds them in tile order (no tile waits on another).
-// Every mbarrier wait is bounded (kWaitLimit polls); on give-up the error
-// word sched[2] is set and the warp stops, after waiting (bounded) for its
-// own copies in flight.  sched[0..1] are not used by this kernel; the
-// per-block-row arrival counters return to zero by the end of every launch.
+// Every mbarrier wait is bounded (`limit` polls); on give-up the error word
+// is set and the warp stops, after waiting (kWaitLimit polls at most) for
+// its own copies in flight.  The per-block-row arrival counters return to
+// zero by the end of every launch that completes.
 // ============================================================================
 using dev::bulk_g2s;
 using dev::fence_mbar_init;
@@ -279,128 +284,99 @@ using dev::mbar_arrive_tx;
 using dev::mbar_init;
 using dev::mbar_wait;
 using dev::policy_evict_first;
+using dev::seg_add;
 constexpr int kStreamWarps = 4;  // warps per CTA
+constexpr int kStreamSteps = 8;  // 32-entry steps: tiles hold <= 256 COO entries
+constexpr uint32_t kNoRow = 63;  // row of a lane past the end of a COO section
 
-// Per-warp shared memory: [acc | xt | mbar[2] | buf[2]]; a buffer holds one
-// tile's COO section (`cap` bytes: indices, then values).
+// Per-warp shared memory: [acc | xt | mbar[2] | buf[2]].  acc: the warp's bs
+// row accumulators; xt: x columns of a tile's CSR/DENSE blocks (only when the
+// layout has such blocks, has_x); buf: one tile's COO section (`cap` bytes:
+// indices, then values).
 template <typename T, int BS>
 struct StreamLayout {
-    static constexpr uint32_t acc_bytes = BS * 32 * sizeof(T);
+    static constexpr uint32_t acc_bytes = a16(BS * sizeof(T));
     static constexpr uint32_t xt_bytes = max_xt(BS) * BS * sizeof(T);
-    static constexpr uint32_t head = a16(acc_bytes + xt_bytes + 16);
-    __host__ __device__ static uint32_t bytes(uint32_t cap) { return head + 2 * cap; }
+    __host__ __device__ static uint32_t head(int has_x) {
+        return acc_bytes + (has_x ? xt_bytes : 0u) + 16u;
+    }
+    __host__ __device__ static uint32_t bytes(uint32_t cap, int has_x) {
+        return a16(head(has_x)) + 2 * cap;
+    }
 };
 
-constexpr int kStreamChunk = 8;  // entries per lane: tiles hold <= 256 entries
-
-// One tile's COO entries held in registers: index words, values, gathered x.
-template <typename T>
-struct Staged {
-    uint32_t w[kStreamChunk];
-    T v[kStreamChunk];
-    T x[kStreamChunk];
-};
-
-// Reads a staged COO section into registers and issues its x gathers (the
-// loads stay in flight until the values are used).
-template <typename T>
-__device__ __forceinline__ void gather_tile(const unsigned char *buf, int E, int unit,
-                                            const T *__restrict__ x, int lane,
-                                            Staged<T> &g) {
-    const uint32_t *sidx = reinterpret_cast<const uint32_t *>(buf);
-    const T *sval = reinterpret_cast<const T *>(buf + a16(4u * E));
-#pragma unroll
-    for (int u = 0; u < kStreamChunk; ++u) {
-        const int e = u * 32 + lane;
-        g.w[u] = e < E ? sidx[e] : 0u;
-        g.v[u] = e < E ? (unit ? T(1) : sval[e]) : T(0);
-    }
-#pragma unroll
-    for (int u = 0; u < kStreamChunk; ++u) {
-        const int e = u * 32 + lane;
-        g.x[u] = e < E ? ldg(&x[g.w[u] & kColMask]) : T(0);
-    }
-}
-
-// Adds a gathered tile into the lane-private accumulators, handles its CSR and
-// DENSE blocks, reduces and stores (or leaves a split row's partials).
+// CSR and DENSE blocks of a tile (read from global memory, their x columns
+// staged in xts), added into the warp's row accumulators.  32 / bs lanes per
+// row (the reference's LANES_PER_ROW, macros.h:84, re-derived for 32-lane
+// warps): a CSR row's entries are split over them, a DENSE row's columns in
+// halves (bs = 16); the lanes of a row meet by a shuffle and the first adds.
 template <typename T, int BS>
-__device__ __forceinline__ void add_tile(const uint4 ta, const uint4 tb, const Staged<T> &g,
-                                         T *acc, T *xts, const uint4 *__restrict__ blocks,
-                                         const uint8_t *__restrict__ payload,
-                                         const int32_t *__restrict__ block_cols, int gather,
-                                         int unit, const T *__restrict__ x, int lane) {
-    T *myacc = &acc[lane];  // row r at myacc[r * 32]
-    const int E = (int)tb.x;
-    add_entries<T, kStreamChunk>(myacc, g.w, g.v, g.x, lane, 32, E);
+__device__ __forceinline__ void stream_blocks(const uint4 ta, T *acc, T *xts,
+                                              const uint4 *__restrict__ blocks,
+                                              const uint8_t *__restrict__ payload,
+                                              const int32_t *__restrict__ block_cols,
+                                              int gather, int unit, const T *__restrict__ x,
+                                              int lane) {
     const int ncoo = (ta.z >> 8) & 0xff;
     const int nxtb = (ta.z >> 16) & 0xff;
-    if (nxtb) {  // CSR and DENSE blocks, read from global memory
-        const uint4 bd =
-            lane < nxtb ? __ldg(&blocks[ta.x + ncoo + lane]) : make_uint4(0, 0, 0, 0);
-        for (int t0 = 0; t0 < nxtb * BS; t0 += 32) {
-            const int t = t0 + lane;
-            const int jb = min(t / BS, nxtb - 1);
-            const uint32_t xb = __shfl_sync(kFull, bd.z, jb);
-            const uint32_t mb = __shfl_sync(kFull, bd.y, jb);
-            const int c = t % BS;
-            if (t < nxtb * BS) {
-                T xv = T(0);
-                if (c < (int)((mb >> 14) & 63)) {
-                    const int64_t col = gather ? (int64_t)__ldg(&block_cols[xb + c])
-                                               : (int64_t)(xb + c);
-                    xv = ldg(&x[col]);
-                }
-                xts[t] = xv;
+    const uint4 bd =
+        lane < nxtb ? __ldg(&blocks[ta.x + ncoo + lane]) : make_uint4(0, 0, 0, 0);
+    for (int t0 = 0; t0 < nxtb * BS; t0 += 32) {
+        const int t = t0 + lane;
+        const int jb = min(t / BS, nxtb - 1);
+        const uint32_t xb = __shfl_sync(kFull, bd.z, jb);
+        const uint32_t mb = __shfl_sync(kFull, bd.y, jb);
+        const int c = t % BS;
+        if (t < nxtb * BS) {
+            T xv = T(0);
+            if (c < (int)((mb >> 14) & 63)) {
+                const int64_t col = gather ? (int64_t)__ldg(&block_cols[xb + c])
+                                           : (int64_t)(xb + c);
+                xv = ldg(&x[col]);
             }
-        }
-        __syncwarp();
-        const uint8_t *gbase = payload + (size_t)ta.w * 16;
-        for (int jb = 0; jb < nxtb; ++jb) {
-            const uint32_t off = __shfl_sync(kFull, bd.x, jb);
-            const uint32_t mb = __shfl_sync(kFull, bd.y, jb);
-            const int k = (mb >> 3) & 2047;
-            const uint8_t *pb = gbase + off;
-            const T *xt = &xts[jb * BS];
-            if ((mb & 3) == 1) {
-                using IdxT = typename std::conditional<BS == 16, uint8_t, uint16_t>::type;
-                const IdxT *rp = reinterpret_cast<const IdxT *>(pb);
-                const IdxT *ci = rp + BS + 1;
-                const T *vv = reinterpret_cast<const T *>(
-                    pb + a16((uint32_t)((BS + 1 + k) * sizeof(IdxT))));
-                constexpr int L = 32 / BS;
-                const int row = lane / L, sub = lane % L;
-                const int kb = __ldg(&rp[row]), ke = __ldg(&rp[row + 1]);
-                T sum = T(0);
-                for (int q = kb + sub; q < ke; q += L)
-                    sum += (unit ? T(1) : __ldg(&vv[q])) * xt[__ldg(&ci[q])];
-                myacc[row * 32] += sum;
-            } else {
-                T sum = T(0);
-                if (BS == 16) {
-                    const int row = lane >> 1, cc = (lane & 1) * 8;
-#pragma unroll
-                    for (int c = 0; c < 8; ++c)
-                        sum += dense_at<T, BS>(pb, unit, row, cc + c) * xt[cc + c];
-                    myacc[row * 32] += sum;
-                } else {
-#pragma unroll 8
-                    for (int c = 0; c < BS; ++c) sum += dense_at<T, BS>(pb, unit, lane, c) * xt[c];
-                    myacc[lane * 32] += sum;
-                }
-            }
+            xts[t] = xv;
         }
     }
+    __syncwarp();
+    constexpr int L = 32 / BS;  // lanes per row
+    const int row = lane / L, sub = lane % L;
+    const uint8_t *gbase = payload + (size_t)ta.w * 16;
+    for (int jb = 0; jb < nxtb; ++jb) {
+        const uint32_t off = __shfl_sync(kFull, bd.x, jb);
+        const uint32_t mb = __shfl_sync(kFull, bd.y, jb);
+        const int k = (mb >> 3) & 2047;
+        const uint8_t *pb = gbase + off;
+        const T *xt = &xts[jb * BS];
+        T sum = T(0);
+        if ((mb & 3) == 1) {
+            using IdxT = typename std::conditional<BS == 16, uint8_t, uint16_t>::type;
+            const IdxT *rp = reinterpret_cast<const IdxT *>(pb);
+            const IdxT *ci = rp + BS + 1;
+            const T *vv = reinterpret_cast<const T *>(
+                pb + a16((uint32_t)((BS + 1 + k) * sizeof(IdxT))));
+            const int kb = __ldg(&rp[row]), ke = __ldg(&rp[row + 1]);
+            for (int q = kb + sub; q < ke; q += L)
+                sum += (unit ? T(1) : __ldg(&vv[q])) * xt[__ldg(&ci[q])];
+        } else {
+            constexpr int W = BS / L;  // columns per lane
+#pragma unroll 8
+            for (int c = 0; c < W; ++c)
+                sum += dense_at<T, BS>(pb, unit, row, sub * W + c) * xt[sub * W + c];
+        }
+        if (L == 2) sum += __shfl_xor_sync(kFull, sum, 1);
+        if (sub == 0) acc[row] += sum;
+    }
+    __syncwarp();  // xts is rewritten by the next tile
 }
 
 // Ends a run of consecutive tiles of one block row in this warp (the last
-// tile `tg`, global index; `runlen` tiles): reduces the accumulators and
-// stores the rows.  A run that holds the whole block row stores y.  Otherwise
-// the row crosses a warp boundary: the run's sum goes to the slot of its first
-// tile, and the last run to arrive on the row's counter adds the row's run
-// sums in tile order and stores y.  Runs start at the row's first tile and at
-// every warp boundary inside the row (wpart), so the order does not depend on
-// which warp arrives last.
+// tile `tg`, global index; `runlen` tiles): reads and clears the warp's row
+// accumulators and stores the rows.  A run that holds the whole block row
+// stores y.  Otherwise the row crosses a warp boundary: the run's sum goes to
+// the slot of its first tile, and the last run to arrive on the row's counter
+// adds the row's run sums in tile order and stores y.  Runs start at the
+// row's first tile and at every warp boundary inside the row (wpart), so the
+// order does not depend on which warp arrives last.
 template <typename T, int BS>
 __device__ __forceinline__ void store_run(const uint4 ta, const uint4 tb, int64_t tg,
                                           int64_t runlen, T *acc, T *__restrict__ y,
@@ -409,7 +385,11 @@ __device__ __forceinline__ void store_run(const uint4 ta, const uint4 tb, int64_
                                           const uint32_t *__restrict__ wpart, int64_t gw,
                                           int lane) {
     __syncwarp();
-    const T sum = reduce_rows<T, BS>(acc, lane);
+    T sum = T(0);
+    if (lane < BS) {
+        sum = acc[lane];
+        acc[lane] = T(0);
+    }
     __syncwarp();
     const int64_t grow = (int64_t)ta.y * BS + lane;
     if (tb.y == 0xffffffffu || runlen == (int64_t)tb.w) {
@@ -446,34 +426,36 @@ __device__ __forceinline__ void store_run(const uint4 ta, const uint4 tb, int64_
     if (lane == 0) atomicExch(&counters[ta.y], 0);
 }
 
-// Warp w processes its tiles i = 0, 1, ... of wpart[w] .. wpart[w+1] in a
-// software pipeline: in step i it waits for tile i+1's staged COO section,
-// reads it into registers and issues its x gathers, starts the bulk copy of
-// tile i+3 into the buffer just read, and only then adds up tile i (whose
-// gathers were issued one step earlier).  Tile i lives in buffer i % 2.
+// Warp w processes its tiles i = 0, 1, ... of wpart[w] .. wpart[w+1]: it
+// waits for tile i's staged COO section, reads the section's indices and
+// issues all of its x gathers (up to 8 per lane), adds the steps up as the
+// gathers return (values read from the staged section), handles the tile's
+// CSR/DENSE blocks, and then starts the bulk copy of tile i+2 into the buffer
+// it has just finished with.  Tile i lives in buffer i % 2.  The descriptors
+// of tiles i .. i+3 are held one word per lane (lanes 8s .. 8s+7 hold the
+// tile in slot s = index % 4) and read by shuffles.
 template <typename T, int BS>
-__global__ void __launch_bounds__(kStreamWarps * 32)
+__global__ void __launch_bounds__(kStreamWarps * 32, 8)
     cb_spmv_stream_kernel(const uint4 *__restrict__ tiles, int64_t ntiles,
                           const uint4 *__restrict__ blocks,
                           const uint8_t *__restrict__ payload,
                           const int32_t *__restrict__ block_cols, int gather,
                           const T *__restrict__ x, T *__restrict__ y, int64_t m,
                           T *__restrict__ partials, int32_t *__restrict__ counters,
-                          uint32_t *__restrict__ sched,
-                          const uint32_t *__restrict__ wpart, uint32_t cap, int unit) {
+                          uint32_t *__restrict__ err, const uint32_t *__restrict__ wpart,
+                          uint32_t cap, int has_x, int unit, uint32_t limit) {
     using SL = StreamLayout<T, BS>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    unsigned char *wbase = smem_raw + (size_t)wib * SL::bytes(cap);
+    unsigned char *wbase = smem_raw + (size_t)wib * SL::bytes(cap, has_x);
     T *acc = reinterpret_cast<T *>(wbase);
     T *xts = reinterpret_cast<T *>(wbase + SL::acc_bytes);
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(wbase + SL::acc_bytes + SL::xt_bytes);
-    unsigned char *const buf0 = wbase + SL::head;  // buffer b at buf0 + b * cap
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(wbase + SL::head(has_x) - 16);
+    unsigned char *const buf0 = wbase + a16(SL::head(has_x));  // buffer b at buf0 + b * cap
     constexpr uint32_t vsz = sizeof(T);
-    const uint64_t pol = policy_evict_first();
 
-    for (int t = lane; t < 32 * BS; t += 32) acc[t] = T(0);
+    if (lane < BS) acc[lane] = T(0);
     if (lane == 0) {
         mbar_init(&mbar[0], 1);
         mbar_init(&mbar[1], 1);
@@ -485,84 +467,98 @@ __global__ void __launch_bounds__(kStreamWarps * 32)
     const int64_t t0 = __ldg(&wpart[gw]);
     const int64_t nt = min((int64_t)__ldg(&wpart[gw + 1]), ntiles) - t0;  // my tiles
     if (nt <= 0) return;
-    auto desc = [&](int64_t i, uint4 &a, uint4 &b) {
-        if (i < nt) {
-            a = __ldg(&tiles[2 * (t0 + i)]);
-            b = __ldg(&tiles[2 * (t0 + i) + 1]);
-        }
+    const uint32_t *tw = reinterpret_cast<const uint32_t *>(tiles) + 8 * t0;
+    uint32_t ring = 0;
+    auto fetch = [&](int64_t k) {  // descriptor of tile k into slot k % 4
+        if (k < nt && (lane >> 3) == (int)(k & 3)) ring = __ldg(&tw[8 * k + (lane & 7)]);
     };
-    auto stage = [&](const uint4 &a, const uint4 &b, int bi) {
+    auto field = [&](int64_t k, int f) -> uint32_t {
+        return __shfl_sync(kFull, ring, (int)((k & 3) << 3) | f);
+    };
+    auto stage = [&](int64_t k, int bi) {  // tile k's COO section into buffer bi
+        const uint32_t E = field(k, 4), p16 = field(k, 3);
         if (lane == 0) {
-            const uint32_t bytes = a16(4u * b.x) + (unit ? 0u : a16(vsz * b.x));
+            const uint32_t bytes = a16(4u * E) + (unit ? 0u : a16(vsz * E));
             if (bytes == 0) {
                 mbar_arrive(&mbar[bi]);
             } else {
                 fence_proxy_async();  // the buffer's previous tile was read
                 mbar_arrive_tx(&mbar[bi], bytes);
-                bulk_g2s(buf0 + bi * cap, payload + (size_t)a.w * 16, bytes, &mbar[bi], pol);
+                bulk_g2s(buf0 + bi * cap, payload + (size_t)p16 * 16, bytes, &mbar[bi],
+                         policy_evict_first());
             }
         }
     };
     uint32_t phase = 0u;     // bit b: parity to wait for on mbar[b]
     uint32_t inflight = 0u;  // bit b: a copy into buffer b is outstanding
-    auto wait_buf = [&](int bi) -> bool {
-        const bool ok = mbar_wait(&mbar[bi], (phase >> bi) & 1u, &sched[2]);
-        phase ^= 1u << bi;
-        inflight &= ~(1u << bi);
-        return ok;
-    };
 
-    // descriptors of tiles i .. i+4 (d0 = the tile being added up)
-    uint4 a0 = make_uint4(0, 0, 0, 0), b0 = a0, a1 = a0, b1 = a0, a2 = a0, b2 = a0,
-          a3 = a0, b3 = a0, a4 = a0, b4 = a0;
-    desc(0, a0, b0);
-    desc(1, a1, b1);
-    desc(2, a2, b2);
-    desc(3, a3, b3);
-    stage(a0, b0, 0);
+    fetch(0);
+    fetch(1);
+    fetch(2);
+    fetch(3);
+    stage(0, 0);
     inflight |= 1u;
     if (nt > 1) {
-        stage(a1, b1, 1);
+        stage(1, 1);
         inflight |= 2u;
     }
-    Staged<T> g0, g1;  // tile i's registers, tile i+1's registers
-    bool ok = wait_buf(0);
-    if (ok) gather_tile(buf0, (int)b0.x, unit, x, lane, g0);
-    __syncwarp();
-    if (ok && nt > 2) {
-        stage(a2, b2, 0);
-        inflight |= 1u;
-    }
     int64_t runlen = 0;  // tiles of the current block row added so far
-    for (int64_t i = 0; ok && i < nt; ++i) {
-        const int nb = (int)((i + 1) & 1);  // buffer of tile i+1
-        desc(i + 4, a4, b4);
-        if (i + 1 < nt) {
-            if (!wait_buf(nb)) break;
-            gather_tile(buf0 + nb * cap, (int)b1.x, unit, x, lane, g1);
-            __syncwarp();
-            if (i + 3 < nt) {
-                stage(a3, b3, nb);
-                inflight |= 1u << nb;
+    for (int64_t i = 0; i < nt; ++i) {
+        const int bi = (int)(i & 1);
+        // on give-up the copy into buffer bi may still be landing: leave it
+        // marked in flight (same parity) for the drain below
+        if (!mbar_wait(&mbar[bi], (phase >> bi) & 1u, err, limit)) break;
+        phase ^= 1u << bi;
+        inflight &= ~(1u << bi);
+        const unsigned char *buf = buf0 + bi * cap;
+        const int E = (int)field(i, 4);
+        const uint32_t *sidx = reinterpret_cast<const uint32_t *>(buf);
+        const T *sval = reinterpret_cast<const T *>(buf + a16(4u * E));
+        uint32_t w[kStreamSteps];
+        T xv[kStreamSteps];
+#pragma unroll
+        for (int u = 0; u < kStreamSteps; ++u) {
+            const int e = u * 32 + lane;
+            w[u] = e < E ? sidx[e] : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < kStreamSteps; ++u) {
+            const int e = u * 32 + lane;
+            xv[u] = e < E ? ldg(&x[w[u] & kColMask]) : T(0);
+        }
+        // COO entries: each adds val * x[col] into its row (the reference's
+        // per-entry accumulate_output, cb-spmv-dcu.hpp:423-426), here summed
+        // per run of equal rows across the lanes first
+#pragma unroll
+        for (int u = 0; u < kStreamSteps; ++u) {
+            if (u * 32 < E) {
+                const int e = u * 32 + lane;
+                const bool valid = e < E;
+                const T v = unit ? T(1) : (valid ? sval[e] : T(0));
+                seg_add<T, BS>(acc, valid ? (w[u] >> 27) : kNoRow, v * xv[u], lane);
             }
         }
-        add_tile<T, BS>(a0, b0, g0, acc, xts, blocks, payload, block_cols, gather, unit, x,
-                        lane);
+        const uint4 ta = make_uint4(field(i, 0), field(i, 1), field(i, 2), field(i, 3));
+        if ((ta.z >> 16) & 0xff)
+            stream_blocks<T, BS>(ta, acc, xts, blocks, payload, block_cols, gather, unit, x,
+                                 lane);
+        __syncwarp();
+        if (i + 2 < nt) {
+            stage(i + 2, bi);
+            inflight |= 1u << bi;
+        }
         ++runlen;
-        if (i + 1 >= nt || a1.y != a0.y) {  // the row's run in this warp ends here
-            store_run<T, BS>(a0, b0, t0 + i, runlen, acc, y, m, partials, counters, wpart, gw,
+        if (i + 1 >= nt || field(i + 1, 1) != ta.y) {  // the row's run in this warp ends here
+            const uint4 tb = make_uint4(E, field(i, 5), field(i, 6), field(i, 7));
+            store_run<T, BS>(ta, tb, t0 + i, runlen, acc, y, m, partials, counters, wpart, gw,
                              lane);
             runlen = 0;
         }
-        g0 = g1;
-        a0 = a1; b0 = b1;
-        a1 = a2; b1 = b2;
-        a2 = a3; b2 = b3;
-        a3 = a4; b3 = b4;
+        fetch(i + 4);
     }
     // never leave with a bulk copy still writing this warp's buffers
     for (int q = 0; q < 2; ++q)
-        if ((inflight >> q) & 1u) mbar_wait(&mbar[q], (phase >> q) & 1u, &sched[2]);
+        if ((inflight >> q) & 1u) mbar_wait(&mbar[q], (phase >> q) & 1u, err, kWaitLimit);
     __syncwarp();
 }
 
@@ -653,23 +649,12 @@ template <typename T, int BS, int CH>
 cudaError_t launch_chunk(const DevLayout &d, const void *x, void *y, int nrhs,
                          int64_t ldx, int64_t ldy, cudaStream_t stream) {
     const size_t smem = sizeof(WarpSmem<T, BS>) * kWarps;
-    static int resident = 0;  // CTAs per SM, per instantiation
-    static int sms = 0;
-    if (!resident) {
-        cudaError_t e = cudaFuncSetAttribute(cb_spmv_tile_kernel<T, BS, CH>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, cb_spmv_tile_kernel<T, BS, CH>,
-                                                      kWarps * 32, smem);
-        if (resident < 1) resident = 1;
-    }
+    const void *fn = reinterpret_cast<const void *>(cb_spmv_tile_kernel<T, BS, CH>);
+    cudaError_t e = dev_enable_smem(fn, smem);
+    if (e != cudaSuccess) return e;
     if (nrhs != 1 || !d.dunit) return cudaErrorInvalidValue;
     int64_t grid = (d.ndunits + kWarps - 1) / kWarps;
-    grid = std::min<int64_t>(grid, (int64_t)sms * resident);
+    grid = std::min<int64_t>(grid, (int64_t)dev_sms() * dev_resident(fn, kWarps * 32, smem));
     if (grid == 0) return cudaSuccess;
     cb_spmv_tile_kernel<T, BS, CH><<<(unsigned)grid, kWarps * 32, smem, stream>>>(
         static_cast<const uint4 *>(d.tiles), static_cast<const uint4 *>(d.blocks), d.payload,
@@ -684,11 +669,10 @@ cudaError_t launch_chunk(const DevLayout &d, const void *x, void *y, int nrhs,
 // types (measured fastest on CSR-heavy matrices; 6 and 8 also spill in
 // FP64); CBSPMV_CHUNK=4|6|8 overrides it for tuning.
 int chunk_choice() {
-    static int forced = -1;
-    if (forced < 0) {
+    static const int forced = [] {
         const char *e = std::getenv("CBSPMV_CHUNK");
-        forced = e ? std::atoi(e) : 0;
-    }
+        return e ? std::atoi(e) : 0;
+    }();
     if (forced == 4 || forced == 6 || forced == 8) return forced;
     return 4;
 }
@@ -704,30 +688,15 @@ template <typename T, int BS>
 cudaError_t stream_config(const DevLayout &d, StreamConfig<T, BS> &c) {
     using SL = StreamLayout<T, BS>;
     const uint32_t E = (uint32_t)d.max_entries;
-    c.cap = std::max<uint32_t>(16, a16(4u * E) + a16((uint32_t)sizeof(T) * E));
-    c.smem = (size_t)SL::bytes(c.cap) * kStreamWarps;
-    static size_t configured = 0;  // largest dynamic smem enabled so far
-    static int sms = 0;
-    if (c.smem > configured) {
-        cudaError_t e = cudaFuncSetAttribute(cb_spmv_stream_kernel<T, BS>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)c.smem);
-        if (e != cudaSuccess) return e;
-        configured = c.smem;
-    }
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    }
-    int resident = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &resident, cb_spmv_stream_kernel<T, BS>, kStreamWarps * 32, c.smem);
+    c.cap = std::max<uint32_t>(16, a16(4u * E) + (d.unit ? 0u : a16((uint32_t)sizeof(T) * E)));
+    c.smem = (size_t)SL::bytes(c.cap, d.has_x) * kStreamWarps;
+    const void *fn = reinterpret_cast<const void *>(cb_spmv_stream_kernel<T, BS>);
+    cudaError_t e = dev_enable_smem(fn, c.smem);
     if (e != cudaSuccess) return e;
-    if (resident < 1) resident = 1;
+    const int resident = dev_resident(fn, kStreamWarps * 32, c.smem);
     const int64_t need = (d.ntiles + kStreamWarps - 1) / kStreamWarps * kStreamWarps;
-    c.warps = std::max<int64_t>(kStreamWarps,
-                                std::min<int64_t>((int64_t)sms * resident * kStreamWarps, need));
+    c.warps = std::max<int64_t>(
+        kStreamWarps, std::min<int64_t>((int64_t)dev_sms() * resident * kStreamWarps, need));
     return cudaSuccess;
 }
 
@@ -737,14 +706,15 @@ cudaError_t launch_stream(const DevLayout &d, const void *x, void *y, cudaStream
     cudaError_t e = stream_config(d, c);
     if (e != cudaSuccess) return e;
     if (d.ntiles == 0) return cudaSuccess;
-    if (!d.wpart || d.nwarps % kStreamWarps || d.max_entries > 32 * kStreamChunk)
+    if (!d.wpart || d.nwarps % kStreamWarps || d.max_entries > 32 * kStreamSteps || !d.err)
         return cudaErrorInvalidValue;
     cb_spmv_stream_kernel<T, BS>
         <<<(unsigned)(d.nwarps / kStreamWarps), kStreamWarps * 32, c.smem, stream>>>(
             static_cast<const uint4 *>(d.tiles), d.ntiles,
             static_cast<const uint4 *>(d.blocks), d.payload, d.block_cols, d.gather,
             static_cast<const T *>(x), static_cast<T *>(y), d.m,
-            static_cast<T *>(d.partials), d.counters, d.sched, d.wpart, c.cap, d.unit);
+            static_cast<T *>(d.partials), d.counters, d.err, d.wpart, c.cap, d.has_x, d.unit,
+            wait_polls());
     note_launch();
     return cudaGetLastError();
 }
@@ -753,7 +723,7 @@ cudaError_t launch_stream(const DevLayout &d, const void *x, void *y, cudaStream
 // (or as chosen by the plan's kernel option; 3 = the staged kernel).
 // (single right-hand side; several go through the direct kernel)
 bool use_stream(const DevLayout &d) {
-    if (d.max_entries > 32 * kStreamChunk) return false;
+    if (d.max_entries > 32 * kStreamSteps) return false;
     if (d.kernel == 1) return true;
     if (d.kernel == 2 || d.kernel == 3) return false;
     return d.coo_share >= 0.5;
@@ -789,6 +759,65 @@ std::vector<uint32_t> direct_units(const uint32_t *tile8, int64_t ntiles) {
 
 int64_t kernel_launches() { return g_kernel_launches.load(); }
 void note_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
+
+namespace {
+std::mutex g_facts_mu;
+std::map<int, int> g_sms;                                    // device -> SMs
+std::map<std::pair<int, const void *>, size_t> g_smem;       // (device, kernel) -> enabled
+std::map<std::tuple<int, const void *, int, size_t>, int> g_resident;
+std::atomic<uint32_t> g_wait_polls{0};                       // 0: kWaitLimit
+
+int current_device() {
+    int d = 0;
+    cudaGetDevice(&d);
+    return d;
+}
+}  // namespace
+
+int dev_sms() {
+    const int d = current_device();
+    std::lock_guard<std::mutex> lock(g_facts_mu);
+    auto it = g_sms.find(d);
+    if (it != g_sms.end()) return it->second;
+    int s = 0;
+    cudaDeviceGetAttribute(&s, cudaDevAttrMultiProcessorCount, d);
+    return g_sms[d] = std::max(1, s);
+}
+
+cudaError_t dev_enable_smem(const void *fn, size_t smem) {
+    const int d = current_device();
+    std::lock_guard<std::mutex> lock(g_facts_mu);
+    size_t &have = g_smem[{d, fn}];
+    if (smem <= have) return cudaSuccess;
+    const cudaError_t e =
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) have = smem;
+    return e;
+}
+
+int dev_resident(const void *fn, int threads, size_t smem) {
+    const int d = current_device();
+    std::lock_guard<std::mutex> lock(g_facts_mu);
+    auto key = std::make_tuple(d, fn, threads, smem);
+    auto it = g_resident.find(key);
+    if (it != g_resident.end()) return it->second;
+    int r = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, fn, threads, smem) != cudaSuccess) {
+        cudaGetLastError();
+        r = 1;
+    }
+    return g_resident[key] = std::max(1, r);
+}
+
+uint32_t wait_polls() {
+    const uint32_t p = g_wait_polls.load(std::memory_order_relaxed);
+    return p ? p - 1 : dev::kWaitLimit;
+}
+
+void set_wait_polls(int64_t polls) {
+    g_wait_polls.store(polls < 0 ? 0u : (uint32_t)std::min<int64_t>(polls, dev::kWaitLimit) + 1u,
+                       std::memory_order_relaxed);
+}
 
 size_t spmv_smem_bytes(int bs, int f32) {
     if (bs == 16)
@@ -901,19 +930,10 @@ void grad_vals_go(int lp, int64_t nvals, const int32_t *vrow, const int32_t *vco
         cb_grad_vals_kernel<T, V, 1, U>, cb_grad_vals_kernel<T, V, 2, U>,
         cb_grad_vals_kernel<T, V, 4, U>, cb_grad_vals_kernel<T, V, 8, U>};
     auto kern = kerns[li];
-    static int resident[4] = {0, 0, 0, 0};  // blocks per SM, per instantiation
-    static int sms = 0;
-    if (!resident[li]) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        int r = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, kern, 256, 0);
-        resident[li] = r < 1 ? 1 : r;
-    }
+    const int resident = dev_resident(reinterpret_cast<const void *>(kern), 256, 0);
     const int64_t per_block = 256 / lp * U;
     const int64_t grid = std::min<int64_t>((nvals + per_block - 1) / per_block,
-                                           (int64_t)sms * resident[li]);
+                                           (int64_t)dev_sms() * resident);
     kern<<<(unsigned)grid, 256, 0, st>>>(nvals, vrow, vcol, gp, ldg, xp, ldx, nrhs, op);
 }
 

@@ -21,6 +21,8 @@ struct DevLayout {
     void *partials = nullptr;         // slots * bs values (scratch)
     int32_t *counters = nullptr;      // gb_m arrival counters (scratch)
     uint32_t *sched = nullptr;        // scheduler words (scratch, zeroed)
+    uint32_t *err = nullptr;          // error word: set when a bounded wait gives up
+    int has_x = 1;                    // the layout has CSR/DENSE blocks
     int64_t max_entries = 0;          // largest COO section of a tile
     int kernel = 0;                   // 0 auto, 1 streaming (TMA), 2 direct
     double coo_share = 1.0;
@@ -79,7 +81,7 @@ int64_t ms_tile_cost(const uint32_t *tile8, const uint32_t *blocks4);
 void ms_unit_starts(const uint32_t *tile8, int64_t ntiles, int64_t target, int64_t base,
                     std::vector<int64_t> &ustart);
 // Y = A X through the multi-right-hand-side kernel (d.mcap, d.ustart,
-// d.nunits set; scheduler words d.sched[0..1], error word d.sched[2]).
+// d.nunits set; scheduler words d.sched[0..1], error word d.err).
 cudaError_t launch_spmm(const DevLayout &d, const void *x, void *y, int nrhs, int64_t ldx,
                         int64_t ldy, cudaStream_t stream);
 // The same kernel over a device table of nmats matrices of one class: tile
@@ -132,6 +134,21 @@ cudaError_t launch_grad_vals(int f32, int64_t nvals, const int32_t *vrow,
 // note_launch() counts one.
 int64_t kernel_launches();
 void note_launch();
+
+// Launch facts of the current device, kept per device (a process may drive
+// several GPUs, and cudaFuncSetAttribute applies to the current device only):
+// its SM count; for a kernel, the dynamic shared memory enabled so far
+// (raised when a launch needs more) and its resident blocks per SM at a block
+// size and shared-memory size.  Thread-safe.
+int dev_sms();
+cudaError_t dev_enable_smem(const void *fn, size_t smem);
+int dev_resident(const void *fn, int threads, size_t smem);
+
+// Polls a bounded device wait makes before giving up (the kernels' `limit`
+// argument): dev::kWaitLimit unless set_wait_polls(p >= 0) set p for tests of
+// the give-up path; set_wait_polls(-1) restores the default.
+uint32_t wait_polls();
+void set_wait_polls(int64_t polls);
 
 // Dynamic shared memory of the SpMV kernel per CTA.
 size_t spmv_smem_bytes(int bs, int f32);

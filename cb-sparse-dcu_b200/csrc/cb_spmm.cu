@@ -422,7 +422,8 @@ __global__ void __launch_bounds__(kMsWarps * 32, 3)
     cb_mstream_kernel(const MatView single, const MatView *__restrict__ mats, int nmats,
                       const int64_t *__restrict__ toff, const int64_t *__restrict__ ustart,
                       int64_t nunits, int dynamic, uint32_t cap,
-                      uint32_t *__restrict__ sched) {
+                      uint32_t *__restrict__ sched, uint32_t *__restrict__ err,
+                      uint32_t limit) {
     using SL = MsLayout<T, BS, RL, V>;
     constexpr int RV = RL * V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -434,7 +435,6 @@ __global__ void __launch_bounds__(kMsWarps * 32, 3)
     uint64_t *mbar = reinterpret_cast<uint64_t *>(wbase + SL::acc_bytes + SL::xt_bytes);
     unsigned char *const buf0 = wbase + SL::head;
     const uint64_t pol = policy_evict_first();
-    uint32_t *err = &sched[2];
 
     for (int t = lane; t < BS * 32 * V; t += 32) acc[t] = T(0);
     if (lane == 0) {
@@ -561,10 +561,11 @@ __global__ void __launch_bounds__(kMsWarps * 32, 3)
             inflight |= 2u;
         }
         for (;;) {
-            const bool ok = mbar_wait(&mbar[bi], (phase >> bi) & 1u, err);
+            // on give-up the copy into buffer bi may still be landing: leave
+            // it marked in flight (same parity) for the drain below
+            if (!mbar_wait(&mbar[bi], (phase >> bi) & 1u, err, limit)) break;
             phase ^= 1u << bi;
             inflight &= ~(1u << bi);
-            if (!ok) break;
             const int k = bi ? sk1 : sk0;
             if (!one && k != mk) {
                 M = mats[k];
@@ -629,46 +630,34 @@ __global__ void __launch_bounds__(kMsWarps * 32, 3)
 
 template <typename T, int BS, int RL, int V>
 cudaError_t ms_configure(uint32_t cap, size_t *smem) {
-    static size_t configured = 0;  // largest dynamic smem enabled so far
     *smem = (size_t)MsLayout<T, BS, RL, V>::bytes(cap) * kMsWarps;
-    if (*smem > configured) {
-        cudaError_t e = cudaFuncSetAttribute(cb_mstream_kernel<T, BS, RL, V>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)*smem);
-        if (e != cudaSuccess) return e;
-        configured = *smem;
-    }
-    return cudaSuccess;
+    return dev_enable_smem(reinterpret_cast<const void *>(cb_mstream_kernel<T, BS, RL, V>),
+                           *smem);
 }
 
 template <typename T, int BS, int RL, int V>
 int64_t ms_warps_t(uint32_t cap) {
     size_t smem = 0;
     if (ms_configure<T, BS, RL, V>(cap, &smem) != cudaSuccess) return 0;
-    int devid = 0, sms = 0, resident = 0;
-    cudaGetDevice(&devid);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, devid);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, cb_mstream_kernel<T, BS, RL, V>,
-                                                  kMsWarps * 32, smem);
-    return (int64_t)std::max(1, resident) * sms * kMsWarps;
+    const int resident = dev_resident(
+        reinterpret_cast<const void *>(cb_mstream_kernel<T, BS, RL, V>), kMsWarps * 32, smem);
+    return (int64_t)resident * dev_sms() * kMsWarps;
 }
 
 template <typename T, int BS, int RL, int V>
 cudaError_t ms_launch_t(const MatView &single, const MatView *mats, int nmats,
                         const int64_t *toff, const int64_t *ustart, int64_t nunits, int dynamic,
-                        uint32_t cap, uint32_t *sched, cudaStream_t stream) {
+                        uint32_t cap, uint32_t *sched, uint32_t *err, cudaStream_t stream) {
     size_t smem = 0;
     cudaError_t e = ms_configure<T, BS, RL, V>(cap, &smem);
     if (e != cudaSuccess) return e;
-    if (cap % 16) return cudaErrorInvalidValue;
+    if (cap % 16 || !sched || !err) return cudaErrorInvalidValue;
     if (nunits <= 0) return cudaSuccess;
-    static int64_t warps = 0;  // resident warps, per instantiation
-    if (!warps) warps = ms_warps_t<T, BS, RL, V>(cap);
     // dynamic: resident warps (or fewer); static: one warp per unit
-    const int64_t w = dynamic ? std::min<int64_t>(warps, nunits) : nunits;
+    const int64_t w = dynamic ? std::min<int64_t>(ms_warps_t<T, BS, RL, V>(cap), nunits) : nunits;
     const int64_t ctas = (w + kMsWarps - 1) / kMsWarps;
     cb_mstream_kernel<T, BS, RL, V><<<(unsigned)ctas, kMsWarps * 32, smem, stream>>>(
-        single, mats, nmats, toff, ustart, nunits, dynamic, cap, sched);
+        single, mats, nmats, toff, ustart, nunits, dynamic, cap, sched, err, wait_polls());
     note_launch();
     return cudaGetLastError();
 }
@@ -778,7 +767,7 @@ cudaError_t launch_spmm(const DevLayout &d, const void *x, void *y, int nrhs, in
     return by_class(d.bs, d.f32, ms_class(nrhs, d.f32), [&](auto t, auto b, auto rl, auto v) {
         using T = decltype(t);
         return ms_launch_t<T, b(), rl(), v()>(M, nullptr, 1, nullptr, d.ustart, d.nunits, 0,
-                                              d.mcap, d.sched, stream);
+                                              d.mcap, d.sched, d.err, stream);
     });
 }
 
@@ -788,7 +777,7 @@ cudaError_t launch_batch(int bs, int f32, MsClass c, const MatView *mats, int nm
     return by_class(bs, f32, c, [&](auto t, auto b, auto rl, auto v) {
         using T = decltype(t);
         return ms_launch_t<T, b(), rl(), v()>(MatView(), mats, nmats, toff, ustart, nunits, 1,
-                                              cap, sched, stream);
+                                              cap, sched, sched + 2, stream);
     });
 }
 

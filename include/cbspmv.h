@@ -39,7 +39,9 @@ enum {
     CBSPMV_ERR_ALLOC = 4,       /* host or device allocation failed       */
     CBSPMV_ERR_CUDA = 5,        /* a CUDA runtime call failed             */
     CBSPMV_ERR_STATE = 6,       /* plan not uploaded / wrong value type   */
-    CBSPMV_ERR_UNSUPPORTED = 7  /* size beyond a documented limit         */
+    CBSPMV_ERR_UNSUPPORTED = 7, /* size beyond a documented limit         */
+    CBSPMV_ERR_DEVICE = 8       /* a bounded device wait gave up in an
+                                   earlier launch (see cbspmv_check)       */
 };
 
 enum { CBSPMV_F64 = 0, CBSPMV_F32 = 1 };
@@ -266,6 +268,23 @@ cbspmv_status cbspmv_destroy(cbspmv_plan *plan);
 /* Message of the calling thread's last error ("" if none); returns its full
  * length. */
 size_t cbspmv_last_error(char *buf, size_t len);
+
+/* Device-side failure reporting.  The kernels wait on their own bulk copies
+ * with bounded waits (no counterpart in the reference, whose row-epoch claim
+ * spins without bound, cb-spmv-dcu.hpp:238-282).  A wait that gives up sets
+ * an error word of the plan (host-mapped memory) and its warp stops, so the
+ * launch's output is incomplete.  cbspmv_check synchronizes `stream` (and the
+ * plan's own streams), and returns CBSPMV_ERR_DEVICE if a launch on the plan
+ * gave up since the last report, else CBSPMV_OK.  Every launching call also
+ * returns CBSPMV_ERR_DEVICE, without launching, when it finds the word set.
+ * Either report clears the word and resets the plan's scratch (arrival
+ * counters, scheduler words) on `stream`, so later calls run normally. */
+cbspmv_status cbspmv_check(cbspmv_plan *plan, void *stream);
+
+/* For tests of that path: the number of polls each device wait makes before
+ * it gives up (0: at once, even when the copy has landed); polls < 0 restores
+ * the default.  Process-wide; applies to launches made afterwards. */
+void cbspmv_debug_wait_polls(int64_t polls);
 
 /* Times the kernels that can run this plan for nrhs right-hand sides (one
  * vector: streaming when the layout allows it, direct, staged; several: the

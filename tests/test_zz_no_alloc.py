@@ -27,8 +27,8 @@ def _fn():
 
 
 @pytest.mark.parametrize("f32", [False, True])
-@pytest.mark.parametrize("nrhs", [1, 3])
-def test_noalloc_matches_spmv(cuda, f32, nrhs):
+@pytest.mark.parametrize("nrhs,kernel", [(1, 0), (1, 2), (3, 0)])
+def test_noalloc_matches_spmv(cuda, f32, nrhs, kernel):
     import torch
     import cbspmv
     import cbdump as cd
@@ -36,7 +36,7 @@ def test_noalloc_matches_spmv(cuda, f32, nrhs):
     # small tiles: many block rows are split, so the partials and counters in
     # the fixed scratch are exercised
     coo = gen.power_law(1 << 15, kmax=4096, band=1024, seed=5)
-    plan = cbspmv.Plan(coo, value_type=int(f32), tile_entries=64)
+    plan = cbspmv.Plan(coo, value_type=int(f32), tile_entries=64, kernel=kernel)
     assert plan.info()["split_rows"] > 0
     dt = torch.float32 if f32 else torch.float64
     X = gen.uniform_x(coo.n, 13, nrhs=max(nrhs, 2))[:nrhs]
@@ -60,6 +60,11 @@ def test_noalloc_matches_spmv(cuda, f32, nrhs):
         ref = want.cpu().numpy().reshape(coo.m, nrhs).T.astype(np.float64)
         assert np.all(np.abs(got - ref) <= TOL[f32] * ab + 1e-300), f"call {call}"
         assert np.all(np.abs(got - yref) <= TOL[f32] * ab + 1e-300), f"call {call}"
+        # the plan's own entry point between the calls is unaffected
+        y2 = plan.spmv(xd)
+        torch.cuda.synchronize()
+        got2 = y2.cpu().numpy().reshape(coo.m, nrhs).T.astype(np.float64)
+        assert np.all(np.abs(got2 - yref) <= TOL[f32] * ab + 1e-300), f"spmv after {call}"
 
 
 def test_noalloc_refuses_oversized_plan(cuda):
