@@ -46,30 +46,65 @@ __device__ __forceinline__ void add_entries(T *myacc, const uint32_t *w, const T
         if (f[u]) myacc[r[u] * 32] = a[u] + s[u];
 }
 
-// One 32-entry step of a row-sorted COO section: lane l holds one entry, its
-// row r (rows never decrease across the lanes; r >= BS marks a lane with no
-// entry, and such lanes come last) and its product p.  The entries of one row
-// are a run of lanes: an inclusive segmented scan -- shuffle levels 1, 2, 4,
-// ... up to the longest run -- leaves each run's sum in its last lane, which
-// adds it into the row's accumulator acc[r] (one per row, shared by the
-// warp).  Distinct runs are distinct rows, so no two lanes of one step touch
-// the same accumulator; the closing __syncwarp orders this step's updates
-// before the next step's, whose run of a row may end in another lane.  The
-// sum's order is fixed by the layout, so results are bitwise reproducible.
-template <typename T, int BS>
-__device__ __forceinline__ void seg_add(T *acc, uint32_t r, T p, int lane) {
-    const uint32_t rprev = __shfl_up_sync(kFull, r, 1);
-    const uint32_t heads = __ballot_sync(kFull, lane == 0 || rprev != r);
+// Adds a tile's COO section into the warp's row accumulators acc[0, BS)
+// (shared memory).  The section is stored in lane slices (coo_slice_pos in
+// cb_layout.hpp): lane l holds the consecutive entries of positions
+// 32 j + l < E, j = 0, 1, ... -- w[j] their index words (row << 27 | column),
+// xv[j] their gathered x values, sval the staged values (unused when unit).
+//   1. Each lane sums its slice along its rows in registers.  The slice's
+//      first row (the head) may have begun in earlier lanes and its last (the
+//      tail) may go on in later ones; rows that begin and end inside the slice
+//      are complete and the lane adds them into acc itself.
+//   2. A segmented shuffle scan over the lanes sums the tails of a row that
+//      runs across several lanes; the lane where such a row ends adds the
+//      row's total (a head that goes on from the previous lane takes that
+//      lane's running sum).
+// Every row of the tile is added into acc exactly once, by one lane, so the
+// lanes never write the same accumulator and the order of the sums is fixed
+// by the layout (bitwise reproducible results).  Ends with a __syncwarp.
+template <typename T, int BS, int K>
+__device__ __forceinline__ void slice_sums(T *acc, const uint32_t (&w)[K], const T (&xv)[K],
+                                           const T *sval, int unit, int E, int lane) {
+    constexpr uint32_t kNone = 63;  // row of an empty lane (after every real row)
+    const bool have = lane < E;
+    const uint32_t rh = have ? (w[0] >> 27) : kNone;  // head row
+    uint32_t rc = rh;                                 // row of the running sum
+    T run = have ? (unit ? T(1) : sval[lane]) * xv[0] : T(0);
+    T head = T(0);
+    bool split = false;  // the slice holds more than one row
+#pragma unroll
+    for (int j = 1; j < K; ++j) {
+        const int pos = 32 * j + lane;
+        if (32 * j < E && pos < E) {
+            const uint32_t r = w[j] >> 27;
+            const T p = (unit ? T(1) : sval[pos]) * xv[j];
+            if (r == rc) {
+                run += p;
+            } else {
+                if (split) acc[rc] += run;  // a row complete inside this slice
+                else head = run;
+                split = true;
+                rc = r;
+                run = p;
+            }
+        }
+    }
+    // rows across lanes: the running sum `run` of the tail row rc
+    const uint32_t rt_prev = __shfl_up_sync(kFull, rc, 1);
+    const uint32_t rh_next = __shfl_down_sync(kFull, rh, 1);
+    const bool cont = lane > 0 && rh == rt_prev;  // my head goes on from the previous lane
+    const uint32_t heads = __ballot_sync(kFull, !cont || split);
     const int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
     const uint32_t longest = __reduce_max_sync(kFull, (uint32_t)(lane - start + 1));
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
         if ((uint32_t)d >= longest) break;
-        const T t = __shfl_up_sync(kFull, p, d);
-        if (lane - d >= start) p += t;
+        const T t = __shfl_up_sync(kFull, run, d);
+        if (lane - d >= start) run += t;
     }
-    const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
-    if (tail && r < (uint32_t)BS) acc[r] += p;
+    const T prev = __shfl_up_sync(kFull, run, 1);
+    if (split) acc[rh] += cont ? head + prev : head;
+    if ((lane == 31 || rh_next != rc) && rc < (uint32_t)BS) acc[rc] += run;
     __syncwarp();
 }
 

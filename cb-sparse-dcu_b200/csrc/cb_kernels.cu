@@ -284,10 +284,9 @@ using dev::mbar_arrive_tx;
 using dev::mbar_init;
 using dev::mbar_wait;
 using dev::policy_evict_first;
-using dev::seg_add;
+using dev::slice_sums;
 constexpr int kStreamWarps = 4;  // warps per CTA
 constexpr int kStreamSteps = 8;  // 32-entry steps: tiles hold <= 256 COO entries
-constexpr uint32_t kNoRow = 63;  // row of a lane past the end of a COO section
 
 // Per-warp shared memory: [acc | xt | mbar[2] | buf[2]].  acc: the warp's bs
 // row accumulators; xt: x columns of a tile's CSR/DENSE blocks (only when the
@@ -517,27 +516,19 @@ __global__ void __launch_bounds__(kStreamWarps * 32, 8)
         uint32_t w[kStreamSteps];
         T xv[kStreamSteps];
 #pragma unroll
-        for (int u = 0; u < kStreamSteps; ++u) {
-            const int e = u * 32 + lane;
-            w[u] = e < E ? sidx[e] : 0u;
+        for (int j = 0; j < kStreamSteps; ++j) {
+            const int pos = 32 * j + lane;
+            w[j] = pos < E ? sidx[pos] : 0u;
         }
 #pragma unroll
-        for (int u = 0; u < kStreamSteps; ++u) {
-            const int e = u * 32 + lane;
-            xv[u] = e < E ? ldg(&x[w[u] & kColMask]) : T(0);
+        for (int j = 0; j < kStreamSteps; ++j) {
+            const int pos = 32 * j + lane;
+            xv[j] = pos < E ? ldg(&x[w[j] & kColMask]) : T(0);
         }
         // COO entries: each adds val * x[col] into its row (the reference's
         // per-entry accumulate_output, cb-spmv-dcu.hpp:423-426), here summed
-        // per run of equal rows across the lanes first
-#pragma unroll
-        for (int u = 0; u < kStreamSteps; ++u) {
-            if (u * 32 < E) {
-                const int e = u * 32 + lane;
-                const bool valid = e < E;
-                const T v = unit ? T(1) : (valid ? sval[e] : T(0));
-                seg_add<T, BS>(acc, valid ? (w[u] >> 27) : kNoRow, v * xv[u], lane);
-            }
-        }
+        // along the lane's slice first, then across lanes (slice_sums)
+        slice_sums<T, BS, kStreamSteps>(acc, w, xv, sval, unit, E, lane);
         const uint4 ta = make_uint4(field(i, 0), field(i, 1), field(i, 2), field(i, 3));
         if ((ta.z >> 16) & 0xff)
             stream_blocks<T, BS>(ta, acc, xts, blocks, payload, block_cols, gather, unit, x,

@@ -326,11 +326,12 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
                           (uint32_t)vc << 14 | steps << 20;
                 if (ty == kCOO) e0 += kk;
             }
-            // The tile's COO section is stored sorted by (row, column) over all
-            // of its COO blocks (keys are unique: distinct blocks hold distinct
-            // columns), so the entries a lane reads, 32 apart, never go down a
-            // row.  Stored value v keeps its block-major number; only its
-            // payload position moves.
+            // The tile's COO section holds the entries of all of its COO
+            // blocks sorted by (row, column) (keys are unique: distinct blocks
+            // hold distinct columns), cut into 32 lane slices of consecutive
+            // entries (coo_slice_pos), so a lane's entries never go down a row
+            // and a row's entries are one run of lanes.  Stored value v keeps
+            // its block-major number; only its payload position moves.
             if (E > 0) {
                 std::vector<uint64_t> key((size_t)E);
                 sorted_val.resize((size_t)E);
@@ -345,12 +346,13 @@ std::string build_layout(const HostCB &g, int f32, int tile_entries, int kernel,
                 }
                 for (int64_t q2 = 0; q2 < E; ++q2) {
                     const int64_t from = (int64_t)(key[q2] & 0xffff);
-                    idx[q2] = (uint32_t)(key[q2] >> 16);
+                    const int64_t pos = coo_slice_pos(q2, E);
+                    idx[pos] = (uint32_t)(key[q2] >> 16);
                     if (c.unit) {  // no value arrays: nothing to place
                         L.val_off[val + from] = 0;
                         continue;
                     }
-                    const int64_t at = byte + vals_at + q2 * vsz;
+                    const int64_t at = byte + vals_at + pos * vsz;
                     put_tile_val(at, sorted_val[from]);
                     L.val_off[val + from] = (uint64_t)at;
                 }

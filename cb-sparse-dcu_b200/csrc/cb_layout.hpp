@@ -37,6 +37,20 @@ constexpr int kTileEntriesStream = 256;  // the streaming kernel's default
 constexpr int kColBits = 27;  // COO idx: column in bits 0..26
 constexpr int64_t kMaxCols = int64_t(1) << kColBits;
 
+// Position of the e-th entry (in (row, column) order) of a tile's COO
+// section of E entries.  The section is cut into 32 lane slices of
+// consecutive entries -- K = ceil(E / 32) entries for the first
+// q = E - 32 (K - 1) lanes, K - 1 for the rest -- and entry j of lane l's
+// slice is stored at position 32 j + l.  A warp that reads positions
+// 32 j + lane (j = 0, 1, ...; valid while below E) is coalesced and gives
+// each lane its slice in order; the positions fill [0, E) exactly.
+inline int64_t coo_slice_pos(int64_t e, int64_t E) {
+    const int64_t K = (E + 31) / 32, q = E - 32 * (K - 1);
+    const int64_t l = e < q * K ? e / K : q + (e - q * K) / (K - 1);
+    const int64_t j = e < q * K ? e % K : (e - q * K) % (K - 1);
+    return 32 * j + l;
+}
+
 // 8 x u32 per tile
 struct TileDesc {
     uint32_t block_begin;  // first block (device order)

@@ -31,6 +31,6 @@ struct PlanImage {
 std::string save_plan(const PlanImage &img, const std::string &path);
 std::string load_plan(const std::string &path, PlanImage &img);
 
-constexpr uint32_t kPlanFileVersion = 3;
+constexpr uint32_t kPlanFileVersion = 4;
 
 }  // namespace cb

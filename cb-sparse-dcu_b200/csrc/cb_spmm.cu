@@ -144,22 +144,42 @@ __device__ __forceinline__ void ms_add(const MatView &M, const uint4 ta, const u
     // Tile entries are sorted by row, so a lane's slots never go down a row:
     // equal-row slots are summed in registers and each run adds once, all
     // accumulator loads ahead of the stores (distinct runs, distinct rows).
+    // The section is stored in 32 lane slices of consecutive entries
+    // (coo_slice_pos, cb_layout.hpp): slice s holds positions 32 j + s < E.
+    // Lane group es takes slices es, es + G, ..., es + G (RL - 1) in turn --
+    // its slots q = t Kt + j, slice es + G t, entry j -- so the rows of its
+    // slots never decrease, and each slot step of the warp reads G
+    // consecutive positions.
     const uint32_t *sidx = reinterpret_cast<const uint32_t *>(buf);
     const T *sval = reinterpret_cast<const T *>(buf + a16(4u * E));
     const int nv = max(0, min(V, M.nrhs - jb));  // this lane's right-hand sides
     const T *__restrict__ xr = static_cast<const T *>(M.x) + jb;
-    uint32_t w[KC];
-    T a[KC], xv[KC][V];
-    auto load = [&](int c0, uint32_t (&w_)[KC], T (&a_)[KC], T (&x_)[KC][V]) {
+    const int Kt = (E + 31) >> 5;  // entries of the longest slices
+    const int nslots = RL * Kt;
+    auto positions = [&](int c0, int (&p_)[KC]) {  // slots c0 .. c0+KC-1 (E: none)
+        int t = Kt ? c0 / Kt : RL, j = c0 - t * Kt;
 #pragma unroll
         for (int u = 0; u < KC; ++u) {
-            const int e = c0 + u * G + es;
+            p_[u] = t < RL ? 32 * j + es + G * t : E;
+            if (++j == Kt) {
+                j = 0;
+                ++t;
+            }
+        }
+    };
+    uint32_t w[KC];
+    T a[KC], xv[KC][V];
+    int pc[KC];
+    auto load = [&](const int (&p_)[KC], uint32_t (&w_)[KC], T (&a_)[KC], T (&x_)[KC][V]) {
+#pragma unroll
+        for (int u = 0; u < KC; ++u) {
+            const int e = p_[u];
             w_[u] = e < E ? sidx[e] : 0u;
             a_[u] = e < E ? (M.unit ? T(1) : sval[e]) : T(0);
         }
 #pragma unroll
         for (int u = 0; u < KC; ++u) {
-            const int e = c0 + u * G + es;
+            const int e = p_[u];
 #pragma unroll
             for (int v = 0; v < V; ++v) x_[u][v] = T(0);
             if (e < E && nv > 0) {
@@ -174,11 +194,16 @@ __device__ __forceinline__ void ms_add(const MatView &M, const uint4 ta, const u
             }
         }
     };
-    if (E > 0) load(0, w, a, xv);
-    for (int c0 = 0; c0 < E; c0 += CH) {
+    if (E > 0) {
+        positions(0, pc);
+        load(pc, w, a, xv);
+    }
+    for (int c0 = 0; c0 < nslots; c0 += KC) {
         uint32_t w2[KC];
         T a2[KC], x2[KC][V];
-        load(c0 + CH, w2, a2, x2);  // slots past E load nothing
+        int pn[KC];
+        positions(c0 + KC, pn);
+        load(pn, w2, a2, x2);  // slots past the last load nothing
         uint32_t r[KC];
         T s[KC][V];
         bool f[KC];
@@ -192,9 +217,9 @@ __device__ __forceinline__ void ms_add(const MatView &M, const uint4 ta, const u
         }
 #pragma unroll
         for (int u = 0; u < KC; ++u) {
-            const int e = c0 + u * G + es;
-            const bool more = u + 1 < KC && e + G < E && r[u + 1 < KC ? u + 1 : u] == r[u];
-            f[u] = e < E && !more;
+            const bool more = u + 1 < KC && pc[u + 1 < KC ? u + 1 : u] < E &&
+                              r[u + 1 < KC ? u + 1 : u] == r[u];
+            f[u] = pc[u] < E && !more;
         }
         T o[KC][V];
 #pragma unroll
@@ -218,6 +243,7 @@ __device__ __forceinline__ void ms_add(const MatView &M, const uint4 ta, const u
         for (int u = 0; u < KC; ++u) {
             w[u] = w2[u];
             a[u] = a2[u];
+            pc[u] = pn[u];
 #pragma unroll
             for (int v = 0; v < V; ++v) xv[u][v] = x2[u][v];
         }

@@ -222,3 +222,35 @@ def test_unit_layout_reads_back(name, coo, bs, f32):
     g = gen.uniform_x(coo.m, 4)
     gref, gab = cd.oracle_spmm_ld(coo, g[None, :], transpose=True)
     assert np.all(np.abs(ld.decode_spmv(p, g, transpose=True) - gref[0]) <= tol * gab[0] + 1e-300)
+
+
+@pytest.mark.parametrize("name,coo", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("tile_entries", [0, 64, 100])
+def test_coo_sections_in_lane_slices(name, coo, tile_entries):
+    """Each tile's COO section is stored in 32 lane slices: read back as
+    slice 0, 1, ... 31 (slice l = positions 32 j + l < E, in j order) the
+    entries are in strictly increasing (row, column) order, slice lengths
+    differ by at most one (longer slices first), and the positions fill
+    [0, E) exactly."""
+    import cbspmv
+    p = cbspmv.Plan(coo, tile_entries=tile_entries)
+    fn = cbspmv.lib().cbspmv_export
+
+    def raw(nm, dt):
+        cnt = fn(p._h, nm.encode(), None)
+        a = np.zeros(cnt, dt)
+        if cnt:
+            fn(p._h, nm.encode(), a.ctypes.data_as(cbspmv.ctypes.c_void_p))
+        return a
+
+    tiles = raw("dev_tiles", np.uint32).reshape(-1, 8)
+    pay = raw("dev_payload", np.uint8)
+    for t in tiles:
+        E = int(t[4])
+        if E == 0:
+            continue
+        idx = pay[int(t[3]) * 16:int(t[3]) * 16 + 4 * E].view(np.uint32).astype(np.int64)
+        lens = [len(range(l, E, 32)) for l in range(32)]
+        assert max(lens) - min(lens) <= 1 and lens == sorted(lens, reverse=True)
+        order = np.concatenate([idx[l:E:32] for l in range(32)])
+        assert order.size == E and np.all(np.diff(order) > 0)
