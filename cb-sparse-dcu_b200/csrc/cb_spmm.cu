@@ -210,7 +210,9 @@ __device__ __forceinline__ void ms_add(const MatView &M, const uint4 ta, const u
 #pragma unroll
         for (int u = 0; u < KC; ++u) {
             r[u] = w[u] >> 27;
-            const bool same = u > 0 && r[u] == r[u > 0 ? u - 1 : 0];
+            // slots with no entry can sit between two slices of a lane group:
+            // a run only goes on from a slot that holds an entry
+            const bool same = u > 0 && pc[u > 0 ? u - 1 : 0] < E && r[u] == r[u > 0 ? u - 1 : 0];
 #pragma unroll
             for (int v = 0; v < V; ++v)
                 s[u][v] = fma(a[u], xv[u][v], same ? s[u > 0 ? u - 1 : 0][v] : T(0));
