@@ -204,24 +204,28 @@ __device__ __forceinline__ void ms_add(const MatView &M, const uint4 ta, const u
         int pn[KC];
         positions(c0 + KC, pn);
         load(pn, w2, a2, x2);  // slots past the last load nothing
+        // A slot with no entry (between two slices of the group, or past
+        // the last) takes the row of the slot before it and adds 0, so equal
+        // rows stay one run per chunk -- every run flushed below is a
+        // distinct row, which lets all accumulator loads go ahead of the
+        // stores.  A run is flushed only if it holds an entry.
         uint32_t r[KC];
         T s[KC][V];
-        bool f[KC];
+        bool f[KC], has[KC];
 #pragma unroll
         for (int u = 0; u < KC; ++u) {
-            r[u] = w[u] >> 27;
-            // slots with no entry can sit between two slices of a lane group:
-            // a run only goes on from a slot that holds an entry
-            const bool same = u > 0 && pc[u > 0 ? u - 1 : 0] < E && r[u] == r[u > 0 ? u - 1 : 0];
+            const bool valid = pc[u] < E;
+            r[u] = valid || u == 0 ? w[u] >> 27 : r[u > 0 ? u - 1 : 0];
+            const bool same = u > 0 && r[u] == r[u > 0 ? u - 1 : 0];
+            has[u] = valid || (same && has[u > 0 ? u - 1 : 0]);
 #pragma unroll
             for (int v = 0; v < V; ++v)
                 s[u][v] = fma(a[u], xv[u][v], same ? s[u > 0 ? u - 1 : 0][v] : T(0));
         }
 #pragma unroll
         for (int u = 0; u < KC; ++u) {
-            const bool more = u + 1 < KC && pc[u + 1 < KC ? u + 1 : u] < E &&
-                              r[u + 1 < KC ? u + 1 : u] == r[u];
-            f[u] = pc[u] < E && !more;
+            const bool more = u + 1 < KC && r[u + 1 < KC ? u + 1 : u] == r[u];
+            f[u] = has[u] && !more;
         }
         T o[KC][V];
 #pragma unroll

@@ -135,15 +135,20 @@ def staged_walk_spmv(plan, x: np.ndarray, RL: int, KC: int) -> np.ndarray:
                     j += 1
                     if j == Kt:
                         j, tt = 0, tt + 1
-                r = [int(idx[e]) >> 27 if e < E else 0 for e in pc]
-                s = []
+                r, s, has = [], [], []
                 for u, e in enumerate(pc):
+                    r.append(int(idx[e]) >> 27 if e < E else (r[u - 1] if u else 0))
                     p = (np.longdouble(val[e]) * x[int(idx[e]) & ((1 << 27) - 1)]
                          if e < E else np.longdouble(0))
-                    same = u > 0 and pc[u - 1] < E and r[u] == r[u - 1]
+                    same = u > 0 and r[u] == r[u - 1]
                     s.append(p + (s[u - 1] if same else 0))
-                for u, e in enumerate(pc):
-                    more = u + 1 < KC and pc[u + 1] < E and r[u + 1] == r[u]
-                    if e < E and not more:
-                        y[int(t[1]) * plan.bs + r[u]] += s[u]
+                    has.append(e < E or (same and has[u - 1]))
+                # every flushed run loads its accumulator before any store, as
+                # the kernel does: two runs of one row in a chunk would lose one
+                flush = [u for u in range(KC)
+                         if has[u] and not (u + 1 < KC and r[u + 1] == r[u])]
+                rows = [r[u] for u in flush]
+                assert len(set(rows)) == len(rows), "two runs of one row in a chunk"
+                for u in flush:
+                    y[int(t[1]) * plan.bs + r[u]] += s[u]
     return y.astype(np.float64)
