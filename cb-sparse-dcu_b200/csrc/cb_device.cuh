@@ -63,8 +63,9 @@ __device__ __forceinline__ void add_entries(T *myacc, const uint32_t *w, const T
 // lanes never write the same accumulator and the order of the sums is fixed
 // by the layout (bitwise reproducible results).  Ends with a __syncwarp.
 template <typename T, int BS, int K>
-__device__ __forceinline__ void slice_sums(T *acc, const uint32_t (&w)[K], const T (&xv)[K],
-                                           const T *sval, int unit, int E, int lane) {
+__device__ __forceinline__ void slice_sums(T *__restrict__ acc, const uint32_t (&w)[K],
+                                           const T (&xv)[K], const T *__restrict__ sval,
+                                           int unit, int E, int lane) {
     constexpr uint32_t kNone = 63;  // row of an empty lane (after every real row)
     const bool have = lane < E;
     const uint32_t rh = have ? (w[0] >> 27) : kNone;  // head row

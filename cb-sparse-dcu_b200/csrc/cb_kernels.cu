@@ -645,7 +645,7 @@ cudaError_t launch_chunk(const DevLayout &d, const void *x, void *y, int nrhs,
     if (e != cudaSuccess) return e;
     if (nrhs != 1 || !d.dunit) return cudaErrorInvalidValue;
     int64_t grid = (d.ndunits + kWarps - 1) / kWarps;
-    grid = std::min<int64_t>(grid, (int64_t)dev_sms() * dev_resident(fn, kWarps * 32, smem));
+    grid = std::min<int64_t>(grid, (int64_t)dev_sms() * dev_resident_l1(fn, kWarps * 32, smem));
     if (grid == 0) return cudaSuccess;
     cb_spmv_tile_kernel<T, BS, CH><<<(unsigned)grid, kWarps * 32, smem, stream>>>(
         static_cast<const uint4 *>(d.tiles), static_cast<const uint4 *>(d.blocks), d.payload,
@@ -684,7 +684,7 @@ cudaError_t stream_config(const DevLayout &d, StreamConfig<T, BS> &c) {
     const void *fn = reinterpret_cast<const void *>(cb_spmv_stream_kernel<T, BS>);
     cudaError_t e = dev_enable_smem(fn, c.smem);
     if (e != cudaSuccess) return e;
-    const int resident = dev_resident(fn, kStreamWarps * 32, c.smem);
+    const int resident = dev_resident_l1(fn, kStreamWarps * 32, c.smem);
     const int64_t need = (d.ntiles + kStreamWarps - 1) / kStreamWarps * kStreamWarps;
     c.warps = std::max<int64_t>(
         kStreamWarps, std::min<int64_t>((int64_t)dev_sms() * resident * kStreamWarps, need));
@@ -756,6 +756,7 @@ std::mutex g_facts_mu;
 std::map<int, int> g_sms;                                    // device -> SMs
 std::map<std::pair<int, const void *>, size_t> g_smem;       // (device, kernel) -> enabled
 std::map<std::tuple<int, const void *, int, size_t>, int> g_resident;
+std::map<std::pair<int, const void *>, int> g_carve;        // carveout set + 1
 std::atomic<uint32_t> g_wait_polls{0};                       // 0: kWaitLimit
 
 int current_device() {
@@ -798,6 +799,27 @@ int dev_resident(const void *fn, int threads, size_t smem) {
         r = 1;
     }
     return g_resident[key] = std::max(1, r);
+}
+
+int dev_resident_l1(const void *fn, int threads, size_t smem) {
+    int r = dev_resident(fn, threads, smem);
+    const int d = current_device();
+    int maxs = 0, reserved = 0;
+    cudaDeviceGetAttribute(&maxs, cudaDevAttrMaxSharedMemoryPerMultiprocessor, d);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, d);
+    if (maxs <= (int)kL1Keep) return r;
+    const size_t per = smem + (size_t)reserved;
+    const size_t cap = (size_t)maxs - kL1Keep;
+    r = std::max(1, std::min<int>(r, (int)(cap / std::max<size_t>(per, 1))));
+    const int pct = (int)std::min<size_t>(100, (r * per * 100 + maxs - 1) / (size_t)maxs);
+    std::lock_guard<std::mutex> lock(g_facts_mu);
+    int &have = g_carve[{d, fn}];
+    if (have != pct + 1 &&
+        cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct) ==
+            cudaSuccess)
+        have = pct + 1;
+    cudaGetLastError();
+    return r;
 }
 
 uint32_t wait_polls() {

@@ -143,6 +143,14 @@ void note_launch();
 int dev_sms();
 cudaError_t dev_enable_smem(const void *fn, size_t smem);
 int dev_resident(const void *fn, int threads, size_t smem);
+// Resident blocks per SM for the gather-heavy SpMV kernels: at most as many
+// as fit in kL1Keep bytes less than the largest shared-memory carveout, with
+// the kernel's carveout set to what they use, so that the SM's unified
+// L1/shared memory keeps at least that much more for the L1 (the x gathers'
+// misses in flight are held there: with the largest carveout the power-law
+// SpMV ran 1.4x slower).
+constexpr size_t kL1Keep = size_t(32) << 10;
+int dev_resident_l1(const void *fn, int threads, size_t smem);
 
 // Polls a bounded device wait makes before giving up (the kernels' `limit`
 // argument): dev::kWaitLimit unless set_wait_polls(p >= 0) set p for tests of
