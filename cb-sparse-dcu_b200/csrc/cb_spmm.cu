@@ -671,7 +671,7 @@ template <typename T, int BS, int RL, int V>
 int64_t ms_warps_t(uint32_t cap) {
     size_t smem = 0;
     if (ms_configure<T, BS, RL, V>(cap, &smem) != cudaSuccess) return 0;
-    const int resident = dev_resident_l1(
+    const int resident = dev_resident(
         reinterpret_cast<const void *>(cb_mstream_kernel<T, BS, RL, V>), kMsWarps * 32, smem);
     return (int64_t)resident * dev_sms() * kMsWarps;
 }
