@@ -73,22 +73,21 @@ __device__ __forceinline__ void slice_sums(T *__restrict__ acc, const uint32_t (
     T run = have ? (unit ? T(1) : sval[lane]) * xv[0] : T(0);
     T head = T(0);
     bool split = false;  // the slice holds more than one row
+    // branch-free: every step selects; only a row complete inside the slice
+    // (a change of row after the first) updates acc, under a predicate
 #pragma unroll
     for (int j = 1; j < K; ++j) {
+        if (32 * j >= E) break;  // warp-uniform
         const int pos = 32 * j + lane;
-        if (32 * j < E && pos < E) {
-            const uint32_t r = w[j] >> 27;
-            const T p = (unit ? T(1) : sval[pos]) * xv[j];
-            if (r == rc) {
-                run += p;
-            } else {
-                if (split) acc[rc] += run;  // a row complete inside this slice
-                else head = run;
-                split = true;
-                rc = r;
-                run = p;
-            }
-        }
+        const bool valid = pos < E;
+        const uint32_t r = valid ? (w[j] >> 27) : rc;
+        const T p = valid ? (unit ? T(1) : sval[pos]) * xv[j] : T(0);
+        const bool chg = r != rc;
+        if (chg && split) acc[rc] += run;
+        head = (chg && !split) ? run : head;
+        split = split || chg;
+        run = chg ? p : run + p;
+        rc = r;
     }
     // rows across lanes: the running sum `run` of the tail row rc
     const uint32_t rt_prev = __shfl_up_sync(kFull, rc, 1);
