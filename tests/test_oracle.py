@@ -1,6 +1,7 @@
 """The oracle, pinned: against the committed golden fixtures (made by the
 reference's own host code, tests/golden/make_golden.py) always, and against
 the reference compiled here (oracle/_ref) when it is present."""
+import os
 import pathlib
 
 import numpy as np
@@ -90,7 +91,7 @@ def test_reference_checker_accepts_oracle_y():
     assert not cd.ref_check(coo, x, y)
 
 
-REF_DATA = pathlib.Path("/root/reference/cb-spmv-dcu/data")
+REF_DATA = pathlib.Path(os.environ.get("CB_REFERENCE", "/root/reference")) / "cb-spmv-dcu" / "data"
 
 
 @pytest.mark.skipif(not (cd.have_ref() and REF_DATA.is_dir()),
