@@ -123,6 +123,7 @@ def _load():
         "cbspmv_batch_run_each": (ctypes.c_int, [_P, _P]),
         "cbspmv_batch_graph_launch": (ctypes.c_int, [_P, ctypes.c_int, _P]),
         "cbspmv_batch_destroy": (ctypes.c_int, [_P]),
+        "cbspmv_batch_check": (ctypes.c_int, [_P, _P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -476,6 +477,11 @@ class Batch:
 
     def graph_launch(self, per_matrix: bool = False, stream=None):
         _check(_lib.cbspmv_batch_graph_launch(self._h, int(per_matrix), _stream(stream)))
+
+    def check(self, stream=None) -> None:
+        """Synchronizes and raises CBSpMVError (status DEVICE) if a batch
+        launch gave up a bounded device wait since the last report."""
+        _check(_lib.cbspmv_batch_check(self._h, _stream(stream)))
 
     def close(self):
         if getattr(self, "_h", None):

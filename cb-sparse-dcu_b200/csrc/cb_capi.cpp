@@ -1031,64 +1031,62 @@ int64_t cbspmv_launch_count(void) { return cb::kernel_launches(); }
 
 // ---- batches ---------------------------------------------------------------
 
-// Matrices of one launch class share a launch: their views are contiguous in
-// the device table from `first`, their tiles concatenated (toff) and split
-// over the launch's warps (wpart).
-struct BatchGroup {
-    cb::MsClass c;
-    int first = 0, count = 0;
-    int64_t *d_toff = nullptr, *d_ustart = nullptr;
-    int64_t ntot = 0, nunits = 0;  // tiles and scheduling units of the group
-    uint32_t *d_sched = nullptr;  // 4 scheduler words (unit counter, warps out, error)
-};
-
+// All matrices of a batch run in one launch: their views are a device table,
+// their tiles concatenated (toff) and cut into scheduling units (ustart) the
+// launch's warps take from a counter.
 struct cbspmv_batch {
-    std::vector<cbspmv_plan *> plans;  // in group order
-    std::vector<int> slot;             // caller's index k -> position in plans
+    std::vector<cbspmv_plan *> plans;  // in the caller's order
     std::vector<cb::MatView> views;    // host copy of the device table
-    std::vector<BatchGroup> groups;
     int bs = 16, f32 = 0, device = -1;
     bool bound = false;
     cb::MatView *d_views = nullptr;
-    uint32_t tile_cap = 16;     // shared buffer bytes: every plan's largest tile
+    int64_t *d_toff = nullptr, *d_ustart = nullptr;
+    int64_t ntot = 0, nunits = 0;   // tiles and scheduling units
+    uint32_t *d_sched = nullptr;    // 2 scheduler words (unit counter, warps out)
+    uint32_t *herr = nullptr, *derr = nullptr;  // error word (host-mapped)
+    uint32_t tile_cap = 16;         // shared buffer bytes: every plan's largest tile
     cudaStream_t cap[8] = {};
     cudaEvent_t ev[9] = {};
     cudaGraphExec_t exec[2] = {};
-    // cbspmv_batch_run: groups after the first run on streams of their own,
-    // forked from and joined back to the caller's stream
-    std::vector<cudaStream_t> side;
-    std::vector<cudaEvent_t> side_done;
-    cudaEvent_t fork = nullptr;
     ~cbspmv_batch() {
-        for (cudaStream_t s : side)
-            if (s) cudaStreamSynchronize(s), cudaStreamDestroy(s);
-        for (cudaEvent_t e : side_done)
-            if (e) cudaEventDestroy(e);
-        if (fork) cudaEventDestroy(fork);
         for (cudaGraphExec_t &g : exec)
             if (g) cudaGraphExecDestroy(g);
         for (cudaEvent_t &e : ev)
             if (e) cudaEventDestroy(e);
         for (cudaStream_t &c : cap)
             if (c) cudaStreamDestroy(c);
-        for (BatchGroup &g : groups) {
-            if (g.d_toff) cudaFree(g.d_toff);
-            if (g.d_sched) cudaFree(g.d_sched);
-            if (g.d_ustart) cudaFree(g.d_ustart);
-        }
-        if (d_views) cudaFree(d_views);
+        for (void *p : {(void *)d_toff, (void *)d_ustart, (void *)d_sched, (void *)d_views})
+            if (p) cudaFree(p);
+        if (herr) cudaFreeHost(herr);
     }
 };
 
 namespace {
 
-cbspmv_status batch_check(cbspmv_batch *b, bool need_bound) {
+// Reports (once) that a batch launch gave up a bounded device wait, and
+// resets the plans' arrival counters and the batch's scheduler words.
+cbspmv_status batch_device_error(cbspmv_batch *b, cudaStream_t st) {
+    if (!b->herr) return CBSPMV_OK;
+    volatile uint32_t *w = b->herr;
+    if (*w == 0) return CBSPMV_OK;
+    *w = 0;
+    for (cbspmv_plan *p : b->plans)
+        if (p->A.counters)
+            CB_CUDA(cudaMemsetAsync(p->A.counters, 0, (p->A.lay.gb_m + 4) * sizeof(int32_t), st),
+                    "reset scratch after a device error");
+    CB_CUDA(cudaMemsetAsync(b->d_sched, 0, 16, st), "reset scratch after a device error");
+    return fail(CBSPMV_ERR_DEVICE,
+                "a bounded device wait gave up in an earlier batch launch: its outputs are "
+                "incomplete; the batch's scratch was reset");
+}
+
+cbspmv_status batch_check(cbspmv_batch *b, bool need_bound, cudaStream_t st) {
     if (!b) return fail(CBSPMV_ERR_INVALID, "null batch");
     if (need_bound && !b->bound) return fail(CBSPMV_ERR_STATE, "batch has no bound x/y arrays");
     int dev = -1;
     cudaGetDevice(&dev);
     if (dev != b->device) return fail(CBSPMV_ERR_STATE, "batch was created on another device");
-    return CBSPMV_OK;
+    return batch_device_error(b, st);
 }
 
 cbspmv_status batch_each(cbspmv_batch *b, cudaStream_t st) {
@@ -1101,32 +1099,12 @@ cbspmv_status batch_each(cbspmv_batch *b, cudaStream_t st) {
     return CBSPMV_OK;
 }
 
-// One persistent launch per lane class.  The classes' launches are
-// independent (own tiles, units and counters), so all but the first run on
-// side streams forked from `st` and joined back to it: one class's tail
-// overlaps the next class's start.
+// One persistent launch over every matrix of the batch.
 cbspmv_status batch_one(cbspmv_batch *b, cudaStream_t st) {
-    const size_t ng = b->groups.size();
-    if (ng > 1) {
-        CB_CUDA(cudaEventRecord(b->fork, st), "batch fork");
-        for (size_t q = 1; q < ng; ++q)
-            CB_CUDA(cudaStreamWaitEvent(b->side[q - 1], b->fork, 0), "batch fork");
-    }
-    cbspmv_status rc = CBSPMV_OK;
-    for (size_t q = 0; q < ng && !rc; ++q) {
-        const BatchGroup &g = b->groups[q];
-        const cudaError_t e =
-            cb::launch_batch(b->bs, b->f32, g.c, b->d_views + g.first, g.count, g.d_toff,
-                             g.d_ustart, g.nunits, b->tile_cap, g.d_sched,
-                             q ? b->side[q - 1] : st);
-        if (e != cudaSuccess) rc = cuda_fail(e, "batch launch");
-    }
-    // join every side stream, also after a failed launch
-    for (size_t q = 1; q < ng; ++q) {
-        CB_CUDA(cudaEventRecord(b->side_done[q - 1], b->side[q - 1]), "batch join");
-        CB_CUDA(cudaStreamWaitEvent(st, b->side_done[q - 1], 0), "batch join");
-    }
-    return rc;
+    const cudaError_t e = cb::launch_batch(b->bs, b->f32, b->d_views, (int)b->plans.size(),
+                                           b->d_toff, b->d_ustart, b->nunits, b->tile_cap,
+                                           b->d_sched, b->derr, st);
+    return e == cudaSuccess ? CBSPMV_OK : cuda_fail(e, "batch launch");
 }
 
 }  // namespace
@@ -1164,65 +1142,42 @@ cbspmv_status cbspmv_batch_create(cbspmv_plan *const *plans, int count, const in
         }
         b->tile_cap = std::max(b->tile_cap, plans[k]->A.d.mcap);
     }
-    // group by launch class, keeping the caller's order inside a group
-    std::vector<int> order(count);
-    std::iota(order.begin(), order.end(), 0);
-    auto key = [&](int k) {
-        const cb::MsClass c = cb::ms_class(nrhs[k], b->f32);
-        return c.V * 64 + c.RL;
-    };
-    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return key(a) < key(c); });
-    b->slot.assign(count, 0);
-    cudaError_t e = cudaSuccess;
-    for (int i = 0; i < count;) {
-        BatchGroup g;
-        g.c = cb::ms_class(nrhs[order[i]], b->f32);
-        g.first = i;
-        std::vector<int64_t> toff(1, 0);
-        for (; i < count && key(order[i]) == key(order[g.first]); ++i) {
-            const int k = order[i];
-            b->slot[k] = i;
-            DevSide &s = plans[k]->A;
-            b->plans.push_back(plans[k]);
-            b->views.push_back(cb::mat_view(s.d, nullptr, nullptr, nrhs[k], nrhs[k], nrhs[k]));
-            toff.push_back(toff.back() + (int64_t)s.lay.tiles.size());
-        }
-        g.count = i - g.first;
-        g.ntot = toff.back();
-        std::vector<int64_t> us;
-        // about four units per resident warp, at least two tiles each
-        const int64_t target = std::max<int64_t>(
-            2, g.ntot / (std::max<int64_t>(1, cb::ms_warps(b->bs, b->f32, b->tile_cap)) * 4));
-        for (int q = g.first; q < i; ++q) {
-            const DevSide &s = b->plans[q]->A;
-            cb::ms_unit_starts(reinterpret_cast<const uint32_t *>(s.lay.tiles.data()),
-                               (int64_t)s.lay.tiles.size(), target, toff[q - g.first], us);
-        }
-        g.nunits = (int64_t)us.size();
-        us.push_back(g.ntot);
-        if (e == cudaSuccess) e = cudaMalloc((void **)&g.d_ustart, us.size() * sizeof(int64_t));
-        if (e == cudaSuccess)
-            e = cudaMemcpy(g.d_ustart, us.data(), us.size() * sizeof(int64_t),
-                           cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMalloc((void **)&g.d_toff, toff.size() * sizeof(int64_t));
-        if (e == cudaSuccess) e = cudaMalloc((void **)&g.d_sched, 16);
-        if (e == cudaSuccess) e = cudaMemset(g.d_sched, 0, 16);
-        if (e == cudaSuccess)
-            e = cudaMemcpy(g.d_toff, toff.data(), toff.size() * sizeof(int64_t),
-                           cudaMemcpyHostToDevice);
-        b->groups.push_back(g);
+    std::vector<int64_t> toff(1, 0);
+    for (int k = 0; k < count; ++k) {
+        DevSide &s = plans[k]->A;
+        b->plans.push_back(plans[k]);
+        b->views.push_back(cb::mat_view(s.d, nullptr, nullptr, nrhs[k], nrhs[k], nrhs[k]));
+        toff.push_back(toff.back() + (int64_t)s.lay.tiles.size());
     }
+    b->ntot = toff.back();
+    // about four units per resident warp, at least two tiles each
+    std::vector<int64_t> us;
+    const int64_t target = std::max<int64_t>(
+        2, b->ntot / (std::max<int64_t>(1, cb::ms_warps(b->bs, b->f32, b->tile_cap)) * 4));
+    for (int k = 0; k < count; ++k) {
+        const DevSide &s = plans[k]->A;
+        cb::ms_unit_starts(reinterpret_cast<const uint32_t *>(s.lay.tiles.data()),
+                           (int64_t)s.lay.tiles.size(), target, toff[k], us);
+    }
+    b->nunits = (int64_t)us.size();
+    us.push_back(b->ntot);
+    std::vector<int64_t> &all = us;
+    cudaError_t e = cudaMalloc((void **)&b->d_ustart, all.size() * sizeof(int64_t));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_ustart, all.data(), all.size() * sizeof(int64_t),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_toff, toff.size() * sizeof(int64_t));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_toff, toff.data(), toff.size() * sizeof(int64_t),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_sched, 16);
+    if (e == cudaSuccess) e = cudaMemset(b->d_sched, 0, 16);
     if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_views, count * sizeof(cb::MatView));
-    for (size_t q = 1; q < b->groups.size() && e == cudaSuccess; ++q) {
-        cudaStream_t s = nullptr;
-        cudaEvent_t d = nullptr;
-        e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
-        if (e == cudaSuccess) b->side.push_back(s);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&d, cudaEventDisableTiming);
-        if (e == cudaSuccess) b->side_done.push_back(d);
+    if (e == cudaSuccess) e = cudaHostAlloc((void **)&b->herr, 16, cudaHostAllocMapped);
+    if (e == cudaSuccess) {
+        std::memset(b->herr, 0, 16);
+        e = cudaHostGetDevicePointer((void **)&b->derr, b->herr, 0);
     }
-    if (e == cudaSuccess && b->groups.size() > 1)
-        e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         delete b;
         return cuda_fail(e, "allocate batch tables");
@@ -1233,15 +1188,14 @@ cbspmv_status cbspmv_batch_create(cbspmv_plan *const *plans, int count, const in
 
 cbspmv_status cbspmv_batch_bind(cbspmv_batch *b, const void *const *x, void *const *y,
                                 void *stream) {
-    cbspmv_status rc = batch_check(b, false);
+    cbspmv_status rc = batch_check(b, false, static_cast<cudaStream_t>(stream));
     if (rc) return rc;
     if (!x || !y) return fail(CBSPMV_ERR_INVALID, "null x or y array");
-    for (size_t k = 0; k < b->slot.size(); ++k) {
-        const int i = b->slot[k];
-        const DevSide &s = b->plans[i]->A;
+    for (size_t k = 0; k < b->plans.size(); ++k) {
+        const DevSide &s = b->plans[k]->A;
         if ((s.lay.m > 0 && !y[k]) || (s.lay.n > 0 && !x[k]))
             return fail(CBSPMV_ERR_INVALID, "null x or y in batch");
-        cb::MatView &v = b->views[i];
+        cb::MatView &v = b->views[k];
         v = cb::mat_view(s.d, x[k], y[k], v.nrhs, v.nrhs, v.nrhs);
     }
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -1258,19 +1212,19 @@ cbspmv_status cbspmv_batch_bind(cbspmv_batch *b, const void *const *x, void *con
 }
 
 cbspmv_status cbspmv_batch_run(cbspmv_batch *b, void *stream) {
-    cbspmv_status rc = batch_check(b, true);
+    cbspmv_status rc = batch_check(b, true, static_cast<cudaStream_t>(stream));
     if (rc) return rc;
     return batch_one(b, static_cast<cudaStream_t>(stream));
 }
 
 cbspmv_status cbspmv_batch_run_each(cbspmv_batch *b, void *stream) {
-    cbspmv_status rc = batch_check(b, true);
+    cbspmv_status rc = batch_check(b, true, static_cast<cudaStream_t>(stream));
     if (rc) return rc;
     return batch_each(b, static_cast<cudaStream_t>(stream));
 }
 
 cbspmv_status cbspmv_batch_graph_launch(cbspmv_batch *b, int per_matrix, void *stream) {
-    cbspmv_status rc = batch_check(b, true);
+    cbspmv_status rc = batch_check(b, true, static_cast<cudaStream_t>(stream));
     if (rc) return rc;
     const int mode = per_matrix ? 1 : 0;
     if (!b->exec[mode]) {
@@ -1317,6 +1271,13 @@ cbspmv_status cbspmv_batch_graph_launch(cbspmv_batch *b, int per_matrix, void *s
     }
     CB_CUDA(cudaGraphLaunch(b->exec[mode], static_cast<cudaStream_t>(stream)), "graph launch");
     return CBSPMV_OK;
+}
+
+cbspmv_status cbspmv_batch_check(cbspmv_batch *b, void *stream) {
+    if (!b) return fail(CBSPMV_ERR_INVALID, "null batch");
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    CB_CUDA(cudaStreamSynchronize(st), "batch check: synchronize");
+    return batch_check(b, false, st);
 }
 
 cbspmv_status cbspmv_batch_destroy(cbspmv_batch *b) {

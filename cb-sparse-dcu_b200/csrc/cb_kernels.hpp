@@ -56,14 +56,6 @@ struct MatView {
     uint32_t pay16_end = 0;     // payload size in 16-byte units
 };
 
-// Launch class of the multi-right-hand-side kernel: RL lanes per stored
-// entry, V right-hand sides per lane (RL * V per pass).
-struct MsClass {
-    int RL = 1, V = 1;
-};
-
-// The class used for nrhs right-hand sides of the given value type.
-MsClass ms_class(int nrhs, int f32);
 // Shared-memory buffer bytes for tiles of at most max_tile_bytes.
 uint32_t ms_cap(int64_t max_tile_bytes);
 MatView mat_view(const DevLayout &d, const void *x, void *y, int nrhs, int64_t ldx,
@@ -84,13 +76,14 @@ void ms_unit_starts(const uint32_t *tile8, int64_t ntiles, int64_t target, int64
 // d.nunits set; scheduler words d.sched[0..1], error word d.err).
 cudaError_t launch_spmm(const DevLayout &d, const void *x, void *y, int nrhs, int64_t ldx,
                         int64_t ldy, cudaStream_t stream);
-// The same kernel over a device table of nmats matrices of one class: tile
-// offsets toff[nmats + 1], units ustart[nunits + 1] over the concatenated
-// tiles, shared buffers of cap bytes (>= every matrix's largest tile), four
-// scheduler words (zero before the first launch; the kernel leaves them zero).
-cudaError_t launch_batch(int bs, int f32, MsClass c, const MatView *mats, int nmats,
-                         const int64_t *toff, const int64_t *ustart, int64_t nunits,
-                         uint32_t cap, uint32_t *sched, cudaStream_t stream);
+// The same kernel over a device table of nmats matrices (each with its own
+// right-hand-side count) in ONE launch: tile offsets toff[nmats + 1], units
+// ustart[nunits + 1] over the concatenated tiles, shared buffers of cap bytes
+// (>= every matrix's largest tile), two scheduler words (zero before the
+// first launch; the kernel leaves them zero) and an error word.
+cudaError_t launch_batch(int bs, int f32, const MatView *mats, int nmats, const int64_t *toff,
+                         const int64_t *ustart, int64_t nunits, uint32_t cap, uint32_t *sched,
+                         uint32_t *err, cudaStream_t stream);
 
 // The direct kernel's scheduling units: each block row's tiles in pieces of
 // at most kDirectUnitTiles, starting at the row's first tile; direct_units

@@ -301,10 +301,11 @@ cbspmv_status cbspmv_autotune(cbspmv_plan *plan, int nrhs, void *stream, int *ke
 /* Many uploaded plans -- same block size and value type, same device -- run
  * together: Y_k = A_k X_k for k < count, X_k row-major n_k x nrhs[k] and Y_k
  * row-major m_k x nrhs[k] (contiguous rows), nrhs[k] >= 1 per matrix.  One
- * batch launch runs every matrix in ONE persistent kernel whose warps take
- * host-balanced ranges of all the matrices' tiles; the warp ranges are
- * computed here for the current device.  A plan may belong to several
- * batches but is run by one of them (or by itself) at a time. */
+ * batch launch runs every matrix, whatever its size and right-hand-side
+ * count, in ONE persistent kernel: its warps take scheduling units of the
+ * matrices' concatenated tiles from a device counter (the units are cut here
+ * for the current device).  A plan may belong to several batches but is run
+ * by one of them (or by itself) at a time. */
 typedef struct cbspmv_batch cbspmv_batch;
 
 cbspmv_status cbspmv_batch_create(cbspmv_plan *const *plans, int count,
@@ -330,6 +331,13 @@ cbspmv_status cbspmv_batch_run_each(cbspmv_batch *batch, void *stream);
  * then launched on `stream`. */
 cbspmv_status cbspmv_batch_graph_launch(cbspmv_batch *batch, int per_matrix,
                                         void *stream);
+
+/* cbspmv_check for a batch: synchronizes `stream` and returns
+ * CBSPMV_ERR_DEVICE if a batch launch gave up a bounded device wait since the
+ * last report (its outputs are then incomplete; the batch's scratch is
+ * reset).  cbspmv_batch_run and the graph launch report it too, without
+ * launching. */
+cbspmv_status cbspmv_batch_check(cbspmv_batch *batch, void *stream);
 
 cbspmv_status cbspmv_batch_destroy(cbspmv_batch *batch);
 

@@ -96,59 +96,3 @@ def decode_spmv(plan, x: np.ndarray, transpose: bool = False) -> np.ndarray:
     assert seen_rows.all(), "a row is not covered by any tile"
     return y.astype(np.float64)
 
-
-def staged_walk_spmv(plan, x: np.ndarray, RL: int, KC: int) -> np.ndarray:
-    """y = A x over the COO sections only (plans whose blocks are all COO),
-    reading each tile the way the several-right-hand-side kernel's lane
-    groups do (cb_spmm.cu, ms_add): group es of G = 32 / RL takes the lane
-    slices es, es + G, ... in turn, KC slots per chunk; equal-row runs of
-    slots that hold an entry are summed before one accumulator update."""
-    import cbspmv
-    fn = cbspmv.lib().cbspmv_export
-
-    def raw(name, dt):
-        cnt = fn(plan._h, name.encode(), None)
-        a = np.zeros(cnt, dt)
-        if cnt:
-            fn(plan._h, name.encode(), a.ctypes.data_as(cbspmv.ctypes.c_void_p))
-        return a
-
-    tiles = raw("dev_tiles", np.uint32).reshape(-1, 8)
-    pay = raw("dev_payload", np.uint8)
-    vt = np.float32 if plan.f32 else np.float64
-    vsz = 4 if plan.f32 else 8
-    G = 32 // RL
-    y = np.zeros(plan.m, np.longdouble)
-    for t in tiles:
-        E, base = int(t[4]), int(t[3]) * 16
-        assert (int(t[2]) >> 16) & 0xFF == 0, "COO-only plans"
-        idx = pay[base:base + 4 * E].view(np.uint32)
-        vo = base + _a16(4 * E)
-        val = pay[vo:vo + vsz * E].view(vt)
-        Kt = (E + 31) >> 5
-        for es in range(G):
-            for c0 in range(0, RL * Kt, KC):
-                tt, j = c0 // Kt, c0 % Kt
-                pc = []
-                for _ in range(KC):
-                    pc.append(32 * j + es + G * tt if tt < RL else E)
-                    j += 1
-                    if j == Kt:
-                        j, tt = 0, tt + 1
-                r, s, has = [], [], []
-                for u, e in enumerate(pc):
-                    r.append(int(idx[e]) >> 27 if e < E else (r[u - 1] if u else 0))
-                    p = (np.longdouble(val[e]) * x[int(idx[e]) & ((1 << 27) - 1)]
-                         if e < E else np.longdouble(0))
-                    same = u > 0 and r[u] == r[u - 1]
-                    s.append(p + (s[u - 1] if same else 0))
-                    has.append(e < E or (same and has[u - 1]))
-                # every flushed run loads its accumulator before any store, as
-                # the kernel does: two runs of one row in a chunk would lose one
-                flush = [u for u in range(KC)
-                         if has[u] and not (u + 1 < KC and r[u + 1] == r[u])]
-                rows = [r[u] for u in flush]
-                assert len(set(rows)) == len(rows), "two runs of one row in a chunk"
-                for u in flush:
-                    y[int(t[1]) * plan.bs + r[u]] += s[u]
-    return y.astype(np.float64)

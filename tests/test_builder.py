@@ -255,24 +255,3 @@ def test_coo_sections_in_lane_slices(name, coo, tile_entries):
         order = np.concatenate([idx[l:E:32] for l in range(32)])
         assert order.size == E and np.all(np.diff(order) > 0)
 
-
-@pytest.mark.parametrize("RL", [1, 2, 4, 8])
-@pytest.mark.parametrize("KC", [4, 6])
-@pytest.mark.parametrize("long_rows", [False, True])
-def test_staged_slot_walk(RL, KC, long_rows):
-    """The several-right-hand-side kernel's walk over lane slices (a group of
-    RL lanes per entry), emulated on CPU: every entry is added exactly once
-    (a slot with no entry between two slices carries the run on, so a chunk
-    never flushes two runs of one row)."""
-    import cbspmv
-    from cbspmv import gen
-    if long_rows:  # rows over many lane slices and tiles
-        coo = gen.power_law(8192, kmax=8192, band=512, seed=11)
-        p = cbspmv.Plan(coo, tile_entries=64)
-    else:
-        coo = gen.power_law(2048, kmax=2048, band=200, seed=3, mean=24)
-        p = cbspmv.Plan(coo, tile_entries=100)
-    x = gen.uniform_x(coo.n, 1)
-    yref, ab = cd.oracle_spmm_ld(coo, x[None, :])
-    y = ld.staged_walk_spmv(p, x, RL, KC)
-    assert np.all(np.abs(y - yref[0]) <= 1e-13 * ab[0] + 1e-300)

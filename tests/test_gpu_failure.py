@@ -95,3 +95,42 @@ def test_giveup_host_call_reports(cuda):
     assert ei.value.status == "DEVICE"
     y = plan.spmv_host(x)
     assert _err(y, coo, x) <= 1e-12
+
+
+def test_batch_giveup_is_reported_and_reset(cuda):
+    """The same for the one-launch batch: cbspmv_batch_check reports the
+    give-up, the batch's scratch is reset, and the next launches are exact."""
+    import torch
+    import cbspmv
+    import cbdump as cd
+    from cbspmv import gen
+    items = gen.batch_uneven(count=12, seed=6, nmin=500, nmax=20000)
+    plans = [cbspmv.Plan(it.coo, tile_entries=64) for it in items]
+    Xs = [np.ascontiguousarray(gen.uniform_x(it.coo.n, 50 + i, nrhs=max(it.nrhs, 2))[:it.nrhs].T)
+          for i, it in enumerate(items)]
+    xs = [torch.from_numpy(X).to(cuda) for X in Xs]
+    ys = [torch.empty(it.coo.m, it.nrhs, dtype=torch.float64, device=cuda) for it in items]
+    b = cbspmv.Batch(plans, [it.nrhs for it in items]).bind(xs, ys)
+
+    def exact():
+        for it, X, y in zip(items, Xs, ys):
+            yref, ab = cd.oracle_spmm_ld(it.coo, X.T)
+            assert np.all(np.abs(y.cpu().numpy().T - yref) <= 1e-12 * ab + 1e-300)
+
+    b.run()
+    b.check()
+    exact()
+    try:
+        cbspmv.debug_wait_polls(0)
+        b.run()
+    finally:
+        cbspmv.debug_wait_polls(-1)
+    with pytest.raises(cbspmv.CBSpMVError) as ei:
+        b.check()
+    assert ei.value.status == "DEVICE"
+    for _ in range(2):
+        for y in ys:
+            y.fill_(float("nan"))
+        b.run()
+        b.check()
+        exact()
