@@ -68,13 +68,13 @@ struct VecOf {
 
 // Per-warp shared memory: [acc | xt | mbar[2] | buf[2]].  acc: BS rows x kRA
 // right-hand sides (row r, column c at acc[r * kRA + c]); xt: the x rows of
-// two CSR/DENSE blocks, V values per column; buf: one tile payload (`cap`
-// bytes).
+// the CSR/DENSE blocks of one step (at most 32 x rows of V values for every
+// block column); buf: one tile payload (`cap` bytes).
 template <typename T, int BS>
 struct MsLayout {
     static constexpr int V = VecOf<T>::V;
     static constexpr uint32_t acc_bytes = BS * kRA * sizeof(T);
-    static constexpr uint32_t xt_bytes = 2 * BS * V * sizeof(T);
+    static constexpr uint32_t xt_bytes = BS * 8 * V * sizeof(T);
     static constexpr uint32_t head = a16(acc_bytes + xt_bytes + 16);
     __host__ __device__ static uint32_t bytes(uint32_t cap) { return head + 2 * cap; }
 };
@@ -100,41 +100,62 @@ __device__ __forceinline__ void ldg_row(const T *p, bool vec, int nv, T (&o)[NV]
     for (int v = 0; v < NV; ++v) o[v] = v < nv ? __ldg(p + v) : T(0);
 }
 
-// One pass of a tile's COO section over right-hand sides c0 + [0, NV) (nv of
-// them real; accumulator columns ca + [0, nv)).  Lane l walks its slice
-// (positions 32 j + l < E) kSub entries at a time, summing along its rows in
-// registers; a row that begins and ends inside the slice is added into acc
-// by the lane itself, and one segmented shuffle scan joins the rows that run
-// across lanes: the scheme of the single-vector streaming kernel
-// (slice_sums, cb_device.cuh), NV values wide.  Each row of the tile is added
-// by exactly one lane, so no two lanes write one accumulator.
-template <typename T, int BS, int NV>
+// The lanes of a warp form G = 32 / RL groups of RL lanes; a group works on
+// one entry (or one block row) at a time, its lanes on NV consecutive
+// right-hand sides each, so one x row is read by RL lanes side by side (RL
+// pieces of NV values).
+//
+// One pass of a tile's COO section over right-hand sides c0 + [0, RL * NV)
+// (accumulator columns ca + ...).  The section is stored in 32 lane slices
+// of consecutive entries (coo_slice_pos, cb_layout.hpp); group g takes the
+// RL slices g RL, ..., g RL + RL - 1 in turn -- slot q = t Kt + j is entry j
+// of slice g RL + t, at position 32 j + g RL + t (none when not below E) --
+// so its entries are one run of the sorted section.  Each lane sums along
+// the rows in registers, kSub slots at a time (a slot with no entry carries
+// the row on and adds 0); a row that begins and ends inside the group's
+// range is added into acc by the group itself, and one segmented shuffle
+// scan over the groups joins the rows that run across groups: the scheme of
+// the single-vector streaming kernel (slice_sums, cb_device.cuh).  Each row
+// of the tile is added by exactly one group, so no two lanes write one
+// accumulator.
+template <typename T, int BS, int RL, int NV>
 __device__ __forceinline__ void coo_pass(const MatView &M, const unsigned char *buf, int E,
                                          int c0, int ca, T *__restrict__ acc, int lane) {
-    constexpr uint32_t kNone = 63;  // row of a lane with no entry (after every real row)
+    constexpr uint32_t kNone = 63;  // row of a group with no entry (after every real row)
+    constexpr int G = 32 / RL;
+    const int g = lane / RL, sub = lane % RL;
     const uint32_t *sidx = reinterpret_cast<const uint32_t *>(buf);
     const T *sval = reinterpret_cast<const T *>(buf + a16(4u * E));
-    const int nv = min(NV, M.nrhs - c0);
-    const T *__restrict__ xr = static_cast<const T *>(M.x) + c0;
+    const int cl = c0 + sub * NV;                    // this lane's first right-hand side
+    const int nv = max(0, min(NV, M.nrhs - cl));     // of them real
+    const int cal = ca + sub * NV;                   // its first accumulator column
+    const T *__restrict__ xr = static_cast<const T *>(M.x) + cl;
     const bool vec = M.xvec != 0;
     const int Kt = (E + 31) >> 5;
+    const int nslots = RL * Kt;
     uint32_t rh = kNone, rc = kNone;  // head row, row of the running sum
-    bool split = false;               // the slice holds more than one row
+    bool split = false;               // the group's range holds more than one row
     T run[NV], head[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) run[v] = head[v] = T(0);
-    for (int j0 = 0; j0 < Kt; j0 += kSub) {
+    int t = 0, j = 0;  // slot being loaded: slice g RL + t, entry j
+    for (int q0 = 0; q0 < nslots; q0 += kSub) {
+        int pos[kSub];
         uint32_t w[kSub];
         T a[kSub], xv[kSub][NV];
 #pragma unroll
         for (int u = 0; u < kSub; ++u) {
-            const int pos = 32 * (j0 + u) + lane;
-            w[u] = pos < E ? sidx[pos] : 0u;
-            a[u] = pos < E ? (M.unit ? T(1) : sval[pos]) : T(0);
+            pos[u] = t < RL ? 32 * j + g * RL + t : E;
+            if (++j == Kt) {
+                j = 0;
+                ++t;
+            }
+            w[u] = pos[u] < E ? sidx[pos[u]] : 0u;
+            a[u] = pos[u] < E ? (M.unit ? T(1) : sval[pos[u]]) : T(0);
         }
 #pragma unroll
         for (int u = 0; u < kSub; ++u) {
-            if (32 * (j0 + u) + lane < E) {
+            if (pos[u] < E && nv > 0) {
                 ldg_row<T, NV>(xr + (size_t)(w[u] & kColMask) * (size_t)M.ldx, vec, nv, xv[u]);
             } else {
 #pragma unroll
@@ -143,20 +164,19 @@ __device__ __forceinline__ void coo_pass(const MatView &M, const unsigned char *
         }
 #pragma unroll
         for (int u = 0; u < kSub; ++u) {
-            if (32 * (j0 + u) >= E) break;  // warp-uniform
-            const bool valid = 32 * (j0 + u) + lane < E;
-            const uint32_t r = valid ? (w[u] >> 27) : rc;
-            if (j0 + u == 0) {  // the slice's first entry
+            if (q0 + u >= nslots) break;  // warp-uniform
+            const uint32_t r = pos[u] < E ? (w[u] >> 27) : rc;
+            if (q0 + u == 0) {  // the group's first slot
                 rh = rc = r;
 #pragma unroll
                 for (int v = 0; v < NV; ++v) run[v] = a[u] * xv[u][v];
                 continue;
             }
             const bool chg = r != rc;
-            if (chg && split) {  // a row complete inside this slice
+            if (chg && split) {  // a row complete inside the group's range
 #pragma unroll
                 for (int v = 0; v < NV; ++v)
-                    if (v < nv) acc[rc * kRA + ca + v] += run[v];
+                    if (v < nv) acc[rc * kRA + cal + v] += run[v];
             }
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
@@ -168,129 +188,170 @@ __device__ __forceinline__ void coo_pass(const MatView &M, const unsigned char *
             rc = r;
         }
     }
-    // rows across lanes: `run` holds the sum of the tail row rc
-    const uint32_t rt_prev = __shfl_up_sync(kFull, rc, 1);
-    const uint32_t rh_next = __shfl_down_sync(kFull, rh, 1);
-    const bool cont = lane > 0 && rh == rt_prev;  // my head goes on from the previous lane
+    // rows across groups: `run` holds the sum of the tail row rc
+    const uint32_t rt_prev = __shfl_up_sync(kFull, rc, RL);
+    const uint32_t rh_next = __shfl_down_sync(kFull, rh, RL);
+    const bool cont = g > 0 && rh == rt_prev;  // my head goes on from the previous group
     const uint32_t heads = __ballot_sync(kFull, !cont || split);
-    const int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
-    const uint32_t longest = __reduce_max_sync(kFull, (uint32_t)(lane - start + 1));
+    const int start = (31 - __clz(heads & (0xffffffffu >> (31 - lane)))) / RL;  // head group
+    const uint32_t longest = __reduce_max_sync(kFull, (uint32_t)(g - start + 1));
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
+    for (int d = 1; d < G; d <<= 1) {
         if ((uint32_t)d >= longest) break;
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-            const T t = __shfl_up_sync(kFull, run[v], d);
-            if (lane - d >= start) run[v] += t;
+            const T tt = __shfl_up_sync(kFull, run[v], d * RL);
+            if (g - d >= start) run[v] += tt;
         }
     }
     T prev[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) prev[v] = __shfl_up_sync(kFull, run[v], 1);
+    for (int v = 0; v < NV; ++v) prev[v] = __shfl_up_sync(kFull, run[v], RL);
     if (split) {
 #pragma unroll
         for (int v = 0; v < NV; ++v)
-            if (v < nv) acc[rh * kRA + ca + v] += cont ? head[v] + prev[v] : head[v];
+            if (v < nv) acc[rh * kRA + cal + v] += cont ? head[v] + prev[v] : head[v];
     }
-    if ((lane == 31 || rh_next != rc) && rc < (uint32_t)BS) {
+    if ((g == G - 1 || rh_next != rc) && rc < (uint32_t)BS) {
 #pragma unroll
         for (int v = 0; v < NV; ++v)
-            if (v < nv) acc[rc * kRA + ca + v] += run[v];
+            if (v < nv) acc[rc * kRA + cal + v] += run[v];
     }
     __syncwarp();
 }
 
 // One pass of a tile's CSR and DENSE blocks over right-hand sides c0 +
-// [0, NV): per step the x rows of BPS blocks are staged in xt (lane t: block
-// t / BS, column t % BS), then one lane per block row sums its row (DENSE
-// columns in a rotated order, so the lanes of a step read distinct banks);
-// for BS = 16 the second block's half-warp hands its sums to the first by a
-// shuffle, so each row is added by one lane.
-template <typename T, int BS, int NV>
+// [0, RL * NV): P = 32 / RL row slots; a step covers BPS = max(1, P / BS)
+// blocks (their x rows staged in xt, column c of block q at
+// xt[(q * BS + c) * RL * NV]), each row slot summing rows p, p + P, ... of
+// its block (DENSE columns in a rotated order, so the slots of a step read
+// distinct banks); with two blocks per step the second block's slots hand
+// their sums to the first by a shuffle, so each row is added by one group.
+template <typename T, int BS, int RL, int NV>
 __device__ __forceinline__ void blk_pass(const MatView &M, const uint4 ta,
                                          const unsigned char *buf, int c0, int ca,
                                          T *__restrict__ acc, T *__restrict__ xt, int lane) {
-    constexpr int BPS = BS == 16 ? 2 : 1;  // blocks per step
+    constexpr int P = 32 / RL;
+    constexpr int BPS = P >= BS ? P / BS : 1;  // blocks per step (1 or 2)
+    constexpr int RW = RL * NV;                // x values per column
     using IdxT = typename std::conditional<BS == 16, uint8_t, uint16_t>::type;
     const int ncoo = (ta.z >> 8) & 0xff, nxt = (ta.z >> 16) & 0xff;
-    const int nv = min(NV, M.nrhs - c0);
+    const int p = lane / RL, sub = lane % RL;
+    const int cl = c0 + sub * NV;
+    const int nv = max(0, min(NV, M.nrhs - cl));
+    const int cal = ca + sub * NV;
     const bool vec = M.xvec != 0;
     const uint4 bd =
         lane < nxt ? __ldg(&M.blocks[ta.x + ncoo + lane]) : make_uint4(0, 0, 0, 0);
-    const T *__restrict__ xb = static_cast<const T *>(M.x) + c0;
-    const int q = lane / BS, row = lane % BS;
+    const int q = BPS > 1 ? p / BS : 0;           // block of this slot in the step
+    const int prow = BPS > 1 ? p % BS : p;        // first row of this slot
     for (int jb = 0; jb < nxt; jb += BPS) {
-        const int j = jb + q;
-        const int jc = min(j, nxt - 1);
-        const uint32_t off = __shfl_sync(kFull, bd.x, jc);
-        const uint32_t mb = __shfl_sync(kFull, bd.y, jc);
-        const uint32_t xbase = __shfl_sync(kFull, bd.z, jc);
-        {
+        // stage the x rows: item i = (block qq, column c, piece s)
+        for (int i = lane; i < BPS * BS * RL; i += 32) {
+            const int s = i % RL, c = (i / RL) % BS, qq = i / (RL * BS);
+            const int jj = min(jb + qq, nxt - 1);
+            const uint32_t mb = __shfl_sync(kFull, bd.y, jj);
+            const uint32_t xbase = __shfl_sync(kFull, bd.z, jj);
+            const int cs = c0 + s * NV;
+            const int ns = max(0, min(NV, M.nrhs - cs));
             T xv[NV];
-            if (j < nxt && row < (int)((mb >> 14) & 63)) {
-                const int64_t col = M.gather ? (int64_t)__ldg(&M.block_cols[xbase + row])
-                                             : (int64_t)(xbase + row);
-                ldg_row<T, NV>(xb + (size_t)col * (size_t)M.ldx, vec, nv, xv);
+            if (jb + qq < nxt && c < (int)((mb >> 14) & 63) && ns > 0) {
+                const int64_t col = M.gather ? (int64_t)__ldg(&M.block_cols[xbase + c])
+                                             : (int64_t)(xbase + c);
+                ldg_row<T, NV>(static_cast<const T *>(M.x) + (size_t)col * (size_t)M.ldx + cs,
+                               vec, ns, xv);
             } else {
 #pragma unroll
                 for (int v = 0; v < NV; ++v) xv[v] = T(0);
             }
 #pragma unroll
-            for (int v = 0; v < NV; ++v) xt[(q * BS + row) * NV + v] = xv[v];
+            for (int v = 0; v < NV; ++v) xt[(qq * BS + c) * RW + s * NV + v] = xv[v];
         }
         __syncwarp();
-        T sum[NV];
+        const int j = jb + q;
+        const int jc = min(j, nxt - 1);
+        const uint32_t off = __shfl_sync(kFull, bd.x, jc);
+        const uint32_t mb = __shfl_sync(kFull, bd.y, jc);
+        const unsigned char *pb = buf + off;
+        const T *xq = xt + q * BS * RW + sub * NV;
+#pragma unroll 1
+        for (int row = prow; row < BS; row += (BPS > 1 ? BS : P)) {
+            T sum[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) sum[v] = T(0);
-        if (j < nxt) {
-            const unsigned char *pb = buf + off;
-            const T *xq = xt + q * BS * NV;
-            if ((mb & 3) == 1) {  // CSR
-                const int k = (mb >> 3) & 2047;
-                const IdxT *rp = reinterpret_cast<const IdxT *>(pb);
-                const IdxT *ci = rp + BS + 1;
-                const T *vv = reinterpret_cast<const T *>(
-                    pb + a16((uint32_t)((BS + 1 + k) * sizeof(IdxT))));
-                for (int t = rp[row]; t < (int)rp[row + 1]; ++t) {
-                    const T av = M.unit ? T(1) : vv[t];
-                    const int c = ci[t];
+            for (int v = 0; v < NV; ++v) sum[v] = T(0);
+            if (j < nxt) {
+                if ((mb & 3) == 1) {  // CSR
+                    const int k = (mb >> 3) & 2047;
+                    const IdxT *rp = reinterpret_cast<const IdxT *>(pb);
+                    const IdxT *ci = rp + BS + 1;
+                    const T *vv = reinterpret_cast<const T *>(
+                        pb + a16((uint32_t)((BS + 1 + k) * sizeof(IdxT))));
+                    for (int e = rp[row]; e < (int)rp[row + 1]; ++e) {
+                        const T av = M.unit ? T(1) : vv[e];
+                        const int c = ci[e];
 #pragma unroll
-                    for (int v = 0; v < NV; ++v) sum[v] = fma(av, xq[c * NV + v], sum[v]);
-                }
-            } else {  // DENSE, row-major BS x BS
+                        for (int v = 0; v < NV; ++v) sum[v] = fma(av, xq[c * RW + v], sum[v]);
+                    }
+                } else {  // DENSE, row-major BS x BS
 #pragma unroll 4
-                for (int c = 0; c < BS; ++c) {
-                    const int cc = (c + row) & (BS - 1);
-                    const T av = dense_at<T, BS>(pb, M.unit, row, cc);
+                    for (int c = 0; c < BS; ++c) {
+                        const int cc = (c + row) & (BS - 1);
+                        const T av = dense_at<T, BS>(pb, M.unit, row, cc);
 #pragma unroll
-                    for (int v = 0; v < NV; ++v) sum[v] = fma(av, xq[cc * NV + v], sum[v]);
+                        for (int v = 0; v < NV; ++v) sum[v] = fma(av, xq[cc * RW + v], sum[v]);
+                    }
                 }
             }
-        }
-        if (BS == 16) {
+            if (BPS > 1) {
 #pragma unroll
-            for (int v = 0; v < NV; ++v) sum[v] += __shfl_down_sync(kFull, sum[v], 16);
-        }
-        if (lane < BS) {
+                for (int v = 0; v < NV; ++v) sum[v] += __shfl_down_sync(kFull, sum[v], BS * RL);
+            }
+            if (q == 0) {
 #pragma unroll
-            for (int v = 0; v < NV; ++v)
-                if (v < nv) acc[row * kRA + ca + v] += sum[v];
+                for (int v = 0; v < NV; ++v)
+                    if (v < nv) acc[row * kRA + cal + v] += sum[v];
+            }
         }
         __syncwarp();
     }
 }
 
 // Adds a staged tile into the accumulators for right-hand sides [cg0, cg1)
-// (accumulator column c - cg0), NV at a time.
-template <typename T, int BS, int NV>
+// (accumulator column c - cg0), RL * NV at a time.
+template <typename T, int BS, int RL, int NV>
 __device__ __forceinline__ void tile_group(const MatView &M, const uint4 ta, const uint4 tb,
                                            const unsigned char *buf, int cg0, int cg1, T *acc,
                                            T *xt, int lane) {
     const int E = (int)tb.x;
     const int nxt = (ta.z >> 16) & 0xff;
-    for (int c0 = cg0; c0 < cg1; c0 += NV) {
-        if (E > 0) coo_pass<T, BS, NV>(M, buf, E, c0, c0 - cg0, acc, lane);
-        if (nxt) blk_pass<T, BS, NV>(M, ta, buf, c0, c0 - cg0, acc, xt, lane);
+    for (int c0 = cg0; c0 < cg1; c0 += RL * NV) {
+        if (E > 0) coo_pass<T, BS, RL, NV>(M, buf, E, c0, c0 - cg0, acc, lane);
+        if (nxt) blk_pass<T, BS, RL, NV>(M, ta, buf, c0, c0 - cg0, acc, xt, lane);
+    }
+}
+
+// Lanes per entry for R right-hand sides: the fewest (a power of two, at
+// most 8) whose RL * V values cover min(R, kRA).
+template <typename T>
+__device__ __forceinline__ int lanes_for(int R) {
+    constexpr int V = VecOf<T>::V;
+    const int need = (min(R, kRA) + V - 1) / V;
+    return need <= 1 ? 1 : need <= 2 ? 2 : need <= 4 ? 4 : 8;
+}
+
+// A tile for right-hand sides [cg0, cg1) with the lane split for R.
+template <typename T, int BS>
+__device__ __forceinline__ void tile_any(const MatView &M, const uint4 ta, const uint4 tb,
+                                         const unsigned char *buf, int cg0, int cg1, T *acc,
+                                         T *xt, int lane) {
+    constexpr int V = VecOf<T>::V;
+    const int R = M.nrhs;
+    if (R == 1) return tile_group<T, BS, 1, 1>(M, ta, tb, buf, cg0, cg1, acc, xt, lane);
+    switch (lanes_for<T>(R)) {
+        case 1: return tile_group<T, BS, 1, V>(M, ta, tb, buf, cg0, cg1, acc, xt, lane);
+        case 2: return tile_group<T, BS, 2, V>(M, ta, tb, buf, cg0, cg1, acc, xt, lane);
+        case 4: return tile_group<T, BS, 4, V>(M, ta, tb, buf, cg0, cg1, acc, xt, lane);
+        default: return tile_group<T, BS, 8, V>(M, ta, tb, buf, cg0, cg1, acc, xt, lane);
     }
 }
 
@@ -549,10 +610,7 @@ __global__ void __launch_bounds__(kMsWarps * 32, 4)
             const unsigned char *buf = buf0 + bi * cap;
             const int R = M.nrhs;
             if (R <= kRA) {  // one column group: runs across the block row's tiles
-                if (R == 1)
-                    tile_group<T, BS, 1>(M, ta, tb, buf, 0, 1, acc, xt, lane);
-                else
-                    tile_group<T, BS, V>(M, ta, tb, buf, 0, R, acc, xt, lane);
+                tile_any<T, BS>(M, ta, tb, buf, 0, R, acc, xt, lane);
                 ++runlen;
                 if (!cont) {
                     ms_flush<T, BS>(M, ta, tb, g, runlen, 0, R, 1, acc, ustart, nunits, lane);
@@ -562,7 +620,7 @@ __global__ void __launch_bounds__(kMsWarps * 32, 4)
                 const int groups = (R + kRA - 1) / kRA;
                 for (int cg0 = 0; cg0 < R; cg0 += kRA) {
                     const int cg1 = min(R, cg0 + kRA);
-                    tile_group<T, BS, V>(M, ta, tb, buf, cg0, cg1, acc, xt, lane);
+                    tile_any<T, BS>(M, ta, tb, buf, cg0, cg1, acc, xt, lane);
                     ms_flush<T, BS>(M, ta, tb, g, 1, cg0, cg1 - cg0, groups, acc, ustart, nunits,
                                     lane);
                 }
