@@ -802,7 +802,10 @@ int dev_resident(const void *fn, int threads, size_t smem) {
 }
 
 int dev_resident_l1(const void *fn, int threads, size_t smem) {
-    int r = dev_resident(fn, threads, smem);
+    // the occupancy query counts the carveout preference a previous launch
+    // set for a smaller footprint, so take the register and thread limit
+    // alone and the shared-memory limit from the largest carveout
+    int r = dev_resident(fn, threads, 0);
     const int d = current_device();
     int maxs = 0, reserved = 0;
     cudaDeviceGetAttribute(&maxs, cudaDevAttrMaxSharedMemoryPerMultiprocessor, d);
@@ -810,6 +813,7 @@ int dev_resident_l1(const void *fn, int threads, size_t smem) {
     if (maxs <= (int)kL1Keep) return r;
     const size_t per = smem + (size_t)reserved;
     const size_t cap = (size_t)maxs - kL1Keep;
+    r = std::min<int>(r, (int)((size_t)maxs / per));  // what fits at all
     r = std::max(1, std::min<int>(r, (int)(cap / std::max<size_t>(per, 1))));
     const int pct = (int)std::min<size_t>(100, (r * per * 100 + maxs - 1) / (size_t)maxs);
     std::lock_guard<std::mutex> lock(g_facts_mu);

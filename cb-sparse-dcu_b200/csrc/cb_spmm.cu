@@ -685,8 +685,10 @@ cudaError_t ms_launch_t(const MatView &single, const MatView *mats, int nmats,
     if (e != cudaSuccess) return e;
     if (cap % 16 || !sched || !err) return cudaErrorInvalidValue;
     if (nunits <= 0) return cudaSuccess;
-    // dynamic: resident warps (or fewer); static: one warp per unit
-    const int64_t w = dynamic ? std::min<int64_t>(ms_warps_t<T, BS>(cap), nunits) : nunits;
+    // dynamic: resident warps (or fewer); static: one warp per unit.  The
+    // resident count also sets the kernel's carveout for this buffer size.
+    const int64_t resident_warps = ms_warps_t<T, BS>(cap);
+    const int64_t w = dynamic ? std::min<int64_t>(resident_warps, nunits) : nunits;
     const int64_t ctas = (w + kMsWarps - 1) / kMsWarps;
     cb_mslice_kernel<T, BS><<<(unsigned)ctas, kMsWarps * 32, smem, stream>>>(
         single, mats, nmats, toff, ustart, nunits, dynamic, cap, sched, err, wait_polls());
