@@ -1041,6 +1041,7 @@ struct cbspmv_batch {
     bool bound = false;
     cb::MatView *d_views = nullptr;
     int64_t *d_toff = nullptr, *d_ustart = nullptr;
+    int32_t *d_uorder = nullptr;    // queue order of the units
     int64_t ntot = 0, nunits = 0;   // tiles and scheduling units
     uint32_t *d_sched = nullptr;    // 2 scheduler words (unit counter, warps out)
     uint32_t *herr = nullptr, *derr = nullptr;  // error word (host-mapped)
@@ -1055,7 +1056,8 @@ struct cbspmv_batch {
             if (e) cudaEventDestroy(e);
         for (cudaStream_t &c : cap)
             if (c) cudaStreamDestroy(c);
-        for (void *p : {(void *)d_toff, (void *)d_ustart, (void *)d_sched, (void *)d_views})
+        for (void *p : {(void *)d_toff, (void *)d_ustart, (void *)d_uorder, (void *)d_sched,
+                        (void *)d_views})
             if (p) cudaFree(p);
         if (herr) cudaFreeHost(herr);
     }
@@ -1102,8 +1104,8 @@ cbspmv_status batch_each(cbspmv_batch *b, cudaStream_t st) {
 // One persistent launch over every matrix of the batch.
 cbspmv_status batch_one(cbspmv_batch *b, cudaStream_t st) {
     const cudaError_t e = cb::launch_batch(b->bs, b->f32, b->d_views, (int)b->plans.size(),
-                                           b->d_toff, b->d_ustart, b->nunits, b->tile_cap,
-                                           b->d_sched, b->derr, st);
+                                           b->d_toff, b->d_ustart, b->d_uorder, b->nunits,
+                                           b->tile_cap, b->d_sched, b->derr, st);
     return e == cudaSuccess ? CBSPMV_OK : cuda_fail(e, "batch launch");
 }
 
@@ -1150,18 +1152,46 @@ cbspmv_status cbspmv_batch_create(cbspmv_plan *const *plans, int count, const in
         toff.push_back(toff.back() + (int64_t)s.lay.tiles.size());
     }
     b->ntot = toff.back();
-    // about four units per resident warp, at least two tiles each
-    std::vector<int64_t> us;
-    const int64_t target = std::max<int64_t>(
-        2, b->ntot / (std::max<int64_t>(1, cb::ms_warps(b->bs, b->f32, b->tile_cap)) * 4));
+    // Scheduling units by cost (a tile's entries and block values times its
+    // passes over the right-hand sides): about eight per resident warp, cut
+    // at block-row starts once a unit holds its share, anywhere at twice
+    // that; queued costliest first, so the launch does not end on a long one.
+    std::vector<int64_t> cost(b->ntot);
+    double total = 0;
     for (int k = 0; k < count; ++k) {
         const DevSide &s = plans[k]->A;
-        cb::ms_unit_starts(reinterpret_cast<const uint32_t *>(s.lay.tiles.data()),
-                           (int64_t)s.lay.tiles.size(), target, toff[k], us);
+        const uint32_t *t8 = reinterpret_cast<const uint32_t *>(s.lay.tiles.data());
+        const uint32_t *b4 = reinterpret_cast<const uint32_t *>(s.lay.blocks.data());
+        for (int64_t t = 0; t < (int64_t)s.lay.tiles.size(); ++t)
+            total += (double)(cost[toff[k] + t] = cb::ms_tile_cost_rhs(t8 + 8 * t, b4, nrhs[k],
+                                                                       b->f32));
     }
-    b->nunits = (int64_t)us.size();
-    us.push_back(b->ntot);
-    std::vector<int64_t> &all = us;
+    const double share =
+        total / (double)(std::max<int64_t>(1, cb::ms_warps(b->bs, b->f32, b->tile_cap)) * 8);
+    std::vector<int64_t> all;
+    std::vector<double> ucost;
+    double acc = 0;
+    for (int k = 0; k < count; ++k) {
+        const DevSide &s = plans[k]->A;
+        const uint32_t *t8 = reinterpret_cast<const uint32_t *>(s.lay.tiles.data());
+        for (int64_t t = 0; t < (int64_t)s.lay.tiles.size(); ++t) {
+            const uint32_t *d = t8 + 8 * t;
+            const bool row_start = d[5] == 0xffffffffu || d[5] == d[6];
+            if (all.empty() || (acc >= share && row_start) || acc >= 2 * share) {
+                if (!all.empty()) ucost.push_back(acc);
+                all.push_back(toff[k] + t);
+                acc = 0;
+            }
+            acc += (double)cost[toff[k] + t];
+        }
+    }
+    if (!all.empty()) ucost.push_back(acc);
+    b->nunits = (int64_t)all.size();
+    all.push_back(b->ntot);
+    std::vector<int32_t> order(b->nunits);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int32_t a, int32_t c) { return ucost[a] > ucost[c]; });
     cudaError_t e = cudaMalloc((void **)&b->d_ustart, all.size() * sizeof(int64_t));
     if (e == cudaSuccess)
         e = cudaMemcpy(b->d_ustart, all.data(), all.size() * sizeof(int64_t),
@@ -1169,6 +1199,11 @@ cbspmv_status cbspmv_batch_create(cbspmv_plan *const *plans, int count, const in
     if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_toff, toff.size() * sizeof(int64_t));
     if (e == cudaSuccess)
         e = cudaMemcpy(b->d_toff, toff.data(), toff.size() * sizeof(int64_t),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && !order.empty())
+        e = cudaMalloc((void **)&b->d_uorder, order.size() * sizeof(int32_t));
+    if (e == cudaSuccess && !order.empty())
+        e = cudaMemcpy(b->d_uorder, order.data(), order.size() * sizeof(int32_t),
                        cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_sched, 16);
     if (e == cudaSuccess) e = cudaMemset(b->d_sched, 0, 16);

@@ -78,12 +78,16 @@ cudaError_t launch_spmm(const DevLayout &d, const void *x, void *y, int nrhs, in
                         int64_t ldy, cudaStream_t stream);
 // The same kernel over a device table of nmats matrices (each with its own
 // right-hand-side count) in ONE launch: tile offsets toff[nmats + 1], units
-// ustart[nunits + 1] over the concatenated tiles, shared buffers of cap bytes
-// (>= every matrix's largest tile), two scheduler words (zero before the
-// first launch; the kernel leaves them zero) and an error word.
+// ustart[nunits + 1] over the concatenated tiles taken in the queue order
+// uorder[nunits], shared buffers of cap bytes (>= every matrix's largest
+// tile), two scheduler words (zero before the first launch; the kernel leaves
+// them zero) and an error word.
 cudaError_t launch_batch(int bs, int f32, const MatView *mats, int nmats, const int64_t *toff,
-                         const int64_t *ustart, int64_t nunits, uint32_t cap, uint32_t *sched,
-                         uint32_t *err, cudaStream_t stream);
+                         const int64_t *ustart, const int32_t *uorder, int64_t nunits,
+                         uint32_t cap, uint32_t *sched, uint32_t *err, cudaStream_t stream);
+// Relative cost of one tile of a matrix with nrhs right-hand sides (the
+// entries and block values it reads, times its passes over V columns).
+int64_t ms_tile_cost_rhs(const uint32_t *tile8, const uint32_t *blocks4, int nrhs, int f32);
 
 // The direct kernel's scheduling units: each block row's tiles in pieces of
 // at most kDirectUnitTiles, starting at the row's first tile; direct_units

@@ -447,14 +447,16 @@ __device__ __forceinline__ void advance(Cursor &c, int64_t g, const int64_t *__r
 // warp w runs unit w (host cost-balanced ranges, one per warp).  dynamic = 1:
 // units of at least two tiles but the last, boundaries at block-row starts
 // where the host could place them, taken from a counter (sched[0]) one unit
-// ahead; the warp whose exit completes sched[1] == number of warps resets
-// both for the next launch.
+// ahead, in the queue order uorder (the costliest first; NULL: unit order);
+// the warp whose exit completes sched[1] == number of warps resets both for
+// the next launch.
 template <typename T, int BS>
 __global__ void __launch_bounds__(kMsWarps * 32, 4)
     cb_mslice_kernel(const MatView single, const MatView *__restrict__ mats, int nmats,
                      const int64_t *__restrict__ toff, const int64_t *__restrict__ ustart,
-                     int64_t nunits, int dynamic, uint32_t cap, uint32_t *__restrict__ sched,
-                     uint32_t *__restrict__ err, uint32_t limit) {
+                     const int32_t *__restrict__ uorder, int64_t nunits, int dynamic,
+                     uint32_t cap, uint32_t *__restrict__ sched, uint32_t *__restrict__ err,
+                     uint32_t limit) {
     using SL = MsLayout<T, BS>;
     constexpr int V = SL::V;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -496,6 +498,7 @@ __global__ void __launch_bounds__(kMsWarps * 32, 4)
     auto resolve = [&]() {
         if (!ub_known) {
             ub = (int64_t)__shfl_sync(kFull, ub_raw, 0);
+            if (ub < nunits && uorder) ub = __ldg(&uorder[ub]);  // queue order
             if (ub < nunits) {
                 ub_s = __ldg(&ustart[ub]);
                 ub_e = __ldg(&ustart[ub + 1]);
@@ -678,8 +681,9 @@ int64_t ms_warps_t(uint32_t cap) {
 
 template <typename T, int BS>
 cudaError_t ms_launch_t(const MatView &single, const MatView *mats, int nmats,
-                        const int64_t *toff, const int64_t *ustart, int64_t nunits, int dynamic,
-                        uint32_t cap, uint32_t *sched, uint32_t *err, cudaStream_t stream) {
+                        const int64_t *toff, const int64_t *ustart, const int32_t *uorder,
+                        int64_t nunits, int dynamic, uint32_t cap, uint32_t *sched,
+                        uint32_t *err, cudaStream_t stream) {
     size_t smem = 0;
     cudaError_t e = ms_configure<T, BS>(cap, &smem);
     if (e != cudaSuccess) return e;
@@ -691,7 +695,8 @@ cudaError_t ms_launch_t(const MatView &single, const MatView *mats, int nmats,
     const int64_t w = dynamic ? std::min<int64_t>(resident_warps, nunits) : nunits;
     const int64_t ctas = (w + kMsWarps - 1) / kMsWarps;
     cb_mslice_kernel<T, BS><<<(unsigned)ctas, kMsWarps * 32, smem, stream>>>(
-        single, mats, nmats, toff, ustart, nunits, dynamic, cap, sched, err, wait_polls());
+        single, mats, nmats, toff, ustart, uorder, nunits, dynamic, cap, sched, err,
+        wait_polls());
     note_launch();
     return cudaGetLastError();
 }
@@ -756,6 +761,11 @@ int64_t ms_tile_cost(const uint32_t *tile8, const uint32_t *blocks4) {
     return work;
 }
 
+int64_t ms_tile_cost_rhs(const uint32_t *tile8, const uint32_t *blocks4, int nrhs, int f32) {
+    const int V = f32 ? 4 : 2;
+    return ms_tile_cost(tile8, blocks4) * (int64_t)((nrhs + V - 1) / V);
+}
+
 void ms_unit_starts(const uint32_t *tile8, int64_t ntiles, int64_t target, int64_t base,
                     std::vector<int64_t> &ustart) {
     for (int64_t t = 0; t < ntiles; ++t) {
@@ -776,18 +786,18 @@ cudaError_t launch_spmm(const DevLayout &d, const void *x, void *y, int nrhs, in
     const MatView M = mat_view(d, x, y, nrhs, ldx, ldy);
     return by_type(d.bs, d.f32, [&](auto t, auto b) {
         using T = decltype(t);
-        return ms_launch_t<T, b()>(M, nullptr, 1, nullptr, d.ustart, d.nunits, 0, d.mcap,
-                                   d.sched, d.err, stream);
+        return ms_launch_t<T, b()>(M, nullptr, 1, nullptr, d.ustart, nullptr, d.nunits, 0,
+                                   d.mcap, d.sched, d.err, stream);
     });
 }
 
 cudaError_t launch_batch(int bs, int f32, const MatView *mats, int nmats, const int64_t *toff,
-                         const int64_t *ustart, int64_t nunits, uint32_t cap, uint32_t *sched,
-                         uint32_t *err, cudaStream_t stream) {
+                         const int64_t *ustart, const int32_t *uorder, int64_t nunits,
+                         uint32_t cap, uint32_t *sched, uint32_t *err, cudaStream_t stream) {
     return by_type(bs, f32, [&](auto t, auto b) {
         using T = decltype(t);
-        return ms_launch_t<T, b()>(MatView(), mats, nmats, toff, ustart, nunits, 1, cap, sched,
-                                   err, stream);
+        return ms_launch_t<T, b()>(MatView(), mats, nmats, toff, ustart, uorder, nunits, 1, cap,
+                                   sched, err, stream);
     });
 }
 
