@@ -1177,7 +1177,10 @@ cbspmv_status cbspmv_batch_create(cbspmv_plan *const *plans, int count, const in
         for (int64_t t = 0; t < (int64_t)s.lay.tiles.size(); ++t) {
             const uint32_t *d = t8 + 8 * t;
             const bool row_start = d[5] == 0xffffffffu || d[5] == d[6];
-            if (all.empty() || (acc >= share && row_start) || acc >= 2 * share) {
+            // (a unit holds two tiles at least, but the last: the kernel stages
+            // two tiles ahead across one unit boundary)
+            const bool two = !all.empty() && toff[k] + t - all.back() >= 2;
+            if (all.empty() || (two && ((acc >= share && row_start) || acc >= 2 * share))) {
                 if (!all.empty()) ucost.push_back(acc);
                 all.push_back(toff[k] + t);
                 acc = 0;

@@ -68,13 +68,13 @@ struct VecOf {
 
 // Per-warp shared memory: [acc | xt | mbar[2] | buf[2]].  acc: BS rows x kRA
 // right-hand sides (row r, column c at acc[r * kRA + c]); xt: the x rows of
-// the CSR/DENSE blocks of one step (at most 32 x rows of V values for every
-// block column); buf: one tile payload (`cap` bytes).
+// the CSR/DENSE blocks of one step (RL * V values for every block column of
+// BPS blocks, at most 4 V); buf: one tile payload (`cap` bytes).
 template <typename T, int BS>
 struct MsLayout {
     static constexpr int V = VecOf<T>::V;
     static constexpr uint32_t acc_bytes = BS * kRA * sizeof(T);
-    static constexpr uint32_t xt_bytes = BS * 8 * V * sizeof(T);
+    static constexpr uint32_t xt_bytes = BS * 4 * V * sizeof(T);
     static constexpr uint32_t head = a16(acc_bytes + xt_bytes + 16);
     __host__ __device__ static uint32_t bytes(uint32_t cap) { return head + 2 * cap; }
 };
@@ -330,13 +330,14 @@ __device__ __forceinline__ void tile_group(const MatView &M, const uint4 ta, con
     }
 }
 
-// Lanes per entry for R right-hand sides: the fewest (a power of two, at
-// most 8) whose RL * V values cover min(R, kRA).
+// Lanes per entry for R right-hand sides: the fewest (1, 2 or 4) whose
+// RL * V values cover min(R, kRA), or 4 (more passes).  Three lane splits
+// keep the kernel's code small enough for the instruction cache.
 template <typename T>
 __device__ __forceinline__ int lanes_for(int R) {
     constexpr int V = VecOf<T>::V;
     const int need = (min(R, kRA) + V - 1) / V;
-    return need <= 1 ? 1 : need <= 2 ? 2 : need <= 4 ? 4 : 8;
+    return need <= 1 ? 1 : need <= 2 ? 2 : 4;
 }
 
 // A tile for right-hand sides [cg0, cg1) with the lane split for R.
@@ -345,13 +346,10 @@ __device__ __forceinline__ void tile_any(const MatView &M, const uint4 ta, const
                                          const unsigned char *buf, int cg0, int cg1, T *acc,
                                          T *xt, int lane) {
     constexpr int V = VecOf<T>::V;
-    const int R = M.nrhs;
-    if (R == 1) return tile_group<T, BS, 1, 1>(M, ta, tb, buf, cg0, cg1, acc, xt, lane);
-    switch (lanes_for<T>(R)) {
+    switch (lanes_for<T>(M.nrhs)) {
         case 1: return tile_group<T, BS, 1, V>(M, ta, tb, buf, cg0, cg1, acc, xt, lane);
         case 2: return tile_group<T, BS, 2, V>(M, ta, tb, buf, cg0, cg1, acc, xt, lane);
-        case 4: return tile_group<T, BS, 4, V>(M, ta, tb, buf, cg0, cg1, acc, xt, lane);
-        default: return tile_group<T, BS, 8, V>(M, ta, tb, buf, cg0, cg1, acc, xt, lane);
+        default: return tile_group<T, BS, 4, V>(M, ta, tb, buf, cg0, cg1, acc, xt, lane);
     }
 }
 
