@@ -1155,7 +1155,8 @@ cbspmv_status cbspmv_batch_create(cbspmv_plan *const *plans, int count, const in
     // Scheduling units by cost (a tile's entries and block values times its
     // passes over the right-hand sides): about eight per resident warp, cut
     // at block-row starts once a unit holds its share, anywhere at twice
-    // that; queued costliest first, so the launch does not end on a long one.
+    // that; queued by lane split, costliest first within one, so the launch
+    // does not end on a long unit.
     std::vector<int64_t> cost(b->ntot);
     double total = 0;
     for (int k = 0; k < count; ++k) {
@@ -1170,6 +1171,11 @@ cbspmv_status cbspmv_batch_create(cbspmv_plan *const *plans, int count, const in
         total / (double)(std::max<int64_t>(1, cb::ms_warps(b->bs, b->f32, b->tile_cap)) * 8);
     std::vector<int64_t> all;
     std::vector<double> ucost;
+    std::vector<int> uclass;  // lane split of the unit's first matrix
+    auto lane_class = [&](int r) {
+        const int V = b->f32 ? 4 : 2, need = (std::min(r, 16) + V - 1) / V;
+        return need <= 1 ? 0 : need <= 2 ? 1 : 2;
+    };
     double acc = 0;
     for (int k = 0; k < count; ++k) {
         const DevSide &s = plans[k]->A;
@@ -1183,6 +1189,7 @@ cbspmv_status cbspmv_batch_create(cbspmv_plan *const *plans, int count, const in
             if (all.empty() || (two && ((acc >= share && row_start) || acc >= 2 * share))) {
                 if (!all.empty()) ucost.push_back(acc);
                 all.push_back(toff[k] + t);
+                uclass.push_back(lane_class(nrhs[k]));
                 acc = 0;
             }
             acc += (double)cost[toff[k] + t];
@@ -1193,8 +1200,11 @@ cbspmv_status cbspmv_batch_create(cbspmv_plan *const *plans, int count, const in
     all.push_back(b->ntot);
     std::vector<int32_t> order(b->nunits);
     std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int32_t a, int32_t c) { return ucost[a] > ucost[c]; });
+    // by lane split first, so the warps on one SM mostly run the same code
+    // (the instruction cache), then costliest first
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t c) {
+        return uclass[a] != uclass[c] ? uclass[a] > uclass[c] : ucost[a] > ucost[c];
+    });
     cudaError_t e = cudaMalloc((void **)&b->d_ustart, all.size() * sizeof(int64_t));
     if (e == cudaSuccess)
         e = cudaMemcpy(b->d_ustart, all.data(), all.size() * sizeof(int64_t),
