@@ -104,6 +104,10 @@ def _load():
         "cbspmv_adjoint": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int, _I64, _I64,
                                           _I64, _P]),
         "cbspmv_num_values": (_I64, [_P]),
+        "cbspmv_adjoint_fused": (ctypes.c_int, [_P, _P, _P, _P, _P, ctypes.c_int, _I64, _I64,
+                                                _I64, _P]),
+        "cbspmv_grad_size_t": (_I64, [_P]),
+        "cbspmv_grad_positions_t": (ctypes.c_int, [_P, _P]),
         "cbspmv_set_values": (ctypes.c_int, [_P, _P, _P]),
         "cbspmv_value_coords": (ctypes.c_int, [_P, _P, _P, _P]),
         "cbspmv_input_slots": (ctypes.c_int, [_P, _P]),
@@ -406,6 +410,32 @@ class Plan:
                                    _dptr(gvals) if gvals is not None else None,
                                    k, k, k, k, _stream(stream)))
         return gx, gvals
+
+    def adjoint_fused(self, g, x, gx=None, gvals_t=None, stream=None):
+        """(A^T g, value gradient) in one kernel launch on the transposed
+        layout; the value gradient is indexed by A^T payload position (see
+        ``grad_positions_t``).  Returns (gx, gvals_t)."""
+        import torch
+        self.upload(stream)
+        self._check_dev(g, x)
+        k = 1 if g.dim() == 1 else g.shape[1]
+        if gx is None:
+            gx = torch.empty((self.n,) if g.dim() == 1 else (self.n, k),
+                             dtype=g.dtype, device=g.device)
+        if gvals_t is None:
+            gvals_t = torch.empty(int(_lib.cbspmv_grad_size_t(self._h)), dtype=g.dtype,
+                                  device=g.device)
+        self._check_dev(gx, gvals_t)
+        _check(_lib.cbspmv_adjoint_fused(self._h, _dptr(g), _dptr(x), _dptr(gx),
+                                         _dptr(gvals_t), k, k, k, k, _stream(stream)))
+        return gx, gvals_t
+
+    def grad_positions_t(self) -> np.ndarray:
+        """For each input nonzero, its position in ``adjoint_fused``'s value
+        gradient."""
+        pos = np.zeros(self.nnz, np.int64)
+        _check(_lib.cbspmv_grad_positions_t(self._h, _np_ptr(pos)))
+        return pos
 
     def set_values(self, vals, stream=None):
         """Re-pack A (and A^T) from new input values (nnz, caller order)."""

@@ -857,6 +857,51 @@ cbspmv_status cbspmv_adjoint(cbspmv_plan *p, const void *g, const void *x, void 
     return rc;
 }
 
+cbspmv_status cbspmv_adjoint_fused(cbspmv_plan *p, const void *g, const void *x, void *gx,
+                                   void *gvals_t, int nrhs, int64_t ldg, int64_t ldx,
+                                   int64_t ldgx, void *stream) {
+    if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
+    if (!p->has_t) return fail(CBSPMV_ERR_STATE, "plan built without want_transpose");
+    if (!p->uploaded) return fail(CBSPMV_ERR_STATE, "plan not uploaded");
+    if (p->AT.lay.unit)
+        return fail(CBSPMV_ERR_UNSUPPORTED,
+                    "this plan stores no values (every value was 1); build it with "
+                    "keep_values = 1 for a value gradient");
+    if (nrhs < 1) return fail(CBSPMV_ERR_INVALID, "nrhs must be >= 1");
+    if (ldg == 0) ldg = nrhs;
+    if (ldx == 0) ldx = nrhs;
+    if (ldgx == 0) ldgx = nrhs;
+    if (ldg < nrhs || ldx < nrhs || ldgx < nrhs)
+        return fail(CBSPMV_ERR_INVALID, "leading dimension smaller than nrhs");
+    DevSide &s = p->AT;
+    if ((s.lay.m > 0 && (!gx || !x)) || (s.lay.n > 0 && !g) || !gvals_t)
+        return fail(CBSPMV_ERR_INVALID, "null g, x, gx or gvals_t");
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev != p->device) return fail(CBSPMV_ERR_STATE, "plan was uploaded to another device");
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cbspmv_status rc = take_device_error(p, 1, st)) return rc;
+    if (cbspmv_status rc = ensure_partials(s, nrhs, vsize(p))) return rc;
+    CB_CUDA(cb::launch_spmm(s.d, g, gx, nrhs, ldg, ldgx, st, gvals_t, x, ldx),
+            "fused adjoint launch");
+    return CBSPMV_OK;
+}
+
+int64_t cbspmv_grad_size_t(const cbspmv_plan *p) {
+    if (!p || !p->has_t) return -1;
+    return (int64_t)(p->AT.lay.payload.size() / vsize(p));
+}
+
+cbspmv_status cbspmv_grad_positions_t(const cbspmv_plan *p, int64_t *pos) {
+    if (!p || !pos) return fail(CBSPMV_ERR_INVALID, "null argument");
+    if (!p->has_t) return fail(CBSPMV_ERR_STATE, "plan built without want_transpose");
+    if (cbspmv_status rc = refuse_spmv_only(p)) return rc;
+    const cb::DeviceLayout &L = p->AT.lay;
+    const int64_t vsz = (int64_t)vsize(p);
+    for (int64_t i = 0; i < p->host.nnz; ++i) pos[i] = (int64_t)L.val_off[L.input_slot[i]] / vsz;
+    return CBSPMV_OK;
+}
+
 int64_t cbspmv_num_values(const cbspmv_plan *p) { return p ? p->A.lay.nvals : -1; }
 
 cbspmv_status cbspmv_set_values(cbspmv_plan *p, const void *input_values,

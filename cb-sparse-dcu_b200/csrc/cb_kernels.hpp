@@ -54,6 +54,12 @@ struct MatView {
     int xvec = 0;               // x rows allow vector loads of V values
     int unit = 0;               // no stored values (all 1), DENSE as bitmasks
     uint32_t pay16_end = 0;     // payload size in 16-byte units
+    // value gradient in the same pass (the transposed layout of an adjoint):
+    // gv[p] = sum_j x[col, j] * xo[row, j] for the value at payload position p
+    // (the payload read as an array of values); NULL: none
+    void *gv = nullptr;
+    const void *xo = nullptr;   // row vectors of the layout's rows, stride ldo
+    int64_t ldo = 0;
 };
 
 // Shared-memory buffer bytes for tiles of at most max_tile_bytes.
@@ -74,8 +80,12 @@ void ms_unit_starts(const uint32_t *tile8, int64_t ntiles, int64_t target, int64
                     std::vector<int64_t> &ustart);
 // Y = A X through the multi-right-hand-side kernel (d.mcap, d.ustart,
 // d.nunits set; scheduler words d.sched[0..1], error word d.err).
+// With gv: also the value gradient of every stored value, gv[p] = sum over
+// the right-hand sides of x[col] . xo[row] for the value at payload position
+// p (the payload read as an array of values; xo row-major, stride ldo).
 cudaError_t launch_spmm(const DevLayout &d, const void *x, void *y, int nrhs, int64_t ldx,
-                        int64_t ldy, cudaStream_t stream);
+                        int64_t ldy, cudaStream_t stream, void *gv = nullptr,
+                        const void *xo = nullptr, int64_t ldo = 0);
 // The same kernel over a device table of nmats matrices (each with its own
 // right-hand-side count) in ONE launch: tile offsets toff[nmats + 1], units
 // ustart[nunits + 1] over the concatenated tiles taken in the queue order

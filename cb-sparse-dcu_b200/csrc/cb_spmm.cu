@@ -66,7 +66,7 @@ struct VecOf {
     static constexpr int V = sizeof(T) == 4 ? 4 : 2;
 };
 
-// Per-warp shared memory: [acc | xt | mbar[2] | buf[2]].  acc: BS rows x kRA
+// Per-warp shared memory: [acc | xt | xo | mbar[2] | buf[2]].  acc: BS rows x kRA
 // right-hand sides (row r, column c at acc[r * kRA + c]); xt: the x rows of
 // the CSR/DENSE blocks of one step (RL * V values for every block column of
 // BPS blocks, at most 4 V); buf: one tile payload (`cap` bytes).
@@ -75,7 +75,8 @@ struct MsLayout {
     static constexpr int V = VecOf<T>::V;
     static constexpr uint32_t acc_bytes = BS * kRA * sizeof(T);
     static constexpr uint32_t xt_bytes = BS * 4 * V * sizeof(T);
-    static constexpr uint32_t head = a16(acc_bytes + xt_bytes + 16);
+    static constexpr uint32_t xo_bytes = BS * 4 * V * sizeof(T);
+    static constexpr uint32_t head = a16(acc_bytes + xt_bytes + xo_bytes + 16);
     __host__ __device__ static uint32_t bytes(uint32_t cap) { return head + 2 * cap; }
 };
 
@@ -118,9 +119,11 @@ __device__ __forceinline__ void ldg_row(const T *p, bool vec, int nv, T (&o)[NV]
 // the single-vector streaming kernel (slice_sums, cb_device.cuh).  Each row
 // of the tile is added by exactly one group, so no two lanes write one
 // accumulator.
-template <typename T, int BS, int RL, int NV>
-__device__ __forceinline__ void coo_pass(const MatView &M, const unsigned char *buf, int E,
-                                         int c0, int ca, T *__restrict__ acc, int lane) {
+template <typename T, int BS, int RL, int NV, bool GV>
+__device__ __forceinline__ void coo_pass(const MatView &M, const uint4 ta,
+                                         const unsigned char *buf, int E, int c0, int ca,
+                                         T *__restrict__ acc, const T *__restrict__ xo,
+                                         int lane) {
     constexpr uint32_t kNone = 63;  // row of a group with no entry (after every real row)
     constexpr int G = 32 / RL;
     const int g = lane / RL, sub = lane % RL;
@@ -160,6 +163,20 @@ __device__ __forceinline__ void coo_pass(const MatView &M, const unsigned char *
             } else {
 #pragma unroll
                 for (int v = 0; v < NV; ++v) xv[u][v] = T(0);
+            }
+        }
+        if (GV) {  // value gradient: x row . own row, summed over the group's lanes
+            T *gv = static_cast<T *>(M.gv) +
+                    ((size_t)ta.w * 16 + a16(4u * E)) / sizeof(T);
+#pragma unroll
+            for (int u = 0; u < kSub; ++u) {
+                const int r = pos[u] < E ? (int)(w[u] >> 27) : 0;
+                T d = T(0);
+#pragma unroll
+                for (int v = 0; v < NV; ++v) d = fma(xv[u][v], xo[r * RL * NV + sub * NV + v], d);
+#pragma unroll
+                for (int o = RL / 2; o > 0; o >>= 1) d += __shfl_xor_sync(kFull, d, o);
+                if (sub == 0 && pos[u] < E) gv[pos[u]] = c0 == 0 ? d : gv[pos[u]] + d;
             }
         }
 #pragma unroll
@@ -227,10 +244,11 @@ __device__ __forceinline__ void coo_pass(const MatView &M, const unsigned char *
 // its block (DENSE columns in a rotated order, so the slots of a step read
 // distinct banks); with two blocks per step the second block's slots hand
 // their sums to the first by a shuffle, so each row is added by one group.
-template <typename T, int BS, int RL, int NV>
+template <typename T, int BS, int RL, int NV, bool GV>
 __device__ __forceinline__ void blk_pass(const MatView &M, const uint4 ta,
                                          const unsigned char *buf, int c0, int ca,
-                                         T *__restrict__ acc, T *__restrict__ xt, int lane) {
+                                         T *__restrict__ acc, T *__restrict__ xt,
+                                         const T *__restrict__ xo, int lane) {
     constexpr int P = 32 / RL;
     constexpr int BPS = P >= BS ? P / BS : 1;  // blocks per step (1 or 2)
     constexpr int RW = RL * NV;                // x values per column
@@ -274,6 +292,9 @@ __device__ __forceinline__ void blk_pass(const MatView &M, const uint4 ta,
         const uint32_t mb = __shfl_sync(kFull, bd.y, jc);
         const unsigned char *pb = buf + off;
         const T *xq = xt + q * BS * RW + sub * NV;
+        // value gradient: the lanes of one row slot sum their pieces
+        const unsigned gmask = (RL == 1 ? 1u : ((1u << RL) - 1u)) << (p * RL);
+        T *gvb = GV ? static_cast<T *>(M.gv) + ((size_t)ta.w * 16 + off) / sizeof(T) : nullptr;
 #pragma unroll 1
         for (int row = prow; row < BS; row += (BPS > 1 ? BS : P)) {
             T sum[NV];
@@ -286,11 +307,21 @@ __device__ __forceinline__ void blk_pass(const MatView &M, const uint4 ta,
                     const IdxT *ci = rp + BS + 1;
                     const T *vv = reinterpret_cast<const T *>(
                         pb + a16((uint32_t)((BS + 1 + k) * sizeof(IdxT))));
+                    const int vo = (int)(a16((uint32_t)((BS + 1 + k) * sizeof(IdxT))) / sizeof(T));
                     for (int e = rp[row]; e < (int)rp[row + 1]; ++e) {
                         const T av = M.unit ? T(1) : vv[e];
                         const int c = ci[e];
 #pragma unroll
                         for (int v = 0; v < NV; ++v) sum[v] = fma(av, xq[c * RW + v], sum[v]);
+                        if (GV) {
+                            T d = T(0);
+#pragma unroll
+                            for (int v = 0; v < NV; ++v)
+                                d = fma(xq[c * RW + v], xo[row * RW + sub * NV + v], d);
+#pragma unroll
+                            for (int o = RL / 2; o > 0; o >>= 1) d += __shfl_xor_sync(gmask, d, o);
+                            if (sub == 0) gvb[vo + e] = c0 == 0 ? d : gvb[vo + e] + d;
+                        }
                     }
                 } else {  // DENSE, row-major BS x BS
 #pragma unroll 4
@@ -299,6 +330,18 @@ __device__ __forceinline__ void blk_pass(const MatView &M, const uint4 ta,
                         const T av = dense_at<T, BS>(pb, M.unit, row, cc);
 #pragma unroll
                         for (int v = 0; v < NV; ++v) sum[v] = fma(av, xq[cc * RW + v], sum[v]);
+                        if (GV) {
+                            T d = T(0);
+#pragma unroll
+                            for (int v = 0; v < NV; ++v)
+                                d = fma(xq[cc * RW + v], xo[row * RW + sub * NV + v], d);
+#pragma unroll
+                            for (int o = RL / 2; o > 0; o >>= 1) d += __shfl_xor_sync(gmask, d, o);
+                            if (sub == 0) {
+                                T *gp = gvb + row * BS + cc;
+                                *gp = c0 == 0 ? d : *gp + d;
+                            }
+                        }
                     }
                 }
             }
@@ -316,17 +359,45 @@ __device__ __forceinline__ void blk_pass(const MatView &M, const uint4 ta,
     }
 }
 
-// Adds a staged tile into the accumulators for right-hand sides [cg0, cg1)
-// (accumulator column c - cg0), RL * NV at a time.
+// Value-gradient passes: the block row's own vectors for right-hand sides
+// c0 + [0, RL * NV) into xo (row r, piece s at xo[r * RL * NV + s * NV]).
 template <typename T, int BS, int RL, int NV>
+__device__ __forceinline__ void stage_xo(const MatView &M, const uint4 ta, int c0, T *xo,
+                                         int lane) {
+    const bool vec = M.xvec != 0;
+    __syncwarp();  // the previous pass is done with xo
+    for (int i = lane; i < BS * RL; i += 32) {
+        const int r = i / RL, sp = i % RL;
+        const int64_t row = (int64_t)ta.y * BS + r;
+        const int cs = c0 + sp * NV;
+        const int ns = max(0, min(NV, M.nrhs - cs));
+        T v[NV];
+        if (row < M.m && ns > 0) {
+            ldg_row<T, NV>(static_cast<const T *>(M.xo) + (size_t)row * (size_t)M.ldo + cs,
+                           vec && M.ldo % NV == 0, ns, v);
+        } else {
+#pragma unroll
+            for (int k = 0; k < NV; ++k) v[k] = T(0);
+        }
+#pragma unroll
+        for (int k = 0; k < NV; ++k) xo[i * NV + k] = v[k];
+    }
+    __syncwarp();
+}
+
+// Adds a staged tile into the accumulators for right-hand sides [cg0, cg1)
+// (accumulator column c - cg0), RL * NV at a time; with M.gv, also the value
+// gradient of every stored value of the tile.
+template <typename T, int BS, int RL, int NV, bool GV>
 __device__ __forceinline__ void tile_group(const MatView &M, const uint4 ta, const uint4 tb,
                                            const unsigned char *buf, int cg0, int cg1, T *acc,
-                                           T *xt, int lane) {
+                                           T *xt, T *xo, int lane) {
     const int E = (int)tb.x;
     const int nxt = (ta.z >> 16) & 0xff;
     for (int c0 = cg0; c0 < cg1; c0 += RL * NV) {
-        if (E > 0) coo_pass<T, BS, RL, NV>(M, buf, E, c0, c0 - cg0, acc, lane);
-        if (nxt) blk_pass<T, BS, RL, NV>(M, ta, buf, c0, c0 - cg0, acc, xt, lane);
+        if (GV) stage_xo<T, BS, RL, NV>(M, ta, c0, xo, lane);
+        if (E > 0) coo_pass<T, BS, RL, NV, GV>(M, ta, buf, E, c0, c0 - cg0, acc, xo, lane);
+        if (nxt) blk_pass<T, BS, RL, NV, GV>(M, ta, buf, c0, c0 - cg0, acc, xt, xo, lane);
     }
 }
 
@@ -341,15 +412,16 @@ __device__ __forceinline__ int lanes_for(int R) {
 }
 
 // A tile for right-hand sides [cg0, cg1) with the lane split for R.
-template <typename T, int BS>
+template <typename T, int BS, bool GV>
 __device__ __forceinline__ void tile_any(const MatView &M, const uint4 ta, const uint4 tb,
                                          const unsigned char *buf, int cg0, int cg1, T *acc,
-                                         T *xt, int lane) {
+                                         T *xt, T *xo, int lane) {
     constexpr int V = VecOf<T>::V;
     switch (lanes_for<T>(M.nrhs)) {
-        case 1: return tile_group<T, BS, 1, V>(M, ta, tb, buf, cg0, cg1, acc, xt, lane);
-        case 2: return tile_group<T, BS, 2, V>(M, ta, tb, buf, cg0, cg1, acc, xt, lane);
-        default: return tile_group<T, BS, 4, V>(M, ta, tb, buf, cg0, cg1, acc, xt, lane);
+        case 1: return tile_group<T, BS, 1, V, GV>(M, ta, tb, buf, cg0, cg1, acc, xt, xo, lane);
+        case 2: return tile_group<T, BS, 2, V, GV>(M, ta, tb, buf, cg0, cg1, acc, xt, xo, lane);
+        default:
+            return tile_group<T, BS, 4, V, GV>(M, ta, tb, buf, cg0, cg1, acc, xt, xo, lane);
     }
 }
 
@@ -448,7 +520,7 @@ __device__ __forceinline__ void advance(Cursor &c, int64_t g, const int64_t *__r
 // ahead, in the queue order uorder (the costliest first; NULL: unit order);
 // the warp whose exit completes sched[1] == number of warps resets both for
 // the next launch.
-template <typename T, int BS>
+template <typename T, int BS, bool GV>
 __global__ void __launch_bounds__(kMsWarps * 32, 4)
     cb_mslice_kernel(const MatView single, const MatView *__restrict__ mats, int nmats,
                      const int64_t *__restrict__ toff, const int64_t *__restrict__ ustart,
@@ -463,7 +535,9 @@ __global__ void __launch_bounds__(kMsWarps * 32, 4)
     unsigned char *wbase = smem_raw + (size_t)wib * SL::bytes(cap);
     T *acc = reinterpret_cast<T *>(wbase);
     T *xt = reinterpret_cast<T *>(wbase + SL::acc_bytes);
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(wbase + SL::acc_bytes + SL::xt_bytes);
+    T *xo = reinterpret_cast<T *>(wbase + SL::acc_bytes + SL::xt_bytes);
+    uint64_t *mbar =
+        reinterpret_cast<uint64_t *>(wbase + SL::acc_bytes + SL::xt_bytes + SL::xo_bytes);
     unsigned char *const buf0 = wbase + SL::head;
     const uint64_t pol = policy_evict_first();
 
@@ -611,7 +685,7 @@ __global__ void __launch_bounds__(kMsWarps * 32, 4)
             const unsigned char *buf = buf0 + bi * cap;
             const int R = M.nrhs;
             if (R <= kRA) {  // one column group: runs across the block row's tiles
-                tile_any<T, BS>(M, ta, tb, buf, 0, R, acc, xt, lane);
+                tile_any<T, BS, GV>(M, ta, tb, buf, 0, R, acc, xt, xo, lane);
                 ++runlen;
                 if (!cont) {
                     ms_flush<T, BS>(M, ta, tb, g, runlen, 0, R, 1, acc, ustart, nunits, lane);
@@ -621,7 +695,7 @@ __global__ void __launch_bounds__(kMsWarps * 32, 4)
                 const int groups = (R + kRA - 1) / kRA;
                 for (int cg0 = 0; cg0 < R; cg0 += kRA) {
                     const int cg1 = min(R, cg0 + kRA);
-                    tile_any<T, BS>(M, ta, tb, buf, cg0, cg1, acc, xt, lane);
+                    tile_any<T, BS, GV>(M, ta, tb, buf, cg0, cg1, acc, xt, xo, lane);
                     ms_flush<T, BS>(M, ta, tb, g, 1, cg0, cg1 - cg0, groups, acc, ustart, nunits,
                                     lane);
                 }
@@ -662,37 +736,37 @@ __global__ void __launch_bounds__(kMsWarps * 32, 4)
     }
 }
 
-template <typename T, int BS>
+template <typename T, int BS, bool GV>
 cudaError_t ms_configure(uint32_t cap, size_t *smem) {
     *smem = (size_t)MsLayout<T, BS>::bytes(cap) * kMsWarps;
-    return dev_enable_smem(reinterpret_cast<const void *>(cb_mslice_kernel<T, BS>), *smem);
+    return dev_enable_smem(reinterpret_cast<const void *>(cb_mslice_kernel<T, BS, GV>), *smem);
 }
 
-template <typename T, int BS>
+template <typename T, int BS, bool GV = false>
 int64_t ms_warps_t(uint32_t cap) {
     size_t smem = 0;
-    if (ms_configure<T, BS>(cap, &smem) != cudaSuccess) return 0;
+    if (ms_configure<T, BS, GV>(cap, &smem) != cudaSuccess) return 0;
     const int resident = dev_resident_l1(
-        reinterpret_cast<const void *>(cb_mslice_kernel<T, BS>), kMsWarps * 32, smem);
+        reinterpret_cast<const void *>(cb_mslice_kernel<T, BS, GV>), kMsWarps * 32, smem);
     return (int64_t)resident * dev_sms() * kMsWarps;
 }
 
-template <typename T, int BS>
+template <typename T, int BS, bool GV>
 cudaError_t ms_launch_t(const MatView &single, const MatView *mats, int nmats,
                         const int64_t *toff, const int64_t *ustart, const int32_t *uorder,
                         int64_t nunits, int dynamic, uint32_t cap, uint32_t *sched,
                         uint32_t *err, cudaStream_t stream) {
     size_t smem = 0;
-    cudaError_t e = ms_configure<T, BS>(cap, &smem);
+    cudaError_t e = ms_configure<T, BS, GV>(cap, &smem);
     if (e != cudaSuccess) return e;
     if (cap % 16 || !sched || !err) return cudaErrorInvalidValue;
     if (nunits <= 0) return cudaSuccess;
     // dynamic: resident warps (or fewer); static: one warp per unit.  The
     // resident count also sets the kernel's carveout for this buffer size.
-    const int64_t resident_warps = ms_warps_t<T, BS>(cap);
+    const int64_t resident_warps = ms_warps_t<T, BS, GV>(cap);
     const int64_t w = dynamic ? std::min<int64_t>(resident_warps, nunits) : nunits;
     const int64_t ctas = (w + kMsWarps - 1) / kMsWarps;
-    cb_mslice_kernel<T, BS><<<(unsigned)ctas, kMsWarps * 32, smem, stream>>>(
+    cb_mslice_kernel<T, BS, GV><<<(unsigned)ctas, kMsWarps * 32, smem, stream>>>(
         single, mats, nmats, toff, ustart, uorder, nunits, dynamic, cap, sched, err,
         wait_polls());
     note_launch();
@@ -778,14 +852,27 @@ void ms_unit_starts(const uint32_t *tile8, int64_t ntiles, int64_t target, int64
 }
 
 cudaError_t launch_spmm(const DevLayout &d, const void *x, void *y, int nrhs, int64_t ldx,
-                        int64_t ldy, cudaStream_t stream) {
+                        int64_t ldy, cudaStream_t stream, void *gv, const void *xo,
+                        int64_t ldo) {
     if (d.ntiles == 0) return cudaSuccess;
     if (!d.ustart) return cudaErrorInvalidValue;
-    const MatView M = mat_view(d, x, y, nrhs, ldx, ldy);
+    MatView M = mat_view(d, x, y, nrhs, ldx, ldy);
+    if (gv) {
+        if (!xo || d.unit) return cudaErrorInvalidValue;
+        M.gv = gv;
+        M.xo = xo;
+        M.ldo = ldo;
+        // own-row vector loads need the same alignment as x's
+        const size_t vsz = d.f32 ? 4 : 8;
+        const int V = d.f32 ? 4 : 2;
+        if (reinterpret_cast<uintptr_t>(xo) % (V * vsz) != 0) M.xvec = 0;
+    }
     return by_type(d.bs, d.f32, [&](auto t, auto b) {
         using T = decltype(t);
-        return ms_launch_t<T, b()>(M, nullptr, 1, nullptr, d.ustart, nullptr, d.nunits, 0,
-                                   d.mcap, d.sched, d.err, stream);
+        return M.gv ? ms_launch_t<T, b(), true>(M, nullptr, 1, nullptr, d.ustart, nullptr,
+                                                d.nunits, 0, d.mcap, d.sched, d.err, stream)
+                    : ms_launch_t<T, b(), false>(M, nullptr, 1, nullptr, d.ustart, nullptr,
+                                                 d.nunits, 0, d.mcap, d.sched, d.err, stream);
     });
 }
 
@@ -794,8 +881,8 @@ cudaError_t launch_batch(int bs, int f32, const MatView *mats, int nmats, const 
                          uint32_t cap, uint32_t *sched, uint32_t *err, cudaStream_t stream) {
     return by_type(bs, f32, [&](auto t, auto b) {
         using T = decltype(t);
-        return ms_launch_t<T, b()>(MatView(), mats, nmats, toff, ustart, uorder, nunits, 1, cap,
-                                   sched, err, stream);
+        return ms_launch_t<T, b(), false>(MatView(), mats, nmats, toff, ustart, uorder, nunits,
+                                          1, cap, sched, err, stream);
     });
 }
 

@@ -225,6 +225,21 @@ cbspmv_status cbspmv_adjoint(cbspmv_plan *plan, const void *g, const void *x,
                              void *gx, void *gvals, int nrhs, int64_t ldg,
                              int64_t ldx, int64_t ldgx, void *stream);
 
+/* The backward pass of Y = A X in ONE kernel launch on the transposed
+ * layout (plans built with want_transpose and with stored values): gx = A^T g
+ * and, from the same gathered rows of g, the value gradient of every stored
+ * value of A^T, g[row] . x[col] summed over the right-hand sides.  gvals_t is
+ * a device array of cbspmv_grad_size_t values indexed by payload position
+ * (A^T's packed payload read as an array of values, so the gradient is
+ * written in packed block order, coalesced); positions that hold no value
+ * are left unchanged.  cbspmv_grad_positions_t gives, for each input nonzero
+ * (caller's order), its position there.  No counterpart in the reference. */
+cbspmv_status cbspmv_adjoint_fused(cbspmv_plan *plan, const void *g, const void *x,
+                                   void *gx, void *gvals_t, int nrhs, int64_t ldg,
+                                   int64_t ldx, int64_t ldgx, void *stream);
+int64_t cbspmv_grad_size_t(const cbspmv_plan *plan);
+cbspmv_status cbspmv_grad_positions_t(const cbspmv_plan *plan, int64_t *pos);
+
 /* Stored values: the plan's packed value slots, in device (tile) order.
  * Dense blocks store all bs*bs values, so there can be more slots than input
  * nonzeros; COO blocks merge duplicates (coo2block.h:249-255), so there can
