@@ -1,8 +1,10 @@
 """Process-group plumbing for multi-GPU runs (one process per GPU).
 
-CB-SpMV of one matrix needs no exchange, so N GPUs run N replicas; the group
-is used only to line the ranks up (barrier) and to time a step as the maximum
-over ranks.  Backend "nccl" on GPUs, "gloo" in CPU tests.
+The replica runs of bench.py (one copy of the workload per GPU) use the group
+only to line the ranks up (barrier) and to time a step as the maximum over
+ranks; one matrix sharded by block rows (cbspmv.shard.RowShard) also
+exchanges x (an all-gather) and, for the adjoint, partial A^T g (a
+reduce-scatter) through it.  Backend "nccl" on GPUs, "gloo" in CPU tests.
 """
 from __future__ import annotations
 

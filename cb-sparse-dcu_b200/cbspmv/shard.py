@@ -18,9 +18,14 @@ x_all holds range s at s * L.  Two ways to run a rank's rows:
   make a plan of nearly one-value blocks, and the second launch and the sum
   cost more than the exchange they hide.
 
-No reduction on y is needed: each rank's rows are its own.  Every part is an
-ordinary CB plan (the reference's coo2block_gather + cb_spmv per rank), so a
-rank runs the single-GPU kernels unchanged.
+No reduction on y is needed: each rank's rows are its own.  The adjoint
+g_x = A^T g is the other way round: every rank's rows touch every column, so
+each rank computes the partial A_rows^T g_rows in the padded layout (on the
+transposed CB layout of its plans) and one reduce-scatter (sum) hands each
+rank its own x range.  Every part is an ordinary CB plan (the reference's
+coo2block_gather + cb_spmv per rank), so a rank runs the single-GPU kernels
+unchanged.  staging="host" runs the exchange through host memory (for a
+process group whose backend has no device transport, e.g. gloo).
 """
 from __future__ import annotations
 
@@ -136,14 +141,69 @@ class RowShard:
         xp[: x_own.shape[0]] = x_own
         return xp
 
-    def spmv(self, x_own, y=None, group=None, x_all=None):
+    def _gather(self, x_own, group, staging):
+        """The padded ranges of every rank end to end (every rank takes part)
+        and the async work handle (device staging) or None."""
+        import torch
+        import torch.distributed as dist
+        piece = self.pad(x_own)
+        shape = (self.world * self.L,) + tuple(piece.shape[1:])
+        if staging == "host":
+            host = torch.empty(shape, dtype=piece.dtype)
+            dist.all_gather_into_tensor(host, piece.cpu(), group=group)
+            return host.to(x_own.device), None
+        x_all = torch.empty(shape, dtype=piece.dtype, device=piece.device)
+        work = dist.all_gather_into_tensor(x_all, piece, group=group, async_op=True)
+        return x_all, work
+
+    def spmv_t(self, g_own, gx=None, group=None, staging="device"):
+        """gx (this rank's x range, (c1 - c0,) or (c1 - c0, k)) = (A^T g) on
+        that range, from g_own (this rank's rows of g).  The plans need
+        want_transpose.  Partial A_rows^T g_own in the padded layout, then a
+        reduce-scatter over the ranks (every rank takes part); staging="host"
+        sums through host memory (all-reduce, then this rank's range)."""
+        import torch
+        k = 1 if g_own.dim() == 1 else g_own.shape[1]
+        if self.world == 1:
+            part = self.full.spmv_t(g_own)
+        else:
+            part = torch.zeros((self.world * self.L,) + tuple(g_own.shape[1:]),
+                               dtype=g_own.dtype, device=g_own.device)
+            if self.full is not None:
+                part += self.full.spmv_t(g_own)
+            else:
+                part[self.rank * self.L: self.rank * self.L + self.c1 - self.c0] += \
+                    self.own.spmv_t(g_own)
+                if self.halo is not None:
+                    part += self.halo.spmv_t(g_own)
+        width = self.c1 - self.c0
+        if gx is None:
+            gx = torch.empty((width,) if g_own.dim() == 1 else (width, k), dtype=g_own.dtype,
+                             device=g_own.device)
+        if self.world == 1:
+            gx.copy_(part[:width])
+            return gx
+        import torch.distributed as dist
+        if staging == "host":
+            host = part.cpu()
+            dist.all_reduce(host, group=group)
+            gx.copy_(host[self.rank * self.L: self.rank * self.L + width].to(gx.device))
+            return gx
+        mine = torch.empty((self.L,) + tuple(part.shape[1:]), dtype=part.dtype,
+                           device=part.device)
+        dist.reduce_scatter_tensor(mine, part, group=group)
+        gx.copy_(mine[:width])
+        return gx
+
+    def spmv(self, x_own, y=None, group=None, x_all=None, staging="device"):
         """y (this rank's rows) = A x on the current stream.  x_own: this
         rank's x range (CUDA tensor, (c1 - c0,) or (c1 - c0, k)).  Without
         `x_all`, every rank of `group` (a torch process group; None = the
         default one) takes part in the all-gather of the padded ranges --
         also a rank whose rows need no halo, so the ranks' collectives stay
         in step -- and it overlaps A_own x_own.  With `x_all` (the padded
-        ranges of every rank laid end to end) there is no collective."""
+        ranges of every rank laid end to end) there is no collective.
+        staging="host": the all-gather runs through host memory."""
         import torch
         k = 1 if x_own.dim() == 1 else x_own.shape[1]
         if y is None:
@@ -152,11 +212,7 @@ class RowShard:
                             device=x_own.device)
         work = None
         if x_all is None and self.world > 1:
-            import torch.distributed as dist
-            piece = self.pad(x_own)
-            x_all = torch.empty((self.world * self.L,) + tuple(piece.shape[1:]),
-                                dtype=piece.dtype, device=piece.device)
-            work = dist.all_gather_into_tensor(x_all, piece, group=group, async_op=True)
+            x_all, work = self._gather(x_own, group, staging)
         if self.full is not None:
             if work is not None:
                 work.wait()  # the current stream waits for the gathered x

@@ -99,9 +99,20 @@ def _rank(rank, world, port, out):
         else:
             y = cd.oracle_spmv(sh.full_coo, x_all.numpy())
         ok = ok and np.allclose(y, want[sh.r0:sh.r1], rtol=1e-12, atol=1e-12)
+    had_halo = sh.halo is not None
+    # the adjoint's exchange: partial A_rows^T g in the padded layout, summed
+    # over the ranks (all-reduce here; reduce-scatter on NCCL), own range kept
+    g = np.random.default_rng(3).uniform(-1, 1, coo.m)
+    gref = cd.oracle_spmm_ld(coo, g[None, :], transpose=True)[0][0]
+    sh = shard.RowShard(coo, world, rank)
+    part = cd.oracle_spmm_ld(sh.full_coo, g[None, sh.r0:sh.r1], transpose=True)[0][0]
+    tot = torch.from_numpy(part.copy())
+    dist.all_reduce(tot)
+    mine = tot.numpy()[rank * sh.L: rank * sh.L + sh.c1 - sh.c0]
+    ok = ok and np.allclose(mine, gref[sh.c0:sh.c1], rtol=1e-12, atol=1e-12)
     dist.barrier()
     dist.destroy_process_group()
-    out.put((rank, bool(ok), sh.halo is not None))
+    out.put((rank, bool(ok), had_halo))
 
 
 @pytest.mark.timeout(180)
@@ -147,3 +158,65 @@ def test_row_shards_on_gpu(cuda, name, coo, world, f32, nrhs, overlap):
     y = torch.cat(ys).cpu().numpy().reshape(coo.m, nrhs).T
     tol = 1e-5 if f32 else 1e-12
     assert np.all(np.abs(y - yref) <= tol * ab + 1e-300)
+
+
+def _gpu_rank(rank, world, port, out):
+    """One rank of a two-process run on one GPU: its own plans, its own
+    exchange (gloo, staged through host memory), forward and adjoint."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port),
+                      WORLD_SIZE=str(world), RANK=str(rank), LOCAL_RANK=str(rank))
+    import sys
+    import pathlib
+    repo = pathlib.Path(__file__).resolve().parent.parent
+    sys.path.insert(0, str(repo / "cb-sparse-dcu_b200"))
+    sys.path.insert(0, str(repo / "tests"))
+    import torch
+    import torch.distributed as dist
+    import cbdump as cd
+    from cbspmv import gen, shard
+    dist.init_process_group("gloo", timeout=__import__("datetime").timedelta(seconds=60))
+    dev = torch.device("cuda:0")
+    coo = gen.power_law(20000, kmax=4000, band=600, seed=6, mean=12)
+    X = gen.uniform_x(coo.n, 4, nrhs=3)  # (3, n)
+    G = gen.uniform_x(coo.m, 5, nrhs=3)
+    errs = []
+    for nrhs in (1, 3):
+        Xk, Gk = X[:nrhs], G[:nrhs]
+        yref, ab = cd.oracle_spmm_ld(coo, Xk)
+        gref, gab = cd.oracle_spmm_ld(coo, Gk, transpose=True)
+        for overlap in (False, True):
+            sh = shard.RowShard(coo, world, rank, overlap=overlap, want_transpose=1)
+            x_own = torch.from_numpy(np.ascontiguousarray(Xk[:, sh.c0:sh.c1].T)).to(dev)
+            g_own = torch.from_numpy(np.ascontiguousarray(Gk[:, sh.r0:sh.r1].T)).to(dev)
+            if nrhs == 1:
+                x_own, g_own = x_own[:, 0].contiguous(), g_own[:, 0].contiguous()
+            y = sh.spmv(x_own, staging="host").cpu().numpy().reshape(-1, nrhs).T
+            gx = sh.spmv_t(g_own, staging="host").cpu().numpy().reshape(-1, nrhs).T
+            e1 = np.max(np.abs(y - yref[:, sh.r0:sh.r1]) / (ab[:, sh.r0:sh.r1] + 1e-300))
+            e2 = np.max(np.abs(gx - gref[:, sh.c0:sh.c1]) / (gab[:, sh.c0:sh.c1] + 1e-300))
+            errs.append(float(max(e1, e2)))
+    dist.barrier()
+    dist.destroy_process_group()
+    out.put((rank, max(errs)))
+
+
+@pytest.mark.gpu
+@pytest.mark.timeout(300)
+def test_two_processes_share_one_gpu(cuda):
+    """Two ranks as two processes on the one GPU, each running RowShard's own
+    exchange (gloo, through host memory) around its own kernels -- forward
+    y = A x (all-gather of x) and adjoint A^T g (sum of the partials, each rank
+    keeping its range) -- checked against the oracle.  The kernels of the two
+    processes never wait on each other."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gpu_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=280) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert all(e <= 1e-12 for _, e in res), res
