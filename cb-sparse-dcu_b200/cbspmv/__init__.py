@@ -67,6 +67,15 @@ _INFO_FIELDS = [
 _CT = {"q": ctypes.c_int64, "i": ctypes.c_int32, "d": ctypes.c_double}
 
 
+class TuneReport(ctypes.Structure):
+    _fields_ = [("block_size", ctypes.c_int), ("tile_entries", ctypes.c_int),
+                ("kernel", ctypes.c_int), ("rhs_lanes", ctypes.c_int),
+                ("ms", ctypes.c_double), ("tried", ctypes.c_int)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class Info(ctypes.Structure):
     _fields_ = [(k, _CT[t]) for k, t in _INFO_FIELDS]
 
@@ -120,6 +129,10 @@ def _load():
         "cbspmv_launch_count": (_I64, []),
         "cbspmv_autotune": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _P]),
         "cbspmv_check": (ctypes.c_int, [_P, _P]),
+        "cbspmv_autotune_ex": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _P, _P]),
+        "cbspmv_set_rhs_lanes": (ctypes.c_int, [_P, ctypes.c_int]),
+        "cbspmv_tune": (ctypes.c_int, [ctypes.POINTER(CooDesc), ctypes.POINTER(Opts), ctypes.c_int,
+                                       _P, ctypes.POINTER(_P), _P]),
         "cbspmv_debug_wait_polls": (None, [_I64]),
         "cbspmv_batch_create": (ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.POINTER(_P)]),
         "cbspmv_batch_bind": (ctypes.c_int, [_P, _P, _P, _P]),
@@ -350,15 +363,21 @@ class Plan:
         _check(_lib.cbspmv_check(self._h, _stream(stream)))
 
     def autotune(self, nrhs: int = 1, stream=None):
-        """Times the kernels that can run this plan for nrhs right-hand sides
-        and keeps the fastest; returns (kernel, ms)."""
+        """Times the kernels (and, for nrhs > 1, the lanes per entry) that can
+        run this plan for nrhs right-hand sides and keeps the fastest;
+        returns (kernel, ms)."""
         self.upload(stream)
         k = ctypes.c_int()
+        rl = ctypes.c_int()
         ms = ctypes.c_double()
-        _check(_lib.cbspmv_autotune(self._h, int(nrhs), _stream(stream), ctypes.byref(k),
-                                    ctypes.byref(ms)))
+        _check(_lib.cbspmv_autotune_ex(self._h, int(nrhs), _stream(stream), ctypes.byref(k),
+                                       ctypes.byref(rl), ctypes.byref(ms)))
         self.opts.kernel = k.value
+        self.rhs_lanes = rl.value
         return k.value, ms.value
+
+    def set_rhs_lanes(self, lanes: int) -> None:
+        _check(_lib.cbspmv_set_rhs_lanes(self._h, int(lanes)))
 
     def spmv_t(self, g, gx=None, stream=None):
         """gx = A^T g (needs want_transpose=1)."""
@@ -523,6 +542,33 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def tune(coo, nrhs: int = 1, stream=None, **opts):
+    """cbspmv_tune: the fastest plan over block size (16, 32), tile size
+    (auto, 128 entries), kernel and lanes per entry, built from `coo`;
+    returns (plan, report dict)."""
+    row = np.ascontiguousarray(coo.row, np.int32)
+    col = np.ascontiguousarray(coo.col, np.int32)
+    val = np.ascontiguousarray(coo.val, np.float64)
+    desc = CooDesc(coo.m, coo.n, row.shape[0], _np_ptr(row), _np_ptr(col), _np_ptr(val))
+    o = default_opts(**opts)
+    h = ctypes.c_void_p()
+    rep = TuneReport()
+    _check(_lib.cbspmv_tune(ctypes.byref(desc), ctypes.byref(o), int(nrhs), _stream(stream),
+                            ctypes.byref(h), ctypes.byref(rep)))
+    plan = Plan.__new__(Plan)
+    plan._h = h
+    plan._row, plan._col, plan._val = row, col, val
+    plan.opts = Opts()
+    _check(_lib.cbspmv_plan_opts(h, ctypes.byref(plan.opts)))
+    plan.m, plan.n, plan.nnz = int(coo.m), int(coo.n), int(row.shape[0])
+    plan.f32 = plan.opts.value_type == F32
+    plan.bs = plan.opts.block_size
+    plan.has_transpose = bool(plan.opts.want_transpose)
+    plan._uploaded = True
+    plan.rhs_lanes = rep.rhs_lanes
+    return plan, rep.as_dict()
 
 
 def coo2block_gather(row, col, val, m, n, **opts) -> Plan:

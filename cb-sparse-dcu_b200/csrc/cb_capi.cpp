@@ -608,20 +608,34 @@ cbspmv_status cbspmv_check(cbspmv_plan *p, void *stream) {
 
 void cbspmv_debug_wait_polls(int64_t polls) { cb::set_wait_polls(polls); }
 
-cbspmv_status cbspmv_autotune(cbspmv_plan *p, int nrhs, void *stream, int *kernel, double *ms) {
+cbspmv_status cbspmv_set_rhs_lanes(cbspmv_plan *p, int lanes) {
+    if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
+    if (lanes != 0 && lanes != 1 && lanes != 2 && lanes != 4)
+        return fail(CBSPMV_ERR_INVALID, "rhs lanes must be 0 (automatic), 1, 2 or 4");
+    p->A.d.rl = lanes;
+    p->AT.d.rl = lanes;
+    return CBSPMV_OK;
+}
+
+cbspmv_status cbspmv_autotune_ex(cbspmv_plan *p, int nrhs, void *stream, int *kernel,
+                                 int *rhs_lanes, double *ms) {
     if (!p) return fail(CBSPMV_ERR_INVALID, "null plan");
     if (!p->uploaded) return fail(CBSPMV_ERR_STATE, "plan not uploaded");
     if (nrhs < 1) return fail(CBSPMV_ERR_INVALID, "nrhs must be >= 1");
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
     DevSide &s = p->A;
-    std::vector<int> cands;
+    // candidates: (kernel, lanes per entry of the several-right-hand-side
+    // kernel; 0 = its automatic choice)
+    std::vector<std::pair<int, int>> cands;
     if (nrhs == 1) {
         cb::DevLayout probe = s.d;
         probe.kernel = 1;
-        if (s.d.wpart && cb::stream_warps(probe) > 0) cands.push_back(1);
-        cands.push_back(2);
+        if (s.d.wpart && cb::stream_warps(probe) > 0) cands.push_back({1, 0});
+        cands.push_back({2, 0});
+        cands.push_back({3, 0});
+    } else {
+        for (int rl : {0, 1, 2, 4}) cands.push_back({3, rl});
     }
-    cands.push_back(3);
     const size_t vsz = vsize(p);
     void *x = nullptr, *y = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -631,20 +645,24 @@ cbspmv_status cbspmv_autotune(cbspmv_plan *p, int nrhs, void *stream, int *kerne
         if (e0) cudaEventDestroy(e0);
         if (e1) cudaEventDestroy(e1);
     };
-    cudaError_t e = cudaMalloc(&x, std::max<size_t>(1, (size_t)s.lay.n * nrhs * vsz));
+    const size_t xb = std::max<size_t>(1, (size_t)s.lay.n * nrhs * vsz);
+    cudaError_t e = cudaMalloc(&x, xb);
     if (e == cudaSuccess) e = cudaMalloc(&y, std::max<size_t>(1, (size_t)s.lay.m * nrhs * vsz));
-    if (e == cudaSuccess) e = cudaMemsetAsync(x, 0, (size_t)s.lay.n * nrhs * vsz, st);
+    // a non-zero x (every byte 0x3c: small positive finite values), so that
+    // no zero shortcut flatters a kernel
+    if (e == cudaSuccess) e = cudaMemsetAsync(x, 0x3c, xb, st);
     if (e == cudaSuccess) e = cudaEventCreate(&e0);
     if (e == cudaSuccess) e = cudaEventCreate(&e1);
     if (e != cudaSuccess) {
         cleanup();
         return cuda_fail(e, "autotune scratch");
     }
-    const int keep = s.d.kernel;
-    int best = -1;
+    const int keep = s.d.kernel, keep_rl = s.d.rl;
+    int best = -1, best_rl = 0;
     float best_ms = 0.f;
-    for (int k : cands) {
-        s.d.kernel = k;
+    for (const auto &c : cands) {
+        s.d.kernel = c.first;
+        s.d.rl = c.second;
         cbspmv_status rc = CBSPMV_OK;
         for (int i = 0; i < 3 && !rc; ++i) rc = run_side(p, s, x, y, nrhs, nrhs, nrhs, st);
         constexpr int reps = 10;
@@ -654,6 +672,7 @@ cbspmv_status cbspmv_autotune(cbspmv_plan *p, int nrhs, void *stream, int *kerne
         e = cudaEventSynchronize(e1);
         if (rc || e != cudaSuccess) {
             s.d.kernel = keep;
+            s.d.rl = keep_rl;
             cleanup();
             return rc ? rc : cuda_fail(e, "autotune timing");
         }
@@ -661,16 +680,74 @@ cbspmv_status cbspmv_autotune(cbspmv_plan *p, int nrhs, void *stream, int *kerne
         cudaEventElapsedTime(&t, e0, e1);
         t /= reps;
         if (best < 0 || t < best_ms) {
-            best = k;
+            best = c.first;
+            best_rl = c.second;
             best_ms = t;
         }
     }
     cleanup();
     s.d.kernel = best;
+    s.d.rl = best_rl;
     p->opts.kernel = best;
-    if (p->has_t) p->AT.d.kernel = best == 1 && !p->AT.d.wpart ? 2 : best;
+    if (p->has_t) {
+        p->AT.d.kernel = best == 1 && !p->AT.d.wpart ? 2 : best;
+        p->AT.d.rl = best_rl;
+    }
     if (kernel) *kernel = best;
+    if (rhs_lanes) *rhs_lanes = best_rl;
     if (ms) *ms = best_ms;
+    return CBSPMV_OK;
+}
+
+cbspmv_status cbspmv_autotune(cbspmv_plan *p, int nrhs, void *stream, int *kernel, double *ms) {
+    return cbspmv_autotune_ex(p, nrhs, stream, kernel, nullptr, ms);
+}
+
+cbspmv_status cbspmv_tune(const cbspmv_coo *coo, const cbspmv_opts *opts, int nrhs,
+                          void *stream, cbspmv_plan **out, cbspmv_tune_report *rep) {
+    if (!coo || !out) return fail(CBSPMV_ERR_INVALID, "null argument");
+    *out = nullptr;
+    cbspmv_opts base;
+    cbspmv_default_opts(&base);
+    if (opts) base = *opts;
+    cbspmv_plan *best = nullptr;
+    cbspmv_tune_report r;
+    std::memset(&r, 0, sizeof r);
+    r.ms = -1.0;
+    for (int bs : {16, 32}) {
+        for (int te : {0, 128}) {
+            cbspmv_opts o = base;
+            o.block_size = bs;
+            o.tile_entries = te;
+            o.kernel = 0;
+            cbspmv_plan *p = nullptr;
+            cbspmv_status rc = cbspmv_coo2block_gather(coo, &o, &p);
+            if (!rc) rc = cbspmv_upload(p, stream);
+            int k = 0, rl = 0;
+            double ms = 0;
+            if (!rc) rc = cbspmv_autotune_ex(p, nrhs, stream, &k, &rl, &ms);
+            if (rc) {
+                cbspmv_destroy(p);
+                if (best) cbspmv_destroy(best);
+                return rc;
+            }
+            ++r.tried;
+            if (r.ms < 0 || ms < r.ms) {
+                if (best) cbspmv_destroy(best);
+                best = p;
+                r.block_size = bs;
+                r.tile_entries = te;
+                r.kernel = k;
+                r.rhs_lanes = rl;
+                r.ms = ms;
+            } else {
+                cbspmv_destroy(p);
+            }
+        }
+    }
+    best->opts.tile_entries = r.tile_entries;
+    *out = best;
+    if (rep) *rep = r;
     return CBSPMV_OK;
 }
 

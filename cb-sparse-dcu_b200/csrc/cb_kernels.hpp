@@ -23,6 +23,8 @@ struct DevLayout {
     uint32_t *sched = nullptr;        // scheduler words (scratch, zeroed)
     uint32_t *err = nullptr;          // error word: set when a bounded wait gives up
     int has_x = 1;                    // the layout has CSR/DENSE blocks
+    int rl = 0;                       // lanes per entry of the several-right-hand-side
+                                      // kernel (0: its automatic choice)
     int64_t max_entries = 0;          // largest COO section of a tile
     int kernel = 0;                   // 0 auto, 1 streaming (TMA), 2 direct
     double coo_share = 1.0;
@@ -60,6 +62,7 @@ struct MatView {
     void *gv = nullptr;
     const void *xo = nullptr;   // row vectors of the layout's rows, stride ldo
     int64_t ldo = 0;
+    int rl = 0;                 // lanes per entry (0: chosen from nrhs)
 };
 
 // Shared-memory buffer bytes for tiles of at most max_tile_bytes.

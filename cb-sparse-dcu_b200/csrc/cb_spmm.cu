@@ -417,7 +417,7 @@ __device__ __forceinline__ void tile_any(const MatView &M, const uint4 ta, const
                                          const unsigned char *buf, int cg0, int cg1, T *acc,
                                          T *xt, T *xo, int lane) {
     constexpr int V = VecOf<T>::V;
-    switch (lanes_for<T>(M.nrhs)) {
+    switch (M.rl ? M.rl : lanes_for<T>(M.nrhs)) {
         case 1: return tile_group<T, BS, 1, V, GV>(M, ta, tb, buf, cg0, cg1, acc, xt, xo, lane);
         case 2: return tile_group<T, BS, 2, V, GV>(M, ta, tb, buf, cg0, cg1, acc, xt, xo, lane);
         default:
@@ -808,6 +808,7 @@ MatView mat_view(const DevLayout &d, const void *x, void *y, int nrhs, int64_t l
     M.gather = d.gather;
     M.pay16_end = d.pay16_end;
     M.unit = d.unit;
+    M.rl = d.rl;
     // vector x loads of V values (4 FP32 / 2 FP64): rows aligned to V values
     // and every V-group a lane reads inside its row (ldx a multiple of V, the
     // last group within ldx)

@@ -311,6 +311,34 @@ void cbspmv_debug_wait_polls(int64_t polls);
 cbspmv_status cbspmv_autotune(cbspmv_plan *plan, int nrhs, void *stream, int *kernel,
                               double *ms);
 
+/* cbspmv_autotune that also tries, for nrhs > 1, the lanes per stored entry
+ * of the several-right-hand-side kernel (1, 2 or 4 lanes side by side on one
+ * x row, or its automatic choice from nrhs), keeps the fastest and returns it
+ * in *rhs_lanes (0 = automatic; may be NULL).  Times on a non-zero x. */
+cbspmv_status cbspmv_autotune_ex(cbspmv_plan *plan, int nrhs, void *stream, int *kernel,
+                                 int *rhs_lanes, double *ms);
+
+/* Lanes per stored entry of the several-right-hand-side kernel for this plan
+ * (0: chosen from nrhs; 1, 2 or 4). */
+cbspmv_status cbspmv_set_rhs_lanes(cbspmv_plan *plan, int lanes);
+
+/* The tuner over the build's dimensions: builds the plan from the COO for
+ * block size 16 and 32 and tile sizes (stored entries per warp tile) auto and
+ * 128, uploads each, autotunes its kernel and lanes per entry
+ * (cbspmv_autotune_ex) for nrhs right-hand sides, keeps the fastest plan in
+ * *out and destroys the others.  The reference fixes these as compile-time
+ * macros (macros.h:38-97, its Makefile:4-7).  rep (may be NULL) receives the
+ * choice and its mean time.  Warps per CTA are fixed per kernel; the resident
+ * count follows from registers and the L1 reserve. */
+typedef struct cbspmv_tune_report {
+    int block_size, tile_entries, kernel, rhs_lanes;
+    double ms;
+    int tried;
+} cbspmv_tune_report;
+
+cbspmv_status cbspmv_tune(const cbspmv_coo *coo, const cbspmv_opts *opts, int nrhs,
+                          void *stream, cbspmv_plan **out, cbspmv_tune_report *rep);
+
 /* ---- batches (no counterpart in the reference) ------------------------ */
 
 /* Many uploaded plans -- same block size and value type, same device -- run

@@ -283,3 +283,32 @@ def test_unit_valued_plans(cuda, name, coo, bs, f32, kernel, nrhs):
     with pytest.raises(cbspmv.CBSpMVError) as e:
         plan.set_values(torch.ones(coo.nnz, dtype=dt, device=cuda))
     assert e.value.status == "UNSUPPORTED"
+
+
+@pytest.mark.parametrize("nrhs", [1, 6])
+@pytest.mark.parametrize("f32", [False, True])
+def test_tuner_over_block_size_tiles_kernels_lanes(cuda, nrhs, f32):
+    """cbspmv_tune tries block size 16/32 x tile size auto/128 x kernel (x
+    lanes per entry for several right-hand sides); the plan it keeps, and every
+    forced lane split, give the oracle's result."""
+    import torch
+    import cbspmv
+    import cbdump as cd
+    from cbspmv import gen
+    coo = gen.power_law(20000, kmax=3000, band=800, seed=12)
+    plan, rep = cbspmv.tune(coo, nrhs, value_type=int(f32))
+    assert rep["tried"] == 4 and rep["block_size"] in (16, 32) and rep["ms"] > 0
+    assert plan.bs == rep["block_size"]
+    dt = torch.float32 if f32 else torch.float64
+    X = gen.uniform_x(coo.n, 8, nrhs=max(nrhs, 2))[:nrhs]
+    if f32:
+        X = X.astype(np.float32).astype(np.float64)
+    yref, ab = cd.oracle_spmm_ld(coo, X)
+    xd = torch.from_numpy(np.ascontiguousarray(X.T)).to(cuda, dt)
+    if nrhs == 1:
+        xd = xd[:, 0].contiguous()
+    for lanes in ([rep["rhs_lanes"]] if nrhs == 1 else [rep["rhs_lanes"], 0, 1, 2, 4]):
+        plan.set_rhs_lanes(lanes)
+        y = plan.spmv(xd)
+        torch.cuda.synchronize()
+        _check(y.cpu().numpy().reshape(coo.m, nrhs).T, yref, ab, f32, f"tuned lanes={lanes}")
