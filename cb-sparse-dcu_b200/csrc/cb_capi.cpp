@@ -65,12 +65,15 @@ struct DevSide {
     int32_t *vsrc = nullptr;
     uint64_t *val_off = nullptr;
     int32_t *val_row = nullptr, *val_col = nullptr;
+    int32_t *pat[4] = {};  // pattern row_ptr, col_idx, output_ptr, output_rows
 
     void release() {
         void *ps[] = {tiles, blocks, payload, block_cols, partials, counters,
-                      wpart, dunit, ustart, vsrc_ptr, vsrc, val_off, val_row, val_col};
+                      wpart, dunit, ustart, vsrc_ptr, vsrc, val_off, val_row, val_col,
+                      pat[0], pat[1], pat[2], pat[3]};
         for (void *p : ps)
             if (p) cudaFree(p);
+        for (int32_t *&q : pat) q = nullptr;
         tiles = blocks = partials = nullptr;
         payload = nullptr;
         block_cols = counters = vsrc = val_row = val_col = nullptr;
@@ -270,6 +273,28 @@ cbspmv_status upload_partition(DevSide &s, int kernel, cudaStream_t st) {
     return CBSPMV_OK;
 }
 
+// The row patterns of a unit-valued plan (the reference's pattern_* arrays,
+// coo2block.h:566-602) for the pattern-reuse schedule; its automatic choice
+// follows the reference's rule: fewer patterns than half the rows
+// (cb-spmv-dcu.hpp:1431-1433).
+cbspmv_status upload_patterns(DevSide &s, const cb::HostCB &g, cudaStream_t st) {
+    s.d.small_direct = s.lay.unit && g.gather_flag && g.compact && g.nnz < 10000 &&
+                       g.o.row_owned;
+    if (!s.lay.unit || g.pat_row_ptr.size() < 2) return CBSPMV_OK;
+    CB_CUDA(upload_vec(g.pat_row_ptr, &s.pat[0], st), "upload patterns");
+    CB_CUDA(upload_vec(g.pat_col, &s.pat[1], st), "upload patterns");
+    CB_CUDA(upload_vec(g.pat_out_ptr, &s.pat[2], st), "upload patterns");
+    CB_CUDA(upload_vec(g.pat_out_rows, &s.pat[3], st), "upload patterns");
+    s.d.pat_ptr = s.pat[0];
+    s.d.pat_col = s.pat[1];
+    s.d.pat_out_ptr = s.pat[2];
+    s.d.pat_out_rows = s.pat[3];
+    s.d.npat = (int64_t)g.pat_row_ptr.size() - 1;
+    s.d.pat_cols = (int64_t)g.pat_col.size();
+    s.d.pat_auto = s.d.npat * 2 < g.m;
+    return CBSPMV_OK;
+}
+
 // Partial slots sized for nrhs right-hand sides.
 cbspmv_status ensure_partials(DevSide &s, int nrhs, size_t vsz) {
     if (s.lay.slots == 0 || s.partial_nrhs >= nrhs) return CBSPMV_OK;
@@ -367,8 +392,8 @@ cbspmv_status cbspmv_coo2block_gather(const cbspmv_coo *coo,
     if (opts) o = *opts;
     if (o.value_type != CBSPMV_F64 && o.value_type != CBSPMV_F32)
         return fail(CBSPMV_ERR_INVALID, "value_type must be CBSPMV_F64 or CBSPMV_F32");
-    if (o.kernel < 0 || o.kernel > 3)
-        return fail(CBSPMV_ERR_INVALID, "kernel must be 0 (auto), 1, 2 or 3");
+    if (o.kernel < 0 || o.kernel > 4)
+        return fail(CBSPMV_ERR_INVALID, "kernel must be 0 (auto), 1, 2, 3 or 4");
     cbspmv_plan *p = new (std::nothrow) cbspmv_plan;
     if (!p) return fail(CBSPMV_ERR_ALLOC, "out of host memory");
     p->opts = o;
@@ -524,7 +549,7 @@ cbspmv_status cbspmv_plan_load(const char *path, cbspmv_plan **out) {
     p->has_t = img.has_t != 0;
     if ((o.block_size != 16 && o.block_size != 32) ||
         (o.value_type != CBSPMV_F64 && o.value_type != CBSPMV_F32) || o.kernel < 0 ||
-        o.kernel > 3 || p->A.lay.bs != o.block_size) {
+        o.kernel > 4 || p->A.lay.bs != o.block_size) {
         delete p;
         return fail(CBSPMV_ERR_INVALID, std::string(path) + " holds inconsistent options");
     }
@@ -544,6 +569,7 @@ cbspmv_status cbspmv_upload(cbspmv_plan *p, void *stream) {
     }
     cbspmv_status rc = upload_side(p->A, st);
     if (!rc) rc = upload_partition(p->A, p->opts.kernel, st);
+    if (!rc) rc = upload_patterns(p->A, p->host, st);
     if (!rc && p->has_t) rc = upload_side(p->AT, st);
     if (!rc && p->has_t) rc = upload_partition(p->AT, p->opts.kernel, st);
     p->A.d.err = p->derr;
@@ -633,6 +659,7 @@ cbspmv_status cbspmv_autotune_ex(cbspmv_plan *p, int nrhs, void *stream, int *ke
         if (s.d.wpart && cb::stream_warps(probe) > 0) cands.push_back({1, 0});
         cands.push_back({2, 0});
         cands.push_back({3, 0});
+        if (s.d.npat) cands.push_back({4, 0});
     } else {
         for (int rl : {0, 1, 2, 4}) cands.push_back({3, rl});
     }

@@ -553,6 +553,42 @@ __global__ void __launch_bounds__(kStreamWarps * 32, 8)
     __syncwarp();
 }
 
+// Pattern reuse: LP lanes per column pattern (a power of two), G = 32 / LP
+// patterns per warp at a time, grid-strided.  The lanes of a pattern sum x
+// over its columns (two loads in flight per lane), meet by shuffles, and
+// write the sum to every output row of the pattern.  Unit values only: the
+// reference's pattern schedules (cb-spmv-dcu.hpp:626-674) read no values.
+template <typename T, int LP>
+__global__ void __launch_bounds__(256)
+    cb_pattern_kernel(const int32_t *__restrict__ ptr, const int32_t *__restrict__ col,
+                      const int32_t *__restrict__ optr, const int32_t *__restrict__ orow,
+                      int64_t npat, const T *__restrict__ x, T *__restrict__ y) {
+    constexpr int G = 32 / LP;
+    const int lane = threadIdx.x & 31, sub = lane % LP, g = lane / LP;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = warp * G; base < npat; base += warps * G) {  // warp-uniform
+        const int64_t p = base + g;
+        T s0 = T(0), s1 = T(0);
+        if (p < npat) {
+            const int c1 = __ldg(&ptr[p + 1]);
+            int i = __ldg(&ptr[p]) + sub;
+            for (; i + LP < c1; i += 2 * LP) {
+                s0 += ldg(&x[__ldg(&col[i])]);
+                s1 += ldg(&x[__ldg(&col[i + LP])]);
+            }
+            if (i < c1) s0 += ldg(&x[__ldg(&col[i])]);
+        }
+        T s = s0 + s1;
+#pragma unroll
+        for (int o = LP / 2; o > 0; o >>= 1) s += __shfl_xor_sync(kFull, s, o);
+        if (p < npat) {
+            const int o1 = __ldg(&optr[p + 1]);
+            for (int i = __ldg(&optr[p]) + sub; i < o1; i += LP) y[__ldg(&orow[i])] = s;
+        }
+    }
+}
+
 template <typename T>
 __global__ void cb_set_values_kernel(int64_t nvals, const int64_t *__restrict__ ptr,
                                      const int32_t *__restrict__ src,
@@ -716,16 +752,49 @@ cudaError_t launch_stream(const DevLayout &d, const void *x, void *y, cudaStream
 bool use_stream(const DevLayout &d) {
     if (d.max_entries > 32 * kStreamSteps) return false;
     if (d.kernel == 1) return true;
-    if (d.kernel == 2 || d.kernel == 3) return false;
+    if (d.kernel == 2 || d.kernel == 3 || d.kernel == 4) return false;
+    if (d.small_direct) return false;
     return d.coo_share >= 0.5;
+}
+
+template <typename T, int LP>
+cudaError_t launch_pattern_t(const DevLayout &d, const void *x, void *y, cudaStream_t st) {
+    const void *fn = reinterpret_cast<const void *>(cb_pattern_kernel<T, LP>);
+    const int64_t want = (d.npat * LP + 255) / 256;
+    const int64_t grid = std::max<int64_t>(
+        1, std::min<int64_t>(want, (int64_t)dev_sms() * dev_resident(fn, 256, 0)));
+    cb_pattern_kernel<T, LP><<<(unsigned)grid, 256, 0, st>>>(
+        d.pat_ptr, d.pat_col, d.pat_out_ptr, d.pat_out_rows, d.npat,
+        static_cast<const T *>(x), static_cast<T *>(y));
+    note_launch();
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_pattern_v(const DevLayout &d, const void *x, void *y, cudaStream_t st) {
+    const double avg = d.npat ? (double)d.pat_cols / (double)d.npat : 0.0;
+    if (avg <= 6) return launch_pattern_t<T, 4>(d, x, y, st);
+    if (avg <= 12) return launch_pattern_t<T, 8>(d, x, y, st);
+    if (avg <= 24) return launch_pattern_t<T, 16>(d, x, y, st);
+    return launch_pattern_t<T, 32>(d, x, y, st);
+}
+
+// the pattern schedule: chosen (kernel 4) or automatic by the reference's
+// rule, patterns fewer than half the rows (cb-spmv-dcu.hpp:1431-1433)
+bool use_pattern(const DevLayout &d) {
+    if (!d.npat || !d.unit) return false;
+    return d.kernel == 4 || (d.kernel == 0 && d.pat_auto);
 }
 
 template <typename T, int BS>
 cudaError_t launch_tiles(const DevLayout &d, const void *x, void *y, int nrhs,
                          int64_t ldx, int64_t ldy, cudaStream_t stream) {
+    if (nrhs == 1 && ldx == 1 && ldy == 1 && use_pattern(d))
+        return launch_pattern_v<T>(d, x, y, stream);
     if (nrhs == 1 && ldx == 1 && ldy == 1 && use_stream(d))
         return launch_stream<T, BS>(d, x, y, stream);
-    if (nrhs > 1 || d.kernel == 3) return launch_spmm(d, x, y, nrhs, ldx, ldy, stream);
+    if (nrhs > 1 || d.kernel == 3 || d.kernel == 4)
+        return launch_spmm(d, x, y, nrhs, ldx, ldy, stream);
     switch (chunk_choice()) {
         case 4: return launch_chunk<T, BS, 4>(d, x, y, nrhs, ldx, ldy, stream);
         case 6: return launch_chunk<T, BS, 6>(d, x, y, nrhs, ldx, ldy, stream);
@@ -853,6 +922,12 @@ int64_t stream_warps_t(const DevLayout &d) {
 int64_t stream_warps(const DevLayout &d) {
     if (d.bs == 16) return d.f32 ? stream_warps_t<float, 16>(d) : stream_warps_t<double, 16>(d);
     return d.f32 ? stream_warps_t<float, 32>(d) : stream_warps_t<double, 32>(d);
+}
+
+cudaError_t launch_pattern(const DevLayout &d, const void *x, void *y, cudaStream_t stream) {
+    if (!d.npat) return cudaErrorInvalidValue;
+    return d.f32 ? launch_pattern_v<float>(d, x, y, stream)
+                 : launch_pattern_v<double>(d, x, y, stream);
 }
 
 cudaError_t launch_spmv(const DevLayout &d, const void *x, void *y, int nrhs,

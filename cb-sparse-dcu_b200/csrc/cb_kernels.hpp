@@ -25,6 +25,16 @@ struct DevLayout {
     int has_x = 1;                    // the layout has CSR/DENSE blocks
     int rl = 0;                       // lanes per entry of the several-right-hand-side
                                       // kernel (0: its automatic choice)
+    // pattern reuse (unit-valued plans, one right-hand side): the rows that
+    // share one column pattern share one sum (kernel 4)
+    const int32_t *pat_ptr = nullptr, *pat_col = nullptr;
+    const int32_t *pat_out_ptr = nullptr, *pat_out_rows = nullptr;
+    int64_t npat = 0, pat_cols = 0;
+    int pat_auto = 0;                 // the automatic choice takes it
+    // small unit-valued gathered matrices: the automatic choice is the
+    // direct kernel, whose block rows then fit one unit each and store y
+    // directly (the reference's EXEC_SMALL_DIRECT, cb-spmv-dcu.hpp:1437-1439)
+    int small_direct = 0;
     int64_t max_entries = 0;          // largest COO section of a tile
     int kernel = 0;                   // 0 auto, 1 streaming (TMA), 2 direct
     double coo_share = 1.0;
@@ -111,6 +121,11 @@ std::vector<uint32_t> direct_units(const uint32_t *tile8, int64_t ntiles);
 // Warps of a streaming-kernel launch for this layout on the current device,
 // or 0 when the direct kernel is the one that runs.
 int64_t stream_warps(const DevLayout &d);
+
+// The pattern-reuse schedule (unit values, one right-hand side): per column
+// pattern, lanes sum x over its columns and write the sum to every row of the
+// pattern (the reference's EXEC_PATTERN_REUSE_*, cb-spmv-dcu.hpp:626-674).
+cudaError_t launch_pattern(const DevLayout &d, const void *x, void *y, cudaStream_t stream);
 
 // y = A x; x: n rows, y: m rows, row-major with leading dims for nrhs > 1.
 cudaError_t launch_spmv(const DevLayout &d, const void *x, void *y, int nrhs,

@@ -63,7 +63,11 @@ typedef struct cbspmv_opts {
                              (TMA-staged tiles, for COO-dominant matrices),
                              2 direct (high occupancy, for CSR/dense-heavy
                              ones), 3 staged (the several-right-hand-side
-                             kernel, one vector); see cbspmv_autotune      */
+                             kernel, one vector), 4 pattern reuse (unit-
+                             valued plans: one sum per row pattern, the
+                             reference's EXEC_PATTERN_REUSE; automatic when
+                             patterns are fewer than half the rows, as in
+                             cb-spmv-dcu.hpp:1431-1433); see cbspmv_autotune */
     int keep_values;      /* 0 (default): when every stored value is 1, store
                              no values and DENSE blocks as bitmasks, as the
                              reference does (UNIT_VALUES,

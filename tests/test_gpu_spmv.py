@@ -312,3 +312,68 @@ def test_tuner_over_block_size_tiles_kernels_lanes(cuda, nrhs, f32):
         y = plan.spmv(xd)
         torch.cuda.synchronize()
         _check(y.cpu().numpy().reshape(coo.m, nrhs).T, yref, ab, f32, f"tuned lanes={lanes}")
+
+
+def _patterned(m=3000, n=2500, npat=70, seed=21):
+    """Unit-valued rows drawn from a few column patterns (the structure the
+    reference's pattern schedule exploits): each row takes one of npat random
+    column sets, some of them empty."""
+    from cbspmv import gen
+    rng = np.random.default_rng(seed)
+    pats = [np.sort(rng.choice(n, size=int(rng.integers(0, 90)), replace=False))
+            for _ in range(npat)]
+    which = rng.integers(0, npat, size=m)
+    rows = np.concatenate([np.full(len(pats[w]), r) for r, w in enumerate(which)])
+    cols = np.concatenate([pats[w] for w in which])
+    return gen.Coo(m, n, rows.astype(np.int32), cols.astype(np.int32), np.ones(rows.size))
+
+
+@pytest.mark.parametrize("f32", [False, True])
+@pytest.mark.parametrize("bs", [16, 32])
+def test_pattern_reuse_schedule(cuda, f32, bs):
+    """Unit values with few row patterns: the automatic choice is the
+    pattern-reuse schedule (one sum per pattern, written to all its rows); it,
+    and every other kernel on the same plan, give the oracle's y."""
+    import torch
+    import cbspmv
+    import cbdump as cd
+    from cbspmv import gen
+    coo = _patterned()
+    plan = cbspmv.Plan(coo, value_type=int(f32), block_size=bs)
+    info = plan.info()
+    assert info["unit_values"] and 0 < info["patterns"] * 2 < coo.m
+    x = gen.uniform_x(coo.n, 3)
+    if f32:
+        x = x.astype(np.float32).astype(np.float64)
+    yref, ab = cd.oracle_spmm_ld(coo, x[None, :])
+    dt = torch.float32 if f32 else torch.float64
+    xd = torch.from_numpy(x).to(cuda, dt)
+    for kernel in (0, 4, 1, 2, 3):
+        p = plan if kernel == 0 else cbspmv.Plan(coo, value_type=int(f32), block_size=bs,
+                                                 kernel=kernel)
+        y = torch.full((coo.m,), float("nan"), dtype=dt, device=cuda)
+        for _ in range(2):
+            p.spmv(xd, y)
+        torch.cuda.synchronize()
+        _check(y.cpu().numpy()[None, :], yref, ab, f32, f"kernel {kernel}")
+    k, _ = plan.autotune(1)
+    assert k in (1, 2, 3, 4)
+
+
+def test_small_direct_schedule(cuda):
+    """Small unit-valued gathered matrices (the reference's small-direct
+    case): the automatic choice is the direct kernel, exact."""
+    import torch
+    import cbspmv
+    import cbdump as cd
+    from cbspmv import gen
+    rng = np.random.default_rng(5)
+    coo = gen.random_small(rng, 900, 700, 6000, unit=True)
+    plan = cbspmv.Plan(coo)
+    ex = plan.export()
+    assert ex["gather_flag"] and ex["compact_coo_indices"] and coo.nnz < 10000
+    x = gen.uniform_x(coo.n, 4)
+    yref, ab = cd.oracle_spmm_ld(coo, x[None, :])
+    y = plan.spmv(torch.from_numpy(x).to(cuda))
+    torch.cuda.synchronize()
+    _check(y.cpu().numpy()[None, :], yref, ab, False, "small direct")
