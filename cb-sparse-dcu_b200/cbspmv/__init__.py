@@ -442,7 +442,7 @@ class Plan:
             gx = torch.empty((self.n,) if g.dim() == 1 else (self.n, k),
                              dtype=g.dtype, device=g.device)
         if gvals_t is None:
-            gvals_t = torch.empty(int(_lib.cbspmv_grad_size_t(self._h)), dtype=g.dtype,
+            gvals_t = torch.zeros(int(_lib.cbspmv_grad_size_t(self._h)), dtype=g.dtype,
                                   device=g.device)
         self._check_dev(gx, gvals_t)
         _check(_lib.cbspmv_adjoint_fused(self._h, _dptr(g), _dptr(x), _dptr(gx),
