@@ -293,7 +293,7 @@ def diff_config(dev, peak, flush, out):
     GX = torch.empty(coo.n, k, device=dev)
     GV = torch.empty(plan.num_values(), device=dev)
     GX2 = torch.empty(coo.n, k, device=dev)
-    GP = torch.empty(cbspmv.lib().cbspmv_grad_size_t(plan._h), device=dev)
+    GP = torch.zeros(cbspmv.lib().cbspmv_grad_size_t(plan._h), device=dev)
     info = plan.info()
     xy = 4 * (coo.n + coo.m) * (k - 1)
     fwd_bytes = info["algorithmic_bytes"] + xy
