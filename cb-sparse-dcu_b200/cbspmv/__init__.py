@@ -63,7 +63,7 @@ _INFO_FIELDS = [
     ("dense_blocks", "q"), ("uniform_blocks", "q"), ("segments", "q"),
     ("patterns", "q"), ("stored_values", "q"), ("tiles", "q"),
     ("split_rows", "q"), ("device_bytes", "q"), ("algorithmic_bytes", "q"),
-    ("scratch_bytes", "q")]
+    ("scratch_bytes", "q"), ("rowseg_bytes", "q")]
 _CT = {"q": ctypes.c_int64, "i": ctypes.c_int32, "d": ctypes.c_double}
 
 

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
 #include <future>
 #include <new>
@@ -17,6 +18,7 @@
 #include "cb_kernels.hpp"
 #include "cb_layout.hpp"
 #include "cb_planfile.hpp"
+#include "cb_rowseg.hpp"
 #include "cbspmv.h"
 
 namespace {
@@ -66,6 +68,10 @@ struct DevSide {
     uint64_t *val_off = nullptr;
     int32_t *val_row = nullptr, *val_col = nullptr;
     int32_t *pat[4] = {};  // pattern row_ptr, col_idx, output_ptr, output_rows
+    // row-segment stream (kernel 5): chunks, segment meta, spans, counters,
+    // partial slots, rowmap, empty rows, value positions
+    void *rs[8] = {};
+    int64_t rs_bytes = 0;
 
     void release() {
         void *ps[] = {tiles, blocks, payload, block_cols, partials, counters,
@@ -73,6 +79,11 @@ struct DevSide {
                       pat[0], pat[1], pat[2], pat[3]};
         for (void *p : ps)
             if (p) cudaFree(p);
+        for (void *&q : rs) {
+            if (q) cudaFree(q);
+            q = nullptr;
+        }
+        rs_bytes = 0;
         for (int32_t *&q : pat) q = nullptr;
         tiles = blocks = partials = nullptr;
         payload = nullptr;
@@ -273,6 +284,46 @@ cbspmv_status upload_partition(DevSide &s, int kernel, cudaStream_t st) {
     return CBSPMV_OK;
 }
 
+// The row-segment stream (kernel 5, and the automatic choice for one
+// right-hand side) of a layout whose stored entries are all in COO blocks,
+// segmented for this device's resident warps.
+cbspmv_status upload_rowseg(DevSide &s, int kernel, cudaStream_t st) {
+    if ((kernel != 0 && kernel != 5) || !cb::rowseg_applies(s.lay)) return CBSPMV_OK;
+    const int64_t warps = cb::rowseg_warps(s.lay.f32);
+    if (warps <= 0) return CBSPMV_OK;
+    cb::RowSegHost R;
+    const std::string msg = cb::build_rowseg(s.lay, warps, R);
+    if (!msg.empty()) return fail(CBSPMV_ERR_UNSUPPORTED, msg);
+    const size_t vsz = s.lay.f32 ? 4 : 8;
+    const std::vector<int32_t> zeros(std::max<size_t>(1, R.spans.size() / 4), 0);
+    CB_CUDA(upload_vec(R.chunks, (uint8_t **)&s.rs[0], st), "upload row segments");
+    CB_CUDA(upload_vec(R.meta, (int32_t **)&s.rs[1], st), "upload row segments");
+    if (!R.spans.empty())
+        CB_CUDA(upload_vec(R.spans, (int32_t **)&s.rs[2], st), "upload row segments");
+    CB_CUDA(upload_vec(zeros, (int32_t **)&s.rs[3], st), "upload row segments");
+    CB_CUDA(cudaMalloc(&s.rs[4], 2 * (size_t)R.nseg * vsz), "allocate row-segment slots");
+    CB_CUDA(upload_vec(R.rowmap, (int32_t **)&s.rs[5], st), "upload row segments");
+    CB_CUDA(upload_vec(R.empty, (int32_t **)&s.rs[6], st), "upload row segments");
+    CB_CUDA(upload_vec(R.vpos, (int32_t **)&s.rs[7], st), "upload row segments");
+    cb::RowSegDev &d = s.d.rs;
+    d.chunks = static_cast<const uint8_t *>(s.rs[0]);
+    d.nch = R.nch;
+    d.M = R.M;
+    d.nseg = R.nseg;
+    d.nord = R.nord;
+    d.meta = static_cast<const int4 *>(s.rs[1]);
+    d.spans = static_cast<const int4 *>(s.rs[2]);
+    d.counters = static_cast<int32_t *>(s.rs[3]);
+    d.part = s.rs[4];
+    d.rowmap = R.rowmap.empty() ? nullptr : static_cast<const int32_t *>(s.rs[5]);
+    d.empty = static_cast<const int32_t *>(s.rs[6]);
+    d.nempty = (int32_t)R.empty.size();
+    d.vpos = static_cast<const int32_t *>(s.rs[7]);
+    s.rs_bytes = (int64_t)(R.chunks.size() + 4 * (R.meta.size() + R.spans.size() +
+                                                  R.rowmap.size() + R.empty.size()));
+    return CBSPMV_OK;
+}
+
 // The row patterns of a unit-valued plan (the reference's pattern_* arrays,
 // coo2block.h:566-602) for the pattern-reuse schedule; its automatic choice
 // follows the reference's rule: fewer patterns than half the rows
@@ -392,8 +443,8 @@ cbspmv_status cbspmv_coo2block_gather(const cbspmv_coo *coo,
     if (opts) o = *opts;
     if (o.value_type != CBSPMV_F64 && o.value_type != CBSPMV_F32)
         return fail(CBSPMV_ERR_INVALID, "value_type must be CBSPMV_F64 or CBSPMV_F32");
-    if (o.kernel < 0 || o.kernel > 4)
-        return fail(CBSPMV_ERR_INVALID, "kernel must be 0 (auto), 1, 2, 3 or 4");
+    if (o.kernel < 0 || o.kernel > 5)
+        return fail(CBSPMV_ERR_INVALID, "kernel must be 0 (auto), 1, 2, 3, 4 or 5");
     cbspmv_plan *p = new (std::nothrow) cbspmv_plan;
     if (!p) return fail(CBSPMV_ERR_ALLOC, "out of host memory");
     p->opts = o;
@@ -549,7 +600,7 @@ cbspmv_status cbspmv_plan_load(const char *path, cbspmv_plan **out) {
     p->has_t = img.has_t != 0;
     if ((o.block_size != 16 && o.block_size != 32) ||
         (o.value_type != CBSPMV_F64 && o.value_type != CBSPMV_F32) || o.kernel < 0 ||
-        o.kernel > 4 || p->A.lay.bs != o.block_size) {
+        o.kernel > 5 || p->A.lay.bs != o.block_size) {
         delete p;
         return fail(CBSPMV_ERR_INVALID, std::string(path) + " holds inconsistent options");
     }
@@ -570,8 +621,10 @@ cbspmv_status cbspmv_upload(cbspmv_plan *p, void *stream) {
     cbspmv_status rc = upload_side(p->A, st);
     if (!rc) rc = upload_partition(p->A, p->opts.kernel, st);
     if (!rc) rc = upload_patterns(p->A, p->host, st);
+    if (!rc) rc = upload_rowseg(p->A, p->opts.kernel, st);
     if (!rc && p->has_t) rc = upload_side(p->AT, st);
     if (!rc && p->has_t) rc = upload_partition(p->AT, p->opts.kernel, st);
+    if (!rc && p->has_t) rc = upload_rowseg(p->AT, p->opts.kernel, st);
     p->A.d.err = p->derr;
     p->AT.d.err = p->derr + 1;
     if (rc) {
@@ -660,6 +713,7 @@ cbspmv_status cbspmv_autotune_ex(cbspmv_plan *p, int nrhs, void *stream, int *ke
         cands.push_back({2, 0});
         cands.push_back({3, 0});
         if (s.d.npat) cands.push_back({4, 0});
+        if (s.d.rs.chunks) cands.push_back({5, 0});
     } else {
         for (int rl : {0, 1, 2, 4}) cands.push_back({3, rl});
     }
@@ -1024,6 +1078,8 @@ cbspmv_status cbspmv_set_values(cbspmv_plan *p, const void *input_values,
         CB_CUDA(cb::launch_set_values(s->lay.f32, s->lay.nvals, s->vsrc_ptr, s->vsrc,
                                       s->val_off, input_values, s->payload, st),
                 "set_values launch");
+        CB_CUDA(cb::launch_rowseg_values(s->d, s->lay.nvals, s->val_off, st),
+                "set_values launch");
     }
     return CBSPMV_OK;
 }
@@ -1082,8 +1138,10 @@ cbspmv_status cbspmv_info_get(const cbspmv_plan *p, cbspmv_info *info) {
     I.split_rows = p->A.lay.split_rows;
     I.device_bytes = (int64_t)(p->A.lay.tiles.size() * sizeof(cb::TileDesc) +
                                p->A.lay.blocks.size() * sizeof(cb::BlockDesc) +
-                               p->A.lay.payload.size() + p->A.lay.block_cols.size() * 4);
+                               p->A.lay.payload.size() + p->A.lay.block_cols.size() * 4) +
+                     p->A.rs_bytes;
     I.algorithmic_bytes = p->A.lay.alg_bytes;
+    I.rowseg_bytes = p->A.rs_bytes;
     I.scratch_bytes = (int64_t)(p->A.lay.slots * p->A.lay.bs * vsize(p) +
                                 (p->A.lay.gb_m + 4) * 4);
     *info = I;
@@ -1119,6 +1177,23 @@ int64_t export_device(const cb::DeviceLayout &L, const std::string &k, void *out
             }
         return L.nvals;
     }
+    // the row-segment stream built for W resident warps: "rs_<field>:<W>"
+    if (k.rfind("rs_", 0) == 0) {
+        const size_t colon = k.find(':');
+        if (colon == std::string::npos) return -1;
+        const int64_t warps = std::atoll(k.c_str() + colon + 1);
+        const std::string f = k.substr(3, colon - 3);
+        cb::RowSegHost R;
+        if (warps <= 0 || !cb::build_rowseg(L, warps, R).empty()) return -1;
+        const int32_t sizes[4] = {R.nch, R.M, R.nseg, R.nord};
+        if (f == "sizes") return raw(sizes, sizeof sizes, 4);
+        if (f == "chunks") return raw(R.chunks.data(), R.chunks.size(), 1);
+        if (f == "meta") return raw(R.meta.data(), R.meta.size() * 4, 4);
+        if (f == "spans") return raw(R.spans.data(), R.spans.size() * 4, 4);
+        if (f == "rowmap") return raw(R.rowmap.data(), R.rowmap.size() * 4, 4);
+        if (f == "empty") return raw(R.empty.data(), R.empty.size() * 4, 4);
+        if (f == "vpos") return raw(R.vpos.data(), R.vpos.size() * 4, 4);
+    }
     return -1;
 }
 }  // namespace
@@ -1136,7 +1211,8 @@ int64_t cbspmv_export(const cbspmv_plan *p, const char *name, void *out) {
     if (!p || !name) return -1;
     const std::string k(name);
     if (!exportable(p, k)) return -1;
-    if (k.rfind("dev_", 0) == 0) return export_device(p->A.lay, k, out);
+    if (k.rfind("dev_", 0) == 0 || k.rfind("rs_", 0) == 0)
+        return export_device(p->A.lay, k, out);
     return cb::export_array(p->host, k, out);
 }
 
@@ -1144,7 +1220,8 @@ int64_t cbspmv_export_t(const cbspmv_plan *p, const char *name, void *out) {
     if (!p || !name || !p->has_t) return -1;
     const std::string k(name);
     if (!exportable(p, k)) return -1;
-    if (k.rfind("dev_", 0) == 0) return export_device(p->AT.lay, k, out);
+    if (k.rfind("dev_", 0) == 0 || k.rfind("rs_", 0) == 0)
+        return export_device(p->AT.lay, k, out);
     return cb::export_array(p->host_t, k, out);
 }
 

@@ -752,7 +752,7 @@ cudaError_t launch_stream(const DevLayout &d, const void *x, void *y, cudaStream
 bool use_stream(const DevLayout &d) {
     if (d.max_entries > 32 * kStreamSteps) return false;
     if (d.kernel == 1) return true;
-    if (d.kernel == 2 || d.kernel == 3 || d.kernel == 4) return false;
+    if (d.kernel >= 2) return false;
     if (d.small_direct) return false;
     return d.coo_share >= 0.5;
 }
@@ -791,6 +791,8 @@ cudaError_t launch_tiles(const DevLayout &d, const void *x, void *y, int nrhs,
                          int64_t ldx, int64_t ldy, cudaStream_t stream) {
     if (nrhs == 1 && ldx == 1 && ldy == 1 && use_pattern(d))
         return launch_pattern_v<T>(d, x, y, stream);
+    if (nrhs == 1 && ldx == 1 && ldy == 1 && d.rs.chunks && (d.kernel == 0 || d.kernel == 5))
+        return launch_rowseg(d, x, y, stream);
     if (nrhs == 1 && ldx == 1 && ldy == 1 && use_stream(d))
         return launch_stream<T, BS>(d, x, y, stream);
     if (nrhs > 1 || d.kernel == 3 || d.kernel == 4)

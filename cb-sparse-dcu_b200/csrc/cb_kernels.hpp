@@ -8,6 +8,21 @@
 
 namespace cb {
 
+// The row-segment stream on the device (layout in cb_rowseg.hpp); chunks is
+// NULL when the plan has none.
+struct RowSegDev {
+    const uint8_t *chunks = nullptr;
+    int32_t nch = 0, M = 0, nseg = 0, nord = 0;
+    const int4 *meta = nullptr;       // per segment: ord0, starts_row, head span, tail span
+    const int4 *spans = nullptr;      // per span: first segment, last segment, ordinal, 0
+    int32_t *counters = nullptr;      // per span, zero between launches
+    void *part = nullptr;             // 2 * nseg partial sums
+    const int32_t *rowmap = nullptr;  // ordinal -> row, NULL when every row is non-empty
+    const int32_t *empty = nullptr;   // rows without stored entries
+    int32_t nempty = 0;
+    const int32_t *vpos = nullptr;    // per stored value: its stream entry
+};
+
 // Device-resident pieces of one DeviceLayout (cb_layout.hpp).
 struct DevLayout {
     const void *tiles = nullptr;      // TileDesc[ntiles]
@@ -36,7 +51,9 @@ struct DevLayout {
     // directly (the reference's EXEC_SMALL_DIRECT, cb-spmv-dcu.hpp:1437-1439)
     int small_direct = 0;
     int64_t max_entries = 0;          // largest COO section of a tile
-    int kernel = 0;                   // 0 auto, 1 streaming (TMA), 2 direct
+    int kernel = 0;                   // 0 auto, 1 streaming (TMA), 2 direct, 3 several
+                                      // right-hand sides, 4 pattern reuse, 5 row segments
+    RowSegDev rs;                     // row-segment stream (kernel 5)
     double coo_share = 1.0;
     const uint32_t *wpart = nullptr;  // streaming: per-warp tile ranges
     int64_t nwarps = 0;               // streaming: warps of the launch
@@ -126,6 +143,15 @@ int64_t stream_warps(const DevLayout &d);
 // pattern, lanes sum x over its columns and write the sum to every row of the
 // pattern (the reference's EXEC_PATTERN_REUSE_*, cb-spmv-dcu.hpp:626-674).
 cudaError_t launch_pattern(const DevLayout &d, const void *x, void *y, cudaStream_t stream);
+
+// Row-segment stream (cb_rowseg_kernels.cu): warps of one launch on the current
+// device (one CTA of kRsWarps warps per SM; 0 when the kernel cannot run);
+// y = A x over d.rs; the stream's values refreshed from the tile payload
+// (after the payload's values changed).
+int64_t rowseg_warps(int f32);
+cudaError_t launch_rowseg(const DevLayout &d, const void *x, void *y, cudaStream_t stream);
+cudaError_t launch_rowseg_values(const DevLayout &d, int64_t nvals, const uint64_t *val_off,
+                                 cudaStream_t stream);
 
 // y = A x; x: n rows, y: m rows, row-major with leading dims for nrhs > 1.
 cudaError_t launch_spmv(const DevLayout &d, const void *x, void *y, int nrhs,

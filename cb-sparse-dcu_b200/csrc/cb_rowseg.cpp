@@ -1,0 +1,119 @@
+// Host build of the row-segment stream (layout in cb_rowseg.hpp).
+#include "cb_rowseg.hpp"
+
+#include <algorithm>
+#include <cstring>
+
+namespace cb {
+
+bool rowseg_applies(const DeviceLayout &L) {
+    if (L.unit || L.nvals <= 0 || L.n > kRsMaxCols || L.m >= (int64_t(1) << 31)) return false;
+    // the per-value arrays (absent from plans loaded from SpMV-only files)
+    if ((int64_t)L.val_row.size() != L.nvals || (int64_t)L.val_col.size() != L.nvals ||
+        (int64_t)L.val_off.size() != L.nvals)
+        return false;
+    for (const BlockDesc &b : L.blocks)
+        if (meta_type(b.meta) != 0) return false;  // a CSR or DENSE block
+    return true;
+}
+
+std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
+    if (!rowseg_applies(L)) return "the layout does not take the row-segment stream";
+    const int64_t nv = L.nvals, m = L.m, C = rs_chunk_entries();
+    const int f32 = L.f32;
+    const int64_t vsz = f32 ? 4 : 8, CB = rs_chunk_bytes(f32);
+    R = RowSegHost();
+    R.f32 = f32;
+    R.m = m;
+    R.n = L.n;
+    // stored values by (row, column): counting sort on rows, then columns
+    std::vector<int64_t> rp((size_t)m + 1, 0);
+    for (int64_t v = 0; v < nv; ++v) ++rp[(size_t)L.val_row[v] + 1];
+    for (int64_t r = 0; r < m; ++r) rp[r + 1] += rp[r];
+    std::vector<int64_t> order((size_t)nv);
+    {
+        std::vector<int64_t> at(rp.begin(), rp.end() - 1);
+        for (int64_t v = 0; v < nv; ++v) order[(size_t)at[(size_t)L.val_row[v]]++] = v;
+    }
+#pragma omp parallel for schedule(dynamic, 4096)
+    for (int64_t r = 0; r < m; ++r)
+        std::sort(order.begin() + rp[r], order.begin() + rp[r + 1],
+                  [&](int64_t a, int64_t b) { return L.val_col[a] < L.val_col[b]; });
+    // ordinals of the non-empty rows
+    int64_t nord = 0;
+    for (int64_t r = 0; r < m; ++r) nord += rp[r + 1] > rp[r];
+    R.nord = (int32_t)nord;
+    if (nord < m) {
+        R.rowmap.reserve((size_t)nord);
+        for (int64_t r = 0; r < m; ++r) {
+            if (rp[r + 1] > rp[r])
+                R.rowmap.push_back((int32_t)r);
+            else
+                R.empty.push_back((int32_t)r);
+        }
+    }
+    const int64_t nch = (nv + C - 1) / C;
+    R.nch = (int32_t)nch;
+    R.chunks.assign((size_t)(nch * CB), 0);
+    R.vpos.resize((size_t)nv);
+    // words, values and per-entry ordinals; padding: value 0 on column 0,
+    // the first padding entry starting the extra ordinal nord
+    std::vector<int32_t> ordv((size_t)(nch * C));
+    std::vector<uint8_t> start((size_t)(nch * C), 0);
+    int64_t ord = 0;
+    for (int64_t e = 0; e < nch * C; ++e) {
+        uint32_t word;
+        if (e < nv) {
+            const int64_t v = order[(size_t)e];
+            const bool st = e > 0 && L.val_row[v] != L.val_row[order[(size_t)e - 1]];
+            ord += st;
+            start[(size_t)e] = st;
+            word = (uint32_t)L.val_col[v] | (st ? kRsStart : 0u);
+            std::memcpy(R.chunks.data() + rs_value_offset(e, f32),
+                        L.payload.data() + L.val_off[v], (size_t)vsz);
+            R.vpos[(size_t)v] = (int32_t)e;
+        } else {
+            const bool st = e == nv;
+            ord = st ? nord : ord;
+            start[(size_t)e] = st;
+            word = st ? kRsStart : 0u;
+        }
+        ordv[(size_t)e] = (int32_t)ord;
+        // with 4 entries per lane the words of a chunk are in entry order
+        const int64_t c = e / C, i = e % C;
+        std::memcpy(R.chunks.data() + c * CB + 4 * i, &word, 4);
+    }
+    // segments of M chunks, about one per warp
+    const int64_t M = std::max<int64_t>(1, (nch + std::max<int64_t>(warps, 1) - 1) /
+                                               std::max<int64_t>(warps, 1));
+    const int64_t nseg = (nch + M - 1) / M;
+    R.M = (int32_t)M;
+    R.nseg = (int32_t)nseg;
+    R.meta.assign((size_t)(4 * nseg), -1);
+    int32_t open = -1;
+    for (int64_t s = 0; s < nseg; ++s) {
+        const int64_t e0 = s * M * C, e1 = std::min(nch, (s + 1) * M) * C - 1;
+        int32_t *mt = &R.meta[(size_t)(4 * s)];
+        mt[0] = ordv[(size_t)e0] - start[(size_t)e0];
+        mt[1] = start[(size_t)e0];
+        int64_t nfl = 0;
+        for (int64_t e = e0; e <= e1; ++e) nfl += start[(size_t)e];
+        if (s > 0 && !start[(size_t)e0]) {  // the first row goes on from segment s - 1
+            if (open < 0) return "row-segment spans out of order";
+            mt[2] = open;
+            R.spans[(size_t)(4 * open + 1)] = (int32_t)s;
+        }
+        const bool cont = s + 1 < nseg && !start[(size_t)((s + 1) * M * C)];
+        if (!cont) {
+            open = -1;
+        } else if (nfl > 0 || mt[2] < 0) {  // the last row starts here: a new span
+            open = (int32_t)(R.spans.size() / 4);
+            R.spans.insert(R.spans.end(), {(int32_t)s, (int32_t)s, ordv[(size_t)e1], 0});
+            mt[3] = open;
+        }
+    }
+    R.alg_bytes = L.alg_bytes;
+    return "";
+}
+
+}  // namespace cb

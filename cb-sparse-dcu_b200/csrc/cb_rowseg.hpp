@@ -1,0 +1,82 @@
+// Row-segment stream: the one-right-hand-side layout of matrices whose
+// stored entries are all in COO blocks (power-law and other scattered
+// matrices, where the blocks hold a few entries each).
+//
+// The stored entries, sorted by (row, column), are cut into CHUNKS of
+// 32 x kRsK entries: lane l of a warp takes the kRsK consecutive entries
+// l*kRsK .. l*kRsK+kRsK-1 of a chunk and adds them up in registers along its
+// rows; one segmented shuffle scan per chunk joins the rows that run across
+// lanes.  Each entry is one u32 index word and one value:
+//
+//   word = column | bit 31 when the entry starts a new non-empty row
+//
+// so a lane finds its rows by counting row starts (an exclusive scan of the
+// lanes' counts) from the chunk's running row: no row index is stored.  A
+// chunk is [u32 words in 4-word vectors | T values in 16-byte vectors],
+// vector q of lane l at q*32 + l, so each warp load is one coalesced 512-byte
+// access.
+//
+// Chunks are grouped in SEGMENTS of M consecutive chunks, about one segment
+// per resident warp (equal entry counts: balanced by construction).  A row
+// that crosses segment boundaries is a SPAN: each of its segments leaves a
+// partial sum in a slot (2 s: the segment's first row, 2 s + 1: its last),
+// and the last segment to arrive on the span's counter adds the slots in
+// segment order and stores y, so results do not depend on timing.
+// Rows are counted as ORDINALS of the non-empty rows (rowmap maps them back
+// when some rows are empty; those rows are listed in `empty` and zeroed).
+// The entry count is padded to whole chunks with entries of value 0 on
+// column 0 that start one extra ordinal (nord), whose sum is never stored.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "cb_layout.hpp"
+
+namespace cb {
+
+constexpr int kRsK = 4;            // entries per lane per chunk
+constexpr int kRsWarps = 32;       // warps per CTA (one CTA per SM)
+constexpr uint32_t kRsStart = 1u << 31;   // word: the entry starts a row
+constexpr uint32_t kRsColMask = (1u << 30) - 1;
+constexpr int64_t kRsMaxCols = int64_t(1) << 30;
+
+inline int rs_chunk_entries() { return 32 * kRsK; }
+inline int64_t rs_chunk_bytes(int f32) { return 32 * kRsK * (4 + (f32 ? 4 : 8)); }
+
+// Byte offset, inside the chunk buffer, of the value of stream entry e.
+inline int64_t rs_value_offset(int64_t e, int f32) {
+    const int64_t C = 32 * kRsK, c = e / C, i = e % C, l = i / kRsK, j = i % kRsK;
+    const int64_t vsz = f32 ? 4 : 8, nv = 16 / vsz;  // values per 16-byte vector
+    const int64_t pos = (j / nv) * 32 * nv + l * nv + j % nv;
+    return c * rs_chunk_bytes(f32) + 4 * C + pos * vsz;
+}
+
+struct RowSegHost {
+    int f32 = 0;
+    int64_t m = 0, n = 0;
+    int32_t nch = 0;        // chunks
+    int32_t M = 0;          // chunks per segment
+    int32_t nseg = 0;
+    int32_t nord = 0;       // non-empty rows
+    std::vector<uint8_t> chunks;
+    std::vector<int32_t> meta;     // per segment: ord0, starts_row, head span, tail span
+    std::vector<int32_t> spans;    // per span: first segment, last segment, ordinal, 0
+    std::vector<int32_t> rowmap;   // ordinal -> row (empty when every row is non-empty)
+    std::vector<int32_t> empty;    // rows with no stored entry
+    std::vector<int32_t> vpos;     // per stored value (device order): its stream entry
+    int64_t alg_bytes = 0;
+};
+
+// Whether the layout takes the row-segment stream: stored values with their
+// per-value arrays, every block a COO block, columns below 2^30, rows below
+// 2^31.
+bool rowseg_applies(const DeviceLayout &L);
+
+// Builds the stream from the layout's stored values (device order: val_row,
+// val_col and the values at val_off in the payload) for `warps` resident
+// warps.  Returns "" or an error.
+std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R);
+
+}  // namespace cb

@@ -67,7 +67,13 @@ typedef struct cbspmv_opts {
                              valued plans: one sum per row pattern, the
                              reference's EXEC_PATTERN_REUSE; automatic when
                              patterns are fewer than half the rows, as in
-                             cb-spmv-dcu.hpp:1431-1433); see cbspmv_autotune */
+                             cb-spmv-dcu.hpp:1431-1433), 5 row segments (the
+                             stored entries sorted by row in chunks of 128,
+                             summed per lane and joined by one scan; built
+                             at upload, and the automatic choice, when every
+                             block is a COO block and values are stored;
+                             keeps a second copy of the values on the
+                             device); see cbspmv_autotune */
     int keep_values;      /* 0 (default): when every stored value is 1, store
                              no values and DENSE blocks as bitmasks, as the
                              reference does (UNIT_VALUES,
@@ -104,6 +110,8 @@ typedef struct cbspmv_info {
     int64_t segments, patterns, stored_values;
     int64_t tiles, split_rows, device_bytes, algorithmic_bytes;
     int64_t scratch_bytes;
+    int64_t rowseg_bytes;   /* device bytes of the row-segment stream (kernel
+                               5) once uploaded, else 0 */
 } cbspmv_info;
 
 typedef struct cbspmv_plan cbspmv_plan;
@@ -269,7 +277,10 @@ cbspmv_status cbspmv_info_get(const cbspmv_plan *plan, cbspmv_info *info);
  * bidx_*, pay_u32, pay_f64, pay_*_off, ...) into out (may be NULL) and
  * returns its length, or -1 for an unknown name.  The names dev_tiles,
  * dev_blocks (uint32 words), dev_payload (bytes) and dev_values (double, one
- * per stored slot) give the device layout itself. */
+ * per stored slot) give the device layout itself; rs_sizes, rs_chunks
+ * (bytes), rs_meta, rs_spans, rs_rowmap, rs_empty and rs_vpos (int32), each
+ * followed by ":W", the row-segment stream as built for W resident warps
+ * (-1 when the layout does not take it). */
 int64_t cbspmv_export(const cbspmv_plan *plan, const char *name, void *out);
 
 /* The same for the CB structure of A^T (plans built with want_transpose). */
@@ -306,9 +317,10 @@ cbspmv_status cbspmv_check(cbspmv_plan *plan, void *stream);
 void cbspmv_debug_wait_polls(int64_t polls);
 
 /* Times the kernels that can run this plan for nrhs right-hand sides (one
- * vector: streaming when the layout allows it, direct, staged; several: the
- * staged kernel) on scratch vectors, keeps the fastest for later calls and
- * returns it in *kernel (1, 2 or 3) with its mean time in *ms (either may be
+ * vector: streaming when the layout allows it, direct, staged, pattern reuse
+ * and row segments when the plan has them; several: the staged kernel) on
+ * scratch vectors, keeps the fastest for later calls and returns it in
+ * *kernel (1 to 5) with its mean time in *ms (either may be
  * NULL).  The plan must be uploaded; allocates and frees scratch device
  * memory and synchronizes `stream`.  No counterpart in the reference (its
  * kernel choice is compile-time, cb-spmv-dcu.hpp:1428-1450). */

@@ -1,0 +1,84 @@
+"""CPU checks of the row-segment stream's host build (cb_rowseg.cpp): read
+back through cbspmv_export and evaluated exactly as the kernel adds it
+(layout_decode.rowseg_spmv), it gives the oracle's y for several resident
+warp counts (one segment per chunk up to one segment for everything), and
+its value positions are a permutation holding the layout's stored values."""
+import numpy as np
+import pytest
+
+TOL = {False: 1e-12, True: 1e-5}
+
+
+def _small_cases():
+    from cbspmv import gen
+    rng = np.random.default_rng(31)
+    out = [("random", gen.random_small(rng, 700, 600, 6000)),
+           ("dups", gen.random_small(rng, 300, 300, 2500, dup=True)),
+           ("power-law", gen.power_law(1 << 11, seed=4))]
+    n = 16 * 3000
+    rows = np.concatenate([np.full(3000, 5), (rng.integers(0, 900, 2000) // 7) * 7])
+    cols = np.concatenate([np.arange(3000) * 16 + 1, rng.integers(0, n, 2000)])
+    key = np.unique(rows.astype(np.int64) * n + cols)
+    out.append(("huge-row-empty-rows",
+                gen.Coo(900, n, (key // n).astype(np.int32), (key % n).astype(np.int32),
+                        rng.standard_normal(key.size))))
+    for nnz in (128 * 9, 128 * 9 + 1, 1):
+        r = np.arange(nnz) // 2
+        c = (np.arange(nnz) * 61) % 4000
+        out.append((f"entries-{nnz}", gen.Coo(int(r.max()) + 1, 4000, r.astype(np.int32),
+                                              c.astype(np.int32), rng.standard_normal(nnz))))
+    return out
+
+
+CASES = _small_cases()
+
+
+@pytest.mark.parametrize("name,coo", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("f32", [False, True])
+@pytest.mark.parametrize("warps", [1, 3, 64, 4736])
+def test_rowseg_layout_decodes_to_oracle(name, coo, f32, warps):
+    import cbspmv
+    import cbdump as cd
+    from cbspmv import gen
+    from layout_decode import rowseg_arrays, rowseg_spmv
+    plan = cbspmv.Plan(coo, value_type=int(f32))
+    rs = rowseg_arrays(plan, warps)
+    assert rs is not None
+    x = gen.uniform_x(coo.n, 2)
+    if f32:
+        x = x.astype(np.float32).astype(np.float64)
+    y = rowseg_spmv(rs, x, coo.m, f32)
+    assert np.all(np.isfinite(y)), "a row was never written"
+    yref, ab = cd.oracle_spmm_ld(coo, x[None, :])
+    err = np.abs(y.astype(np.float64)[None, :] - yref)
+    assert np.all(err <= TOL[f32] * ab + 1e-300)
+    nch, M, nseg, nord = (int(v) for v in rs["sizes"])
+    assert nseg == -(-nch // M) and nseg <= max(warps, 1) + 1
+    # every stored value sits once in the stream, at its value position
+    vp = rs["vpos"]
+    assert np.array_equal(np.sort(vp), np.arange(vp.size))
+    cnt = cbspmv.lib().cbspmv_export(plan._h, b"dev_values", None)
+    dv = np.zeros(cnt, np.float64)
+    cbspmv.lib().cbspmv_export(plan._h, b"dev_values", dv.ctypes.data_as(cbspmv.ctypes.c_void_p))
+    T = np.float32 if f32 else np.float64
+    vsz = 4 if f32 else 8
+    C, nv = 128, 16 // vsz
+    i = vp % C
+    pos = ((i % 4) // nv) * 32 * nv + (i // 4) * nv + (i % 4) % nv
+    flat = rs["chunks"].reshape(nch, -1)[vp // C, :]
+    got = np.array([flat[k, 4 * C + pos[k] * vsz: 4 * C + (pos[k] + 1) * vsz].view(T)[0]
+                    for k in range(vp.size)])
+    assert np.array_equal(got.astype(np.float64), dv)
+
+
+def test_rowseg_not_built_for_csr_layouts():
+    """A layout with CSR/DENSE blocks keeps the tile kernels (no stream)."""
+    import cbspmv
+    from cbspmv import gen
+    from layout_decode import rowseg_arrays
+    rng = np.random.default_rng(3)
+    coo = gen.random_small(rng, 100, 100, 9000)  # dense blocks
+    plan = cbspmv.Plan(coo)
+    info = plan.info()
+    assert info["csr_blocks"] + info["dense_blocks"] > 0
+    assert rowseg_arrays(plan, 64) is None
