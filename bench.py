@@ -15,7 +15,8 @@ value       algorithmic GB/s of the whole job: the bytes of the packed CB
 e2e         the same metric through the C ABI with host buffers
             (cbspmv_spmv_host_async: pinned x copied in, y copied out every
             step; consecutive steps overlap copy in, kernel and copy out).
-roofline    the streaming kernel (the one launch of a step) against the
+roofline    the kernel of the one launch of a step (the row-segment stream
+            kernel: every block of this matrix is a COO block) against the
             measured HBM copy bandwidth; traffic = its DRAM bytes per launch
             from the committed ncu summary (profiles/).
 cpu_baseline  the reference's own CPU SpMV (utils.h:98-111, compiled from its
@@ -68,11 +69,12 @@ def _peaks():
         return 6650.0, "fallback"
 
 
-def _ncu_traffic():
-    """DRAM bytes per launch of the tile kernel from the committed ncu
-    summary (profiles/), or None."""
+def _ncu_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` on the PL FP64 workload from the
+    committed ncu summaries (profiles/), or None."""
+    pat = r"dram_bytes_per_launch_pl_fp64\[" + re.escape(kernel) + r"\]\s*=\s*([0-9.eE+]+)"
     for p in sorted((REPO / "profiles").glob("*.md")):
-        m = re.search(r"dram_bytes_per_launch_pl_fp64\s*=\s*([0-9.eE+]+)", p.read_text())
+        m = re.search(pat, p.read_text())
         if m:
             return float(m.group(1))
     return None
@@ -661,11 +663,12 @@ def main():
     e2e_value = world * alg / (ms_e2e * 1e-3) / 1e9
 
     peak, peak_kind = _peaks()
+    kname = "cb_rowseg_kernel" if plan.info()["rowseg_bytes"] > 0 else "cb_spmv_stream_kernel"
     achieved = alg / (ms * 1e-3) / 1e9
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-            "traffic": _ncu_traffic(),
-            "kernel": "cb_spmv_stream_kernel (the one launch of each SpMV)"}
+            "traffic": _ncu_traffic(kname),
+            "kernel": f"{kname} (the one launch of each SpMV)"}
 
     # library comparator: cuSPARSE CSR SpMV (through torch) on the same matrix
     comparator = None
