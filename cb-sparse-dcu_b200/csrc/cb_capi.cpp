@@ -1202,7 +1202,8 @@ int64_t export_device(const cb::DeviceLayout &L, const std::string &k, void *out
 // block arrays and no per-value arrays: those names give -1.
 bool exportable(const cbspmv_plan *p, const std::string &k) {
     if (!p->spmv_only) return true;
-    const bool ok = k == "dev_tiles" || k == "dev_blocks" || k == "dev_payload";
+    const bool ok = k == "dev_tiles" || k == "dev_blocks" || k == "dev_payload" ||
+                    k.rfind("rs_", 0) == 0;
     if (!ok) fail(CBSPMV_ERR_STATE, "plan loaded from an SpMV-only plan file: no " + k);
     return ok;
 }

@@ -2,16 +2,18 @@
 #include "cb_rowseg.hpp"
 
 #include <algorithm>
+#include <climits>
 #include <cstring>
+#include <utility>
 
 namespace cb {
 
+namespace {
+int64_t a16_64(int64_t x) { return (x + 15) & ~int64_t(15); }
+}  // namespace
+
 bool rowseg_applies(const DeviceLayout &L) {
     if (L.unit || L.nvals <= 0 || L.n > kRsMaxCols || L.m >= (int64_t(1) << 31)) return false;
-    // the per-value arrays (absent from plans loaded from SpMV-only files)
-    if ((int64_t)L.val_row.size() != L.nvals || (int64_t)L.val_col.size() != L.nvals ||
-        (int64_t)L.val_off.size() != L.nvals)
-        return false;
     for (const BlockDesc &b : L.blocks)
         if (meta_type(b.meta) != 0) return false;  // a CSR or DENSE block
     return true;
@@ -19,26 +21,46 @@ bool rowseg_applies(const DeviceLayout &L) {
 
 std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
     if (!rowseg_applies(L)) return "the layout does not take the row-segment stream";
-    const int64_t nv = L.nvals, m = L.m, C = rs_chunk_entries();
+    const int64_t m = L.m, C = rs_chunk_entries();
     const int f32 = L.f32;
     const int64_t vsz = f32 ? 4 : 8, CB = rs_chunk_bytes(f32);
     R = RowSegHost();
     R.f32 = f32;
     R.m = m;
     R.n = L.n;
-    // stored values by (row, column): counting sort on rows, then columns
+    // the entries of the tiles' COO sections (every block is a COO block):
+    // row, column and the payload offset of the value
+    int64_t nv = 0;
+    for (const TileDesc &t : L.tiles) nv += t.coo_entries;
+    if (nv != L.nvals) return "row-segment stream: COO entries and stored values differ";
+    std::vector<int32_t> erow((size_t)nv), ecol((size_t)nv);
+    std::vector<int64_t> eoff((size_t)nv);
+    {
+        int64_t k = 0;
+        for (const TileDesc &t : L.tiles) {
+            const int64_t E = t.coo_entries, base = (int64_t)t.payload16 * 16;
+            const uint32_t *idx = reinterpret_cast<const uint32_t *>(L.payload.data() + base);
+            const int64_t vals = base + a16_64(4 * E);
+            for (int64_t q = 0; q < E; ++q, ++k) {
+                erow[(size_t)k] = (int32_t)((int64_t)t.block_row * L.bs + (idx[q] >> kColBits));
+                ecol[(size_t)k] = (int32_t)(idx[q] & ((1u << kColBits) - 1));
+                eoff[(size_t)k] = vals + q * vsz;
+            }
+        }
+    }
+    // entries by (row, column): counting sort on rows, then columns
     std::vector<int64_t> rp((size_t)m + 1, 0);
-    for (int64_t v = 0; v < nv; ++v) ++rp[(size_t)L.val_row[v] + 1];
+    for (int64_t v = 0; v < nv; ++v) ++rp[(size_t)erow[v] + 1];
     for (int64_t r = 0; r < m; ++r) rp[r + 1] += rp[r];
     std::vector<int64_t> order((size_t)nv);
     {
         std::vector<int64_t> at(rp.begin(), rp.end() - 1);
-        for (int64_t v = 0; v < nv; ++v) order[(size_t)at[(size_t)L.val_row[v]]++] = v;
+        for (int64_t v = 0; v < nv; ++v) order[(size_t)at[(size_t)erow[v]]++] = v;
     }
 #pragma omp parallel for schedule(dynamic, 4096)
     for (int64_t r = 0; r < m; ++r)
         std::sort(order.begin() + rp[r], order.begin() + rp[r + 1],
-                  [&](int64_t a, int64_t b) { return L.val_col[a] < L.val_col[b]; });
+                  [&](int64_t a, int64_t b) { return ecol[a] < ecol[b]; });
     // ordinals of the non-empty rows
     int64_t nord = 0;
     for (int64_t r = 0; r < m; ++r) nord += rp[r + 1] > rp[r];
@@ -55,7 +77,6 @@ std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
     const int64_t nch = (nv + C - 1) / C;
     R.nch = (int32_t)nch;
     R.chunks.assign((size_t)(nch * CB), 0);
-    R.vpos.resize((size_t)nv);
     // words, values and per-entry ordinals; padding: value 0 on column 0,
     // the first padding entry starting the extra ordinal nord
     std::vector<int32_t> ordv((size_t)(nch * C));
@@ -65,13 +86,13 @@ std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
         uint32_t word;
         if (e < nv) {
             const int64_t v = order[(size_t)e];
-            const bool st = e > 0 && L.val_row[v] != L.val_row[order[(size_t)e - 1]];
+            const bool st = e > 0 && erow[v] != erow[order[(size_t)e - 1]];
             ord += st;
             start[(size_t)e] = st;
-            word = (uint32_t)L.val_col[v] | (st ? kRsStart : 0u);
+            word = (uint32_t)ecol[v] | (st ? kRsStart : 0u);
             std::memcpy(R.chunks.data() + rs_value_offset(e, f32),
-                        L.payload.data() + L.val_off[v], (size_t)vsz);
-            R.vpos[(size_t)v] = (int32_t)e;
+                        L.payload.data() + eoff[v], (size_t)vsz);
+            eoff[v] = -1 - e;  // from here on: the entry's place in the stream
         } else {
             const bool st = e == nv;
             ord = st ? nord : ord;
@@ -110,6 +131,31 @@ std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
             open = (int32_t)(R.spans.size() / 4);
             R.spans.insert(R.spans.end(), {(int32_t)s, (int32_t)s, ordv[(size_t)e1], 0});
             mt[3] = open;
+        }
+    }
+    // per stored value (device order) its stream entry, for value updates:
+    // stored value v sits at payload offset val_off[v] (absent from plans
+    // loaded from SpMV-only files, which take no new values)
+    if ((int64_t)L.val_off.size() == nv) {
+        std::vector<std::pair<int64_t, int32_t>> by_off((size_t)nv);
+        {
+            int64_t k = 0;
+            for (const TileDesc &t : L.tiles) {
+                const int64_t E = t.coo_entries, base = (int64_t)t.payload16 * 16;
+                for (int64_t q = 0; q < E; ++q, ++k)
+                    by_off[(size_t)k] = {base + a16_64(4 * E) + q * vsz,
+                                         (int32_t)(-1 - eoff[(size_t)k])};
+            }
+        }
+        std::sort(by_off.begin(), by_off.end());
+        R.vpos.resize((size_t)nv);
+        for (int64_t v = 0; v < nv; ++v) {
+            const int64_t off = (int64_t)L.val_off[v];
+            auto it = std::lower_bound(by_off.begin(), by_off.end(),
+                                       std::make_pair(off, INT32_MIN));
+            if (it == by_off.end() || it->first != off)
+                return "row-segment stream: a stored value outside the COO sections";
+            R.vpos[(size_t)v] = it->second;
         }
     }
     R.alg_bytes = L.alg_bytes;

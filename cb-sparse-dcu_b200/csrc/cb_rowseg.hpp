@@ -65,18 +65,19 @@ struct RowSegHost {
     std::vector<int32_t> spans;    // per span: first segment, last segment, ordinal, 0
     std::vector<int32_t> rowmap;   // ordinal -> row (empty when every row is non-empty)
     std::vector<int32_t> empty;    // rows with no stored entry
-    std::vector<int32_t> vpos;     // per stored value (device order): its stream entry
+    std::vector<int32_t> vpos;     // per stored value (device order): its stream entry,
+                                   // or empty without per-value offsets
     int64_t alg_bytes = 0;
 };
 
-// Whether the layout takes the row-segment stream: stored values with their
-// per-value arrays, every block a COO block, columns below 2^30, rows below
-// 2^31.
+// Whether the layout takes the row-segment stream: stored values, every
+// block a COO block, columns below 2^30, rows below 2^31.
 bool rowseg_applies(const DeviceLayout &L);
 
-// Builds the stream from the layout's stored values (device order: val_row,
-// val_col and the values at val_off in the payload) for `warps` resident
-// warps.  Returns "" or an error.
+// Builds the stream from the tiles' COO sections (row, column and value of
+// every entry) for `warps` resident warps; vpos only when the layout has its
+// per-value offsets (val_off).  Every plan of one matrix and value type gets
+// the same stream, so the same sums.  Returns "" or an error.
 std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R);
 
 }  // namespace cb

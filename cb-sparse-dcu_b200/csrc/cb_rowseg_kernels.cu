@@ -259,7 +259,7 @@ cudaError_t launch_rowseg(const DevLayout &d, const void *x, void *y, cudaStream
 
 cudaError_t launch_rowseg_values(const DevLayout &d, int64_t nvals, const uint64_t *val_off,
                                  cudaStream_t stream) {
-    if (!d.rs.chunks || nvals <= 0) return cudaSuccess;
+    if (!d.rs.chunks || !d.rs.vpos || nvals <= 0) return cudaSuccess;
     const unsigned grid =
         (unsigned)std::min<int64_t>((nvals + 255) / 256, (int64_t)dev_sms() * 16);
     if (d.f32)

@@ -156,7 +156,9 @@ cbspmv_status cbspmv_plan_load(const char *path, cbspmv_plan **out);
  * calls that need per-value data (cbspmv_set_values, cbspmv_grad_vals, the
  * value gradient of cbspmv_adjoint, cbspmv_value_coords,
  * cbspmv_input_slots) return CBSPMV_ERR_STATE, and cbspmv_export returns -1
- * for every name but dev_tiles, dev_blocks and dev_payload. */
+ * for every name but dev_tiles, dev_blocks, dev_payload and the rs_* names
+ * (the row-segment stream is built from the tiles, so it is the same as the
+ * saved plan's). */
 #define CBSPMV_PLAN_SPMV_ONLY 1
 cbspmv_status cbspmv_plan_save_ex(const cbspmv_plan *plan, const char *path,
                                   int flags);

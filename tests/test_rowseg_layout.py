@@ -82,3 +82,23 @@ def test_rowseg_not_built_for_csr_layouts():
     info = plan.info()
     assert info["csr_blocks"] + info["dense_blocks"] > 0
     assert rowseg_arrays(plan, 64) is None
+
+
+@pytest.mark.parametrize("spmv_only", [False, True])
+def test_rowseg_same_stream_after_plan_file(tmp_path, spmv_only):
+    """A plan loaded from a plan file (SpMV-only files carry no per-value
+    arrays) builds the same stream as the plan it was saved from, so both
+    give bit-identical sums."""
+    import cbspmv
+    from cbspmv import gen
+    from layout_decode import rowseg_arrays
+    coo = gen.power_law(1 << 11, seed=6)
+    p = cbspmv.Plan(coo)
+    path = tmp_path / "p.cbplan"
+    p.save(path, spmv_only=spmv_only)
+    q = cbspmv.Plan.load(path)
+    a, b = rowseg_arrays(p, 64), rowseg_arrays(q, 64)
+    assert a is not None and b is not None
+    for k in ("sizes", "chunks", "meta", "spans", "rowmap", "empty"):
+        assert np.array_equal(a[k], b[k]), k
+    assert b["vpos"].size == (0 if spmv_only else coo.nnz)
