@@ -69,8 +69,8 @@ struct DevSide {
     int32_t *val_row = nullptr, *val_col = nullptr;
     int32_t *pat[4] = {};  // pattern row_ptr, col_idx, output_ptr, output_rows
     // row-segment stream (kernel 5): chunks, segment meta, spans, counters,
-    // partial slots, rowmap, empty rows, value positions
-    void *rs[8] = {};
+    // partial slots, rowmap, empty rows, value positions, window bases
+    void *rs[9] = {};
     int64_t rs_bytes = 0;
 
     void release() {
@@ -305,6 +305,7 @@ cbspmv_status upload_rowseg(DevSide &s, int kernel, cudaStream_t st) {
     CB_CUDA(upload_vec(R.rowmap, (int32_t **)&s.rs[5], st), "upload row segments");
     CB_CUDA(upload_vec(R.empty, (int32_t **)&s.rs[6], st), "upload row segments");
     CB_CUDA(upload_vec(R.vpos, (int32_t **)&s.rs[7], st), "upload row segments");
+    CB_CUDA(upload_vec(R.wbase, (int32_t **)&s.rs[8], st), "upload row segments");
     cb::RowSegDev &d = s.d.rs;
     d.chunks = static_cast<const uint8_t *>(s.rs[0]);
     d.nch = R.nch;
@@ -319,6 +320,10 @@ cbspmv_status upload_rowseg(DevSide &s, int kernel, cudaStream_t st) {
     d.empty = static_cast<const int32_t *>(s.rs[6]);
     d.nempty = (int32_t)R.empty.size();
     d.vpos = static_cast<const int32_t *>(s.rs[7]);
+    d.G = R.G;
+    d.W = R.W;
+    d.wbase = static_cast<const int32_t *>(s.rs[8]);
+    d.n = R.n;
     s.rs_bytes = (int64_t)(R.chunks.size() + 4 * (R.meta.size() + R.spans.size() +
                                                   R.rowmap.size() + R.empty.size()));
     return CBSPMV_OK;
@@ -1185,7 +1190,7 @@ int64_t export_device(const cb::DeviceLayout &L, const std::string &k, void *out
         const std::string f = k.substr(3, colon - 3);
         cb::RowSegHost R;
         if (warps <= 0 || !cb::build_rowseg(L, warps, R).empty()) return -1;
-        const int32_t sizes[4] = {R.nch, R.M, R.nseg, R.nord};
+        const int32_t sizes[6] = {R.nch, R.M, R.nseg, R.nord, R.G, R.W};
         if (f == "sizes") return raw(sizes, sizeof sizes, 4);
         if (f == "chunks") return raw(R.chunks.data(), R.chunks.size(), 1);
         if (f == "meta") return raw(R.meta.data(), R.meta.size() * 4, 4);
@@ -1193,6 +1198,7 @@ int64_t export_device(const cb::DeviceLayout &L, const std::string &k, void *out
         if (f == "rowmap") return raw(R.rowmap.data(), R.rowmap.size() * 4, 4);
         if (f == "empty") return raw(R.empty.data(), R.empty.size() * 4, 4);
         if (f == "vpos") return raw(R.vpos.data(), R.vpos.size() * 4, 4);
+        if (f == "wbase") return raw(R.wbase.data(), R.wbase.size() * 4, 4);
     }
     return -1;
 }

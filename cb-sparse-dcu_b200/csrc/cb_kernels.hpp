@@ -21,6 +21,9 @@ struct RowSegDev {
     const int32_t *empty = nullptr;   // rows without stored entries
     int32_t nempty = 0;
     const int32_t *vpos = nullptr;    // per stored value: its stream entry
+    int32_t G = 0, W = 0;             // CTAs of every launch; window length (values)
+    const int32_t *wbase = nullptr;   // per CTA: first column of its x window
+    int64_t n = 0;                    // columns (length of x)
 };
 
 // Device-resident pieces of one DeviceLayout (cb_layout.hpp).

@@ -133,6 +133,42 @@ std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
             mt[3] = open;
         }
     }
+    // the CTAs' windows of x: per CTA, the W consecutive columns holding the
+    // most of its entries (a sliding window over its sorted columns)
+    const int64_t G = std::max<int64_t>(1, std::max<int64_t>(warps, 1) / kRsWarps);
+    const int64_t W = kRsWindowBytes / vsz;
+    R.G = (int32_t)G;
+    R.W = (int32_t)W;
+    R.wbase.assign((size_t)G, 0);
+    std::vector<int32_t> cols;
+    for (int64_t b = 0; b < G; ++b) {
+        const int64_t s0 = b * nseg / G, s1 = (b + 1) * nseg / G;
+        const int64_t e0 = std::min(nv, s0 * M * C), e1 = std::min(nv, s1 * M * C);
+        if (e0 >= e1) continue;
+        cols.clear();
+        for (int64_t e = e0; e < e1; ++e) cols.push_back(ecol[order[(size_t)e]]);
+        std::sort(cols.begin(), cols.end());
+        size_t best = 0, lo = 0;
+        int32_t wb = cols[0];
+        for (size_t hi = 0; hi < cols.size(); ++hi) {
+            while ((int64_t)cols[hi] - cols[lo] >= W) ++lo;
+            if (hi - lo + 1 > best) {
+                best = hi - lo + 1;
+                wb = cols[lo];
+            }
+        }
+        R.wbase[(size_t)b] = wb;
+        for (int64_t e = e0; e < e1; ++e) {
+            const int64_t col = ecol[order[(size_t)e]];
+            if (col >= wb && col < wb + W) {
+                const int64_t c = e / C, i = e % C;
+                uint32_t word;
+                std::memcpy(&word, R.chunks.data() + c * CB + 4 * i, 4);
+                word |= kRsWin;
+                std::memcpy(R.chunks.data() + c * CB + 4 * i, &word, 4);
+            }
+        }
+    }
     // per stored value (device order) its stream entry, for value updates:
     // stored value v sits at payload offset val_off[v] (absent from plans
     // loaded from SpMV-only files, which take no new values)

@@ -22,6 +22,13 @@
 // partial sum in a slot (2 s: the segment's first row, 2 s + 1: its last),
 // and the last segment to arrive on the span's counter adds the slots in
 // segment order and stores y, so results do not depend on timing.
+// Each CTA also holds a WINDOW of x in shared memory: kRsWindowBytes of
+// consecutive columns from wbase[b], chosen on the host to cover the most
+// entries of the CTA's segments; an entry whose column lies in its CTA's
+// window carries bit 30 and reads x from there (a shared-memory gather costs
+// a few wavefronts per warp where 32 scattered global loads cost 32 L1 tag
+// lookups).  The segments are assigned to CTAs for a grid of G CTAs fixed at
+// build time, so every launch uses that grid.
 // Rows are counted as ORDINALS of the non-empty rows (rowmap maps them back
 // when some rows are empty; those rows are listed in `empty` and zeroed).
 // The entry count is padded to whole chunks with entries of value 0 on
@@ -39,7 +46,9 @@ namespace cb {
 constexpr int kRsK = 4;            // entries per lane per chunk
 constexpr int kRsWarps = 32;       // warps per CTA (one CTA per SM)
 constexpr uint32_t kRsStart = 1u << 31;   // word: the entry starts a row
+constexpr uint32_t kRsWin = 1u << 30;    // word: x[column] is in the CTA's window
 constexpr uint32_t kRsColMask = (1u << 30) - 1;
+constexpr int64_t kRsWindowBytes = int64_t(128) << 10;
 constexpr int64_t kRsMaxCols = int64_t(1) << 30;
 
 inline int rs_chunk_entries() { return 32 * kRsK; }
@@ -60,6 +69,9 @@ struct RowSegHost {
     int32_t M = 0;          // chunks per segment
     int32_t nseg = 0;
     int32_t nord = 0;       // non-empty rows
+    int32_t G = 0;          // CTAs of every launch
+    int32_t W = 0;          // window length in values
+    std::vector<int32_t> wbase;    // per CTA: first column of its window
     std::vector<uint8_t> chunks;
     std::vector<int32_t> meta;     // per segment: ord0, starts_row, head span, tail span
     std::vector<int32_t> spans;    // per span: first segment, last segment, ordinal, 0
@@ -75,7 +87,7 @@ struct RowSegHost {
 bool rowseg_applies(const DeviceLayout &L);
 
 // Builds the stream from the tiles' COO sections (row, column and value of
-// every entry) for `warps` resident warps; vpos only when the layout has its
+// every entry) for `warps` resident warps (G = warps / kRsWarps CTAs); vpos only when the layout has its
 // per-value offsets (val_off).  Every plan of one matrix and value type gets
 // the same stream, so the same sums.  Returns "" or an error.
 std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R);

@@ -7,7 +7,9 @@
 //   * holds the NEXT chunk's words and values in registers, loaded with
 //     coalesced 16-byte loads that do not allocate in L1 (L1 is left to the
 //     x gathers) and are marked evict-first in L2 (x stays in L2),
-//   * gathers x for its kRsK entries, all loads in flight at once,
+//   * gathers x for its kRsK entries, all loads in flight at once: from the
+//     CTA's window of x in shared memory (staged at the start) when the
+//     entry's word says so, else from global memory,
 //   * counts its row starts; an exclusive warp scan of the counts gives the
 //     ordinal of the row it starts in,
 //   * adds its entries along its rows in registers; a row that starts and
@@ -95,11 +97,17 @@ __global__ void __launch_bounds__(kRsWarps * 32, 1)
     using V = typename RsVec<T>::V;
     constexpr int K = kRsK, NV = RsVec<T>::n;
     constexpr int64_t CB = 32 * K * (4 + (int64_t)sizeof(T));
+    extern __shared__ __align__(16) unsigned char rs_smem[];
+    T *xs = reinterpret_cast<T *>(rs_smem);  // x[wb .. wb + W)
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     for (int i = (blockIdx.x * kRsWarps + wib) * 32 + lane; i < rs.nempty;
          i += gridDim.x * kRsWarps * 32)
         y[__ldg(&rs.empty[i])] = T(0);
     const int G = gridDim.x, b = blockIdx.x;
+    const int64_t wb = __ldg(&rs.wbase[b]);
+    for (int i = threadIdx.x; i < rs.W; i += kRsWarps * 32)
+        xs[i] = wb + i < rs.n ? __ldg(x + wb + i) : T(0);
+    __syncthreads();
     const int sb0 = (int)((int64_t)b * rs.nseg / G);
     const int sb1 = (int)((int64_t)(b + 1) * rs.nseg / G);
     int s = sb0 + wib;
@@ -148,7 +156,10 @@ __global__ void __launch_bounds__(kRsWarps * 32, 1)
                 if (cn >= 0) load(cn);
             }
 #pragma unroll
-            for (int j = 0; j < K; ++j) xv[j] = __ldg(x + (w[j] & kRsColMask));
+            for (int j = 0; j < K; ++j) {
+                const uint32_t col = w[j] & kRsColMask;
+                xv[j] = (w[j] & kRsWin) ? xs[col - wb] : __ldg(x + col);
+            }
             int cnt = 0;
 #pragma unroll
             for (int j = 0; j < K; ++j) cnt += (int)(w[j] >> 31);
@@ -238,20 +249,32 @@ const void *rowseg_fn() {
 }
 
 int64_t rowseg_warps(int f32) {
-    // no shared memory: the carveout leaves the whole unified L1/shared
-    // memory to the L1 (the x gathers)
+    // the x window in shared memory; the carveout leaves the rest of the
+    // unified L1/shared memory to the L1 (the other x gathers)
     const void *fn = f32 ? rowseg_fn<float>() : rowseg_fn<double>();
-    return (int64_t)dev_sms() * dev_resident_l1(fn, kRsWarps * 32, 0) * kRsWarps;
+    if (dev_enable_smem(fn, (size_t)kRsWindowBytes) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return (int64_t)dev_sms() * dev_resident_l1(fn, kRsWarps * 32, (size_t)kRsWindowBytes) *
+           kRsWarps;
 }
 
 cudaError_t launch_rowseg(const DevLayout &d, const void *x, void *y, cudaStream_t stream) {
-    if (!d.rs.chunks || d.rs.nseg <= 0) return cudaErrorInvalidValue;
-    const unsigned grid = (unsigned)(rowseg_warps(d.f32) / kRsWarps);
+    if (!d.rs.chunks || d.rs.nseg <= 0 || d.rs.G <= 0 || !d.rs.wbase)
+        return cudaErrorInvalidValue;
+    const size_t smem = (size_t)d.rs.W * (d.f32 ? 4 : 8);
+    const void *fn = d.f32 ? rowseg_fn<float>() : rowseg_fn<double>();
+    cudaError_t e = dev_enable_smem(fn, smem);
+    if (e != cudaSuccess) return e;
+    dev_resident_l1(fn, kRsWarps * 32, smem);  // sets the carveout
+    // the grid the segments and windows were assigned for
+    const unsigned grid = (unsigned)d.rs.G;
     if (d.f32)
-        cb_rowseg_kernel<float><<<grid, kRsWarps * 32, 0, stream>>>(
+        cb_rowseg_kernel<float><<<grid, kRsWarps * 32, smem, stream>>>(
             d.rs, static_cast<const float *>(x), static_cast<float *>(y));
     else
-        cb_rowseg_kernel<double><<<grid, kRsWarps * 32, 0, stream>>>(
+        cb_rowseg_kernel<double><<<grid, kRsWarps * 32, smem, stream>>>(
             d.rs, static_cast<const double *>(x), static_cast<double *>(y));
     note_launch();
     return cudaGetLastError();

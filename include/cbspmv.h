@@ -279,8 +279,9 @@ cbspmv_status cbspmv_info_get(const cbspmv_plan *plan, cbspmv_info *info);
  * bidx_*, pay_u32, pay_f64, pay_*_off, ...) into out (may be NULL) and
  * returns its length, or -1 for an unknown name.  The names dev_tiles,
  * dev_blocks (uint32 words), dev_payload (bytes) and dev_values (double, one
- * per stored slot) give the device layout itself; rs_sizes, rs_chunks
- * (bytes), rs_meta, rs_spans, rs_rowmap, rs_empty and rs_vpos (int32), each
+ * per stored slot) give the device layout itself; rs_sizes (nch, M, nseg,
+ * nord, G, W), rs_chunks (bytes), rs_meta, rs_spans, rs_rowmap, rs_empty,
+ * rs_vpos and rs_wbase (int32), each
  * followed by ":W", the row-segment stream as built for W resident warps
  * (-1 when the layout does not take it). */
 int64_t cbspmv_export(const cbspmv_plan *plan, const char *name, void *out);

@@ -106,7 +106,7 @@ def rowseg_arrays(plan, warps: int, transpose: bool = False) -> dict | None:
     out = {}
     for name, dt in (("sizes", np.int32), ("chunks", np.uint8), ("meta", np.int32),
                      ("spans", np.int32), ("rowmap", np.int32), ("empty", np.int32),
-                     ("vpos", np.int32)):
+                     ("vpos", np.int32), ("wbase", np.int32)):
         key = f"rs_{name}:{warps}".encode()
         cnt = fn(plan._h, key, None)
         if cnt < 0:
@@ -126,7 +126,7 @@ def rowseg_spmv(rs: dict, x: np.ndarray, m: int, f32: bool) -> np.ndarray:
     K, C = 4, 128
     T = np.float32 if f32 else np.float64
     x = np.asarray(x, T)
-    nch, M, nseg, nord = (int(v) for v in rs["sizes"])
+    nch, M, nseg, nord, G, W = (int(v) for v in rs["sizes"])
     vsz = 4 if f32 else 8
     CB = C * (4 + vsz)
     chunks = rs["chunks"].reshape(nch, CB)
@@ -155,6 +155,7 @@ def rowseg_spmv(rs: dict, x: np.ndarray, m: int, f32: bool) -> np.ndarray:
             cnt[sp] = 0
 
     for s in range(nseg):
+        wb = int(rs["wbase"][next(b for b in range(G) if s < (b + 1) * nseg // G)])
         first, starts, hs, ts = (int(t) for t in meta[s])
         ord0, carry = first, T(0)
         for c in range(s * M, min(nch, (s + 1) * M)):
@@ -177,7 +178,10 @@ def rowseg_spmv(rs: dict, x: np.ndarray, m: int, f32: bool) -> np.ndarray:
                         head[ln] = run[ln]
                     seen[ln] |= f
                     o += int(f)
-                    p = T(vals[ln, j]) * x[int(words[ln, j]) & ((1 << 30) - 1)]
+                    col = int(words[ln, j]) & ((1 << 30) - 1)
+                    if words[ln, j] & (1 << 30):  # the CTA's window of x
+                        assert wb <= col < wb + W
+                    p = T(vals[ln, j]) * x[col]
                     run[ln] = p if f else T(run[ln] + p)
                 ordE[ln] = o
             sc = run.copy()

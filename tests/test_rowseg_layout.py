@@ -52,7 +52,8 @@ def test_rowseg_layout_decodes_to_oracle(name, coo, f32, warps):
     yref, ab = cd.oracle_spmm_ld(coo, x[None, :])
     err = np.abs(y.astype(np.float64)[None, :] - yref)
     assert np.all(err <= TOL[f32] * ab + 1e-300)
-    nch, M, nseg, nord = (int(v) for v in rs["sizes"])
+    nch, M, nseg, nord, G, W = (int(v) for v in rs["sizes"])
+    assert G == max(1, warps // 32) and W == (32768 if f32 else 16384)
     assert nseg == -(-nch // M) and nseg <= max(warps, 1) + 1
     # every stored value sits once in the stream, at its value position
     vp = rs["vpos"]
@@ -99,6 +100,6 @@ def test_rowseg_same_stream_after_plan_file(tmp_path, spmv_only):
     q = cbspmv.Plan.load(path)
     a, b = rowseg_arrays(p, 64), rowseg_arrays(q, 64)
     assert a is not None and b is not None
-    for k in ("sizes", "chunks", "meta", "spans", "rowmap", "empty"):
+    for k in ("sizes", "chunks", "meta", "spans", "rowmap", "empty", "wbase"):
         assert np.array_equal(a[k], b[k]), k
     assert b["vpos"].size == (0 if spmv_only else coo.nnz)
