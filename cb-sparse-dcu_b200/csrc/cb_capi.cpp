@@ -324,6 +324,7 @@ cbspmv_status upload_rowseg(DevSide &s, int kernel, cudaStream_t st) {
     d.W = R.W;
     d.wbase = static_cast<const int32_t *>(s.rs[8]);
     d.n = R.n;
+    d.unit = R.unit;
     s.rs_bytes = (int64_t)(R.chunks.size() + 4 * (R.meta.size() + R.spans.size() +
                                                   R.rowmap.size() + R.empty.size()));
     return CBSPMV_OK;

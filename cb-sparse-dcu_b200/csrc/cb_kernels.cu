@@ -791,7 +791,10 @@ cudaError_t launch_tiles(const DevLayout &d, const void *x, void *y, int nrhs,
                          int64_t ldx, int64_t ldy, cudaStream_t stream) {
     if (nrhs == 1 && ldx == 1 && ldy == 1 && use_pattern(d))
         return launch_pattern_v<T>(d, x, y, stream);
-    if (nrhs == 1 && ldx == 1 && ldy == 1 && d.rs.chunks && (d.kernel == 0 || d.kernel == 5))
+    // the row-segment stream: when chosen, and the automatic choice for
+    // all-COO layouts except the reference's small-direct case
+    if (nrhs == 1 && ldx == 1 && ldy == 1 && d.rs.chunks &&
+        (d.kernel == 5 || (d.kernel == 0 && !d.small_direct)))
         return launch_rowseg(d, x, y, stream);
     if (nrhs == 1 && ldx == 1 && ldy == 1 && use_stream(d))
         return launch_stream<T, BS>(d, x, y, stream);

@@ -24,6 +24,7 @@ struct RowSegDev {
     int32_t G = 0, W = 0;             // CTAs of every launch; window length (values)
     const int32_t *wbase = nullptr;   // per CTA: first column of its x window
     int64_t n = 0;                    // columns (length of x)
+    int unit = 0;                     // words only: every stored value is 1
 };
 
 // Device-resident pieces of one DeviceLayout (cb_layout.hpp).

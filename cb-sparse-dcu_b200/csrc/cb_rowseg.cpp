@@ -13,7 +13,7 @@ int64_t a16_64(int64_t x) { return (x + 15) & ~int64_t(15); }
 }  // namespace
 
 bool rowseg_applies(const DeviceLayout &L) {
-    if (L.unit || L.nvals <= 0 || L.n > kRsMaxCols || L.m >= (int64_t(1) << 31)) return false;
+    if (L.nvals <= 0 || L.n > kRsMaxCols || L.m >= (int64_t(1) << 31)) return false;
     for (const BlockDesc &b : L.blocks)
         if (meta_type(b.meta) != 0) return false;  // a CSR or DENSE block
     return true;
@@ -23,9 +23,11 @@ std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
     if (!rowseg_applies(L)) return "the layout does not take the row-segment stream";
     const int64_t m = L.m, C = rs_chunk_entries();
     const int f32 = L.f32;
-    const int64_t vsz = f32 ? 4 : 8, CB = rs_chunk_bytes(f32);
+    const int unit = L.unit;
+    const int64_t vsz = f32 ? 4 : 8, CB = rs_chunk_bytes(f32, unit);
     R = RowSegHost();
     R.f32 = f32;
+    R.unit = unit;
     R.m = m;
     R.n = L.n;
     // the entries of the tiles' COO sections (every block is a COO block):
@@ -40,7 +42,7 @@ std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
         for (const TileDesc &t : L.tiles) {
             const int64_t E = t.coo_entries, base = (int64_t)t.payload16 * 16;
             const uint32_t *idx = reinterpret_cast<const uint32_t *>(L.payload.data() + base);
-            const int64_t vals = base + a16_64(4 * E);
+            const int64_t vals = base + a16_64(4 * E);  // (none when unit)
             for (int64_t q = 0; q < E; ++q, ++k) {
                 erow[(size_t)k] = (int32_t)((int64_t)t.block_row * L.bs + (idx[q] >> kColBits));
                 ecol[(size_t)k] = (int32_t)(idx[q] & ((1u << kColBits) - 1));
@@ -90,8 +92,9 @@ std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
             ord += st;
             start[(size_t)e] = st;
             word = (uint32_t)ecol[v] | (st ? kRsStart : 0u);
-            std::memcpy(R.chunks.data() + rs_value_offset(e, f32),
-                        L.payload.data() + eoff[v], (size_t)vsz);
+            if (!unit)
+                std::memcpy(R.chunks.data() + rs_value_offset(e, f32),
+                            L.payload.data() + eoff[v], (size_t)vsz);
             eoff[v] = -1 - e;  // from here on: the entry's place in the stream
         } else {
             const bool st = e == nv;
@@ -172,7 +175,7 @@ std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
     // per stored value (device order) its stream entry, for value updates:
     // stored value v sits at payload offset val_off[v] (absent from plans
     // loaded from SpMV-only files, which take no new values)
-    if ((int64_t)L.val_off.size() == nv) {
+    if (!unit && (int64_t)L.val_off.size() == nv) {
         std::vector<std::pair<int64_t, int32_t>> by_off((size_t)nv);
         {
             int64_t k = 0;

@@ -52,7 +52,10 @@ constexpr int64_t kRsWindowBytes = int64_t(128) << 10;
 constexpr int64_t kRsMaxCols = int64_t(1) << 30;
 
 inline int rs_chunk_entries() { return 32 * kRsK; }
-inline int64_t rs_chunk_bytes(int f32) { return 32 * kRsK * (4 + (f32 ? 4 : 8)); }
+// unit-valued layouts (every stored value 1) keep no values: words only
+inline int64_t rs_chunk_bytes(int f32, int unit = 0) {
+    return 32 * kRsK * (4 + (unit ? 0 : f32 ? 4 : 8));
+}
 
 // Byte offset, inside the chunk buffer, of the value of stream entry e.
 inline int64_t rs_value_offset(int64_t e, int f32) {
@@ -64,6 +67,7 @@ inline int64_t rs_value_offset(int64_t e, int f32) {
 
 struct RowSegHost {
     int f32 = 0;
+    int unit = 0;           // no values in the chunks (every stored value is 1)
     int64_t m = 0, n = 0;
     int32_t nch = 0;        // chunks
     int32_t M = 0;          // chunks per segment
@@ -82,8 +86,8 @@ struct RowSegHost {
     int64_t alg_bytes = 0;
 };
 
-// Whether the layout takes the row-segment stream: stored values, every
-// block a COO block, columns below 2^30, rows below 2^31.
+// Whether the layout takes the row-segment stream: every block a COO block,
+// columns below 2^30, rows below 2^31.
 bool rowseg_applies(const DeviceLayout &L);
 
 // Builds the stream from the tiles' COO sections (row, column and value of

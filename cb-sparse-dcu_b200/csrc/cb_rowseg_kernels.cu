@@ -91,12 +91,12 @@ __device__ __forceinline__ void rs_arrive(const RowSegDev &rs, T *__restrict__ y
     }
 }
 
-template <typename T>
+template <typename T, bool UNIT>
 __global__ void __launch_bounds__(kRsWarps * 32, 1)
     cb_rowseg_kernel(const RowSegDev rs, const T *__restrict__ x, T *__restrict__ y) {
     using V = typename RsVec<T>::V;
     constexpr int K = kRsK, NV = RsVec<T>::n;
-    constexpr int64_t CB = 32 * K * (4 + (int64_t)sizeof(T));
+    constexpr int64_t CB = 32 * K * (4 + (UNIT ? 0 : (int64_t)sizeof(T)));
     extern __shared__ __align__(16) unsigned char rs_smem[];
     T *xs = reinterpret_cast<T *>(rs_smem);  // x[wb .. wb + W)
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -121,8 +121,10 @@ __global__ void __launch_bounds__(kRsWarps * 32, 1)
         const V *gv = reinterpret_cast<const V *>(rs.chunks + (int64_t)c * CB + 32 * K * 4);
 #pragma unroll
         for (int q = 0; q < K / 4; ++q) nw[q] = ld_stream(gw + q * 32 + lane, pol);
+        if (!UNIT) {
 #pragma unroll
-        for (int q = 0; q < K / NV; ++q) nv[q] = ld_stream(gv + q * 32 + lane, pol);
+            for (int q = 0; q < K / NV; ++q) nv[q] = ld_stream(gv + q * 32 + lane, pol);
+        }
     };
     auto rid = [&](int32_t o) { return rs.rowmap ? __ldg(&rs.rowmap[o]) : o; };
     int c = s * M;
@@ -145,8 +147,13 @@ __global__ void __launch_bounds__(kRsWarps * 32, 1)
                 w[4 * q + 2] = nw[q].z;
                 w[4 * q + 3] = nw[q].w;
             }
+            if (UNIT) {
 #pragma unroll
-            for (int q = 0; q < K / NV; ++q) unpack(nv[q], v + q * NV);
+                for (int j = 0; j < K; ++j) v[j] = T(1);
+            } else {
+#pragma unroll
+                for (int q = 0; q < K / NV; ++q) unpack(nv[q], v + q * NV);
+            }
             {  // the next chunk of this segment, or the first of the warp's next
                 int cn = c + 1;
                 if (cn >= cend) {
@@ -243,15 +250,28 @@ __global__ void cb_rowseg_values_kernel(const RowSegDev rs, const uint8_t *__res
 
 }  // namespace
 
-template <typename T>
+template <typename T, bool UNIT>
 const void *rowseg_fn() {
-    return reinterpret_cast<const void *>(cb_rowseg_kernel<T>);
+    return reinterpret_cast<const void *>(cb_rowseg_kernel<T, UNIT>);
+}
+
+template <typename T, bool UNIT>
+cudaError_t launch_rowseg_t(const DevLayout &d, const void *x, void *y, size_t smem,
+                            cudaStream_t stream) {
+    const void *fn = rowseg_fn<T, UNIT>();
+    cudaError_t e = dev_enable_smem(fn, smem);
+    if (e != cudaSuccess) return e;
+    dev_resident_l1(fn, kRsWarps * 32, smem);  // sets the carveout
+    // the grid the segments and windows were assigned for
+    cb_rowseg_kernel<T, UNIT><<<(unsigned)d.rs.G, kRsWarps * 32, smem, stream>>>(
+        d.rs, static_cast<const T *>(x), static_cast<T *>(y));
+    return cudaSuccess;
 }
 
 int64_t rowseg_warps(int f32) {
     // the x window in shared memory; the carveout leaves the rest of the
     // unified L1/shared memory to the L1 (the other x gathers)
-    const void *fn = f32 ? rowseg_fn<float>() : rowseg_fn<double>();
+    const void *fn = f32 ? rowseg_fn<float, false>() : rowseg_fn<double, false>();
     if (dev_enable_smem(fn, (size_t)kRsWindowBytes) != cudaSuccess) {
         cudaGetLastError();
         return 0;
@@ -264,18 +284,12 @@ cudaError_t launch_rowseg(const DevLayout &d, const void *x, void *y, cudaStream
     if (!d.rs.chunks || d.rs.nseg <= 0 || d.rs.G <= 0 || !d.rs.wbase)
         return cudaErrorInvalidValue;
     const size_t smem = (size_t)d.rs.W * (d.f32 ? 4 : 8);
-    const void *fn = d.f32 ? rowseg_fn<float>() : rowseg_fn<double>();
-    cudaError_t e = dev_enable_smem(fn, smem);
+    const cudaError_t e =
+        d.f32 ? (d.rs.unit ? launch_rowseg_t<float, true>(d, x, y, smem, stream)
+                           : launch_rowseg_t<float, false>(d, x, y, smem, stream))
+              : (d.rs.unit ? launch_rowseg_t<double, true>(d, x, y, smem, stream)
+                           : launch_rowseg_t<double, false>(d, x, y, smem, stream));
     if (e != cudaSuccess) return e;
-    dev_resident_l1(fn, kRsWarps * 32, smem);  // sets the carveout
-    // the grid the segments and windows were assigned for
-    const unsigned grid = (unsigned)d.rs.G;
-    if (d.f32)
-        cb_rowseg_kernel<float><<<grid, kRsWarps * 32, smem, stream>>>(
-            d.rs, static_cast<const float *>(x), static_cast<float *>(y));
-    else
-        cb_rowseg_kernel<double><<<grid, kRsWarps * 32, smem, stream>>>(
-            d.rs, static_cast<const double *>(x), static_cast<double *>(y));
     note_launch();
     return cudaGetLastError();
 }

@@ -128,7 +128,8 @@ def rowseg_spmv(rs: dict, x: np.ndarray, m: int, f32: bool) -> np.ndarray:
     x = np.asarray(x, T)
     nch, M, nseg, nord, G, W = (int(v) for v in rs["sizes"])
     vsz = 4 if f32 else 8
-    CB = C * (4 + vsz)
+    CB = rs["chunks"].size // max(nch, 1)
+    unit = CB == 4 * C  # words only: every stored value is 1
     chunks = rs["chunks"].reshape(nch, CB)
     meta = rs["meta"].reshape(-1, 4)
     spans = rs["spans"].reshape(-1, 4)
@@ -160,7 +161,8 @@ def rowseg_spmv(rs: dict, x: np.ndarray, m: int, f32: bool) -> np.ndarray:
         ord0, carry = first, T(0)
         for c in range(s * M, min(nch, (s + 1) * M)):
             words = chunks[c, :4 * C].view(np.uint32).reshape(32, K)
-            vals = chunks[c, 4 * C:].view(T)[vpos].reshape(32, K)
+            vals = (np.ones((32, K), T) if unit
+                    else chunks[c, 4 * C:].view(T)[vpos].reshape(32, K))
             flags = (words >> 31).astype(np.int64)
             cntl = flags.sum(axis=1)
             ordS = ord0 + np.cumsum(cntl) - cntl

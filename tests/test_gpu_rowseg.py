@@ -31,7 +31,8 @@ def _cases():
            ("dups", gen.random_small(rng, 1200, 1000, 9000, dup=True)),
            ("wide", gen.random_small(rng, 300, 200000, 30000)),
            ("tall", gen.random_small(rng, 200000, 300, 30000)),
-           ("power-law", gen.power_law(1 << 15, seed=3))]
+           ("power-law", gen.power_law(1 << 15, seed=3)),
+           ("unit", gen.random_small(rng, 3000, 2500, 40000, unit=True))]
     # one row of 60000 entries (one per 16x16 block: COO blocks) crossing
     # many segments, and every ninth row of the rest non-empty
     n = 16 * 60000
