@@ -231,7 +231,7 @@ def secondary_configs(dev, peak: float, want=("lap", "pl32", "st", "diff", "bat"
     flush = lambda: l2_flush.zero_()  # noqa: E731
     out = {}
 
-    def single(name, coo, f32, reps=50):
+    def single(name, coo, f32, reps=50, bsr=False):
         plan = cbspmv.Plan(coo, value_type=int(f32))
         kernel, _ = plan.autotune(1)
         dt = torch.float32 if f32 else torch.float64
@@ -252,6 +252,14 @@ def secondary_configs(dev, peak: float, want=("lap", "pl32", "st", "diff", "bat"
                      "parity": _parity(y.cpu().numpy()[None, :], yref, ab, f32),
                      "l2": "flushed before each step" if small else "inputs larger than L2"}
         del plan
+        if bsr and not f32:
+            try:
+                c = bsr_comparator(coo, xh, dev)
+                if c["ms"]:
+                    c["this_library_speedup"] = round(c["ms"] / ms, 2)
+                out[name]["comparator_bsr"] = c
+            except Exception as exc:  # the comparator is informative only
+                out[name]["comparator_bsr"] = {"unavailable": str(exc)[:200]}
 
     if "lap" in want:
         single("LAP fp64 (256^2 5-point)", gen.laplacian_2d(), False)
@@ -264,7 +272,7 @@ def secondary_configs(dev, peak: float, want=("lap", "pl32", "st", "diff", "bat"
         del pl
     if "st" in want:
         st = gen.stencil_27pt()
-        single("ST fp64 (64^3 x 3 dof 27-point)", st, False, reps=20)
+        single("ST fp64 (64^3 x 3 dof 27-point)", st, False, reps=20, bsr=True)
         single("ST fp32 (64^3 x 3 dof 27-point)", st, True, reps=20)
         del st
     if "diff" in want:
@@ -272,6 +280,98 @@ def secondary_configs(dev, peak: float, want=("lap", "pl32", "st", "diff", "bat"
     if "bat" in want:
         bat_config(dev, peak, bat_count, out)
     return out
+
+
+def _cusparse():
+    """The cuSPARSE library torch loads (a comparator only)."""
+    import torch
+    here = pathlib.Path(torch.__file__).parent.parent / "nvidia" / "cusparse" / "lib"
+    for cand in (here / "libcusparse.so.12", "libcusparse.so.12"):
+        try:
+            return ctypes.CDLL(str(cand))
+        except OSError:
+            continue
+    raise OSError("libcusparse.so.12 not found")
+
+
+def bsr_comparator(coo, xh, dev, sizes=(2, 4, 8, 16)):
+    """cuSPARSE BSR SpMV on the same matrix, FP64: the analogue of the
+    reference's hipSPARSE BSR baseline (cb-spmv-dcu/benchmark/hipSparse-bsr/
+    main.hip.cpp:99-187): CSR converted to BSR on the device (csr2bsr,
+    row-major blocks) for block sizes 2, 4, 8 and 16, each timed with bsrmv,
+    the fastest reported.  Its y is checked against the oracle's."""
+    import numpy as np
+    import torch
+    cd = _oracle()
+    lib = _cusparse()
+    P, I = ctypes.c_void_p, ctypes.c_int
+    lib.cusparseCreate.argtypes = [ctypes.POINTER(P)]
+    lib.cusparseSetStream.argtypes = [P, P]
+    lib.cusparseCreateMatDescr.argtypes = [ctypes.POINTER(P)]
+    lib.cusparseDestroyMatDescr.argtypes = [P]
+    lib.cusparseDestroy.argtypes = [P]
+    lib.cusparseXcsr2bsrNnz.argtypes = [P, I, I, I, P, P, P, I, P, P, ctypes.POINTER(I)]
+    lib.cusparseDcsr2bsr.argtypes = [P, I, I, I, P, P, P, P, I, P, P, P, P]
+    lib.cusparseDbsrmv.argtypes = [P, I, I, I, I, I, ctypes.POINTER(ctypes.c_double), P, P, P,
+                                   P, I, P, ctypes.POINTER(ctypes.c_double), P]
+    m, n = coo.m, coo.n
+    crow = np.zeros(m + 1, np.int64)
+    np.add.at(crow, coo.row.astype(np.int64) + 1, 1)
+    crow_d = torch.from_numpy(np.cumsum(crow).astype(np.int32)).to(dev)
+    col_d = torch.from_numpy(coo.col.astype(np.int32)).to(dev)
+    val_d = torch.from_numpy(coo.val.astype(np.float64)).to(dev)
+    yref, ab = cd.oracle_spmm_ld(coo, xh[None, :])
+    h, dA, dC = P(), P(), P()
+    ok = lambda rc, what: None if rc == 0 else (_ for _ in ()).throw(  # noqa: E731
+        RuntimeError(f"{what}: cusparse status {rc}"))
+    ok(lib.cusparseCreate(ctypes.byref(h)), "create")
+    ok(lib.cusparseSetStream(h, P(torch.cuda.current_stream().cuda_stream)), "stream")
+    ok(lib.cusparseCreateMatDescr(ctypes.byref(dA)), "descr")
+    ok(lib.cusparseCreateMatDescr(ctypes.byref(dC)), "descr")
+    alpha, beta = ctypes.c_double(1.0), ctypes.c_double(0.0)
+    per = {}
+    try:
+        for bd in sizes:
+            mb, nb = (m + bd - 1) // bd, (n + bd - 1) // bd
+            xp = torch.zeros(nb * bd, dtype=torch.float64, device=dev)
+            xp[:n] = torch.from_numpy(xh).to(dev)
+            yp = torch.empty(mb * bd, dtype=torch.float64, device=dev)
+            rowp = torch.empty(mb + 1, dtype=torch.int32, device=dev)
+            nnzb = I(0)
+            ok(lib.cusparseXcsr2bsrNnz(h, 0, m, n, dA, P(crow_d.data_ptr()), P(col_d.data_ptr()),
+                                       bd, dC, P(rowp.data_ptr()), ctypes.byref(nnzb)), "nnz")
+            torch.cuda.synchronize()
+            nbytes = nnzb.value * bd * bd * 8
+            if nbytes > (48 << 30):
+                per[bd] = {"skipped": f"{nbytes / 2**30:.0f} GiB of blocks"}
+                continue
+            colb = torch.empty(max(nnzb.value, 1), dtype=torch.int32, device=dev)
+            valb = torch.empty(max(nnzb.value * bd * bd, 1), dtype=torch.float64, device=dev)
+            ok(lib.cusparseDcsr2bsr(h, 0, m, n, dA, P(val_d.data_ptr()), P(crow_d.data_ptr()),
+                                    P(col_d.data_ptr()), bd, dC, P(valb.data_ptr()),
+                                    P(rowp.data_ptr()), P(colb.data_ptr())), "csr2bsr")
+
+            def mv():
+                ok(lib.cusparseDbsrmv(h, 0, 0, mb, nb, nnzb.value, ctypes.byref(alpha), dC,
+                                      P(valb.data_ptr()), P(rowp.data_ptr()),
+                                      P(colb.data_ptr()), bd, P(xp.data_ptr()),
+                                      ctypes.byref(beta), P(yp.data_ptr())), "bsrmv")
+            ms = _timed(mv, 50, 5)
+            torch.cuda.synchronize()
+            err = float(np.max(np.abs(yp[:m].cpu().numpy() - yref[0]) / (ab[0] + 1e-300)))
+            per[bd] = {"ms": round(ms, 4), "blocks": nnzb.value,
+                       "block_bytes": nbytes, "max_err_rowscaled": float(f"{err:.3g}")}
+            del colb, valb, xp, yp, rowp
+            torch.cuda.empty_cache()
+    finally:
+        lib.cusparseDestroyMatDescr(dA)
+        lib.cusparseDestroyMatDescr(dC)
+        lib.cusparseDestroy(h)
+    timed = {k: v for k, v in per.items() if "ms" in v}
+    best = min(timed, key=lambda k: timed[k]["ms"]) if timed else None
+    return {"library": "cuSPARSE BSR SpMV (csr2bsr + bsrmv, FP64, row-major blocks)",
+            "block_sizes": per, "best_block": best,
+            "ms": timed[best]["ms"] if best else None}
 
 
 def diff_config(dev, peak, flush, out):
@@ -693,6 +793,15 @@ def main():
             del A
         except Exception as exc:  # the comparator is informative only
             comparator = {"unavailable": str(exc)[:200]}
+    # and cuSPARSE BSR (the reference's own library baseline is hipSPARSE BSR)
+    if rank == 0 and world == 1 and args.configs != "none":
+        try:
+            cb = bsr_comparator(coo, x_host, dev)
+            if cb["ms"]:
+                cb["this_library_speedup"] = round(cb["ms"] / ms, 2)
+            comparator = {"csr": comparator, "bsr": cb}
+        except Exception as exc:
+            comparator = {"csr": comparator, "bsr": {"unavailable": str(exc)[:200]}}
 
     line = None
     configs = None
