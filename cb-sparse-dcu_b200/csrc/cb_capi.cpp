@@ -301,7 +301,8 @@ cbspmv_status upload_rowseg(DevSide &s, int kernel, cudaStream_t st) {
     if (!R.spans.empty())
         CB_CUDA(upload_vec(R.spans, (int32_t **)&s.rs[2], st), "upload row segments");
     CB_CUDA(upload_vec(zeros, (int32_t **)&s.rs[3], st), "upload row segments");
-    CB_CUDA(cudaMalloc(&s.rs[4], 2 * (size_t)R.nseg * vsz), "allocate row-segment slots");
+    CB_CUDA(cudaMalloc(&s.rs[4], 2 * (size_t)R.nseg * cb::kRsSlotValues * vsz),
+            "allocate row-segment slots");
     CB_CUDA(upload_vec(R.rowmap, (int32_t **)&s.rs[5], st), "upload row segments");
     CB_CUDA(upload_vec(R.empty, (int32_t **)&s.rs[6], st), "upload row segments");
     CB_CUDA(upload_vec(R.vpos, (int32_t **)&s.rs[7], st), "upload row segments");
@@ -722,6 +723,7 @@ cbspmv_status cbspmv_autotune_ex(cbspmv_plan *p, int nrhs, void *stream, int *ke
         if (s.d.rs.chunks) cands.push_back({5, 0});
     } else {
         for (int rl : {0, 1, 2, 4}) cands.push_back({3, rl});
+        if (s.d.rs.chunks) cands.push_back({5, 0});
     }
     const size_t vsz = vsize(p);
     void *x = nullptr, *y = nullptr;

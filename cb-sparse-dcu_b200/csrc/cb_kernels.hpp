@@ -154,6 +154,11 @@ cudaError_t launch_pattern(const DevLayout &d, const void *x, void *y, cudaStrea
 // (after the payload's values changed).
 int64_t rowseg_warps(int f32);
 cudaError_t launch_rowseg(const DevLayout &d, const void *x, void *y, cudaStream_t stream);
+// Y = A X over d.rs for nrhs right-hand sides (row-major, leading dims ldx,
+// ldy; slabs of 16 per launch); partial slots hold 16 values.
+constexpr int kRsSlotValues = 16;
+cudaError_t launch_rowseg_mrhs(const DevLayout &d, const void *x, void *y, int nrhs,
+                               int64_t ldx, int64_t ldy, cudaStream_t stream);
 cudaError_t launch_rowseg_values(const DevLayout &d, int64_t nvals, const uint64_t *val_off,
                                  cudaStream_t stream);
 

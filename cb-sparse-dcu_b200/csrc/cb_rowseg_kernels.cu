@@ -230,6 +230,213 @@ __global__ void __launch_bounds__(kRsWarps * 32, 1)
     }
 }
 
+// Several right-hand sides over the same stream: G lanes per entry, lane q
+// of a group holding the V = 16 / sizeof(T) right-hand sides q*V .. q*V+V-1
+// of its rows; P = 32 / G groups per warp, group p taking the 4G consecutive
+// entries 4Gp .. 4Gp+4G-1 of each chunk (the entries lanes Gp .. Gp+G-1 take
+// in the one-vector kernel).  A group walks its entries in steps of 4: the
+// step's words and values are loaded by every lane of the group (one 16-byte
+// access, broadcast), its four x rows gathered (one 16-byte load per lane
+// and entry), then added along the rows in registers.  Row starts are
+// counted per group and scanned over the groups; one segmented scan over the
+// groups joins rows across groups.  No x window (the window holds single
+// vectors).
+constexpr int kRsMaxRhs = kRsSlotValues;  // right-hand sides per launch (slots hold this many)
+
+template <typename T, int G, bool UNIT>
+__global__ void __launch_bounds__(kRsWarps * 32, 1)
+    cb_rowseg_mrhs_kernel(const RowSegDev rs, const T *__restrict__ x, T *__restrict__ y,
+                          int nrhs, int64_t ldx, int64_t ldy, int xvec, int yvec) {
+    using VT = typename RsVec<T>::V;
+    constexpr int V = RsVec<T>::n, P = 32 / G, NV = RsVec<T>::n;
+    constexpr int64_t CB = 128 * (4 + (UNIT ? 0 : (int64_t)sizeof(T)));
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int p = lane / G, q = lane % G, c0 = q * V;
+    const unsigned gmask = (G == 32 ? kFull : ((1u << G) - 1u)) << (p * G);
+    {  // rows without entries
+        const int64_t total = (int64_t)rs.nempty * nrhs;
+        for (int64_t i = ((int64_t)blockIdx.x * kRsWarps + wib) * 32 + lane; i < total;
+             i += (int64_t)gridDim.x * kRsWarps * 32)
+            y[(int64_t)__ldg(&rs.empty[i / nrhs]) * ldy + i % nrhs] = T(0);
+    }
+    const int NB = gridDim.x, b = blockIdx.x;
+    const int sb0 = (int)((int64_t)b * rs.nseg / NB);
+    const int sb1 = (int)((int64_t)(b + 1) * rs.nseg / NB);
+    int s = sb0 + wib;
+    if (s >= sb1) return;
+    const int M = rs.M, nch = rs.nch, nord = rs.nord;
+    const uint64_t pol = dev::policy_evict_first();
+    auto rid = [&](int32_t o) -> int64_t { return rs.rowmap ? __ldg(&rs.rowmap[o]) : o; };
+    auto load_x = [&](uint32_t col, T *o) {
+        const T *px = x + (int64_t)col * ldx + c0;
+        if (xvec) {
+            if (c0 < nrhs) unpack(__ldg(reinterpret_cast<const VT *>(px)), o);
+            else
+#pragma unroll
+                for (int k = 0; k < V; ++k) o[k] = T(0);
+        } else {
+#pragma unroll
+            for (int k = 0; k < V; ++k) o[k] = c0 + k < nrhs ? __ldg(px + k) : T(0);
+        }
+    };
+    auto store_y = [&](int64_t row, const T *v) {
+        T *py = y + row * ldy + c0;
+        if (yvec && c0 + V <= nrhs) {
+            VT t;
+            T *tv = reinterpret_cast<T *>(&t);
+#pragma unroll
+            for (int k = 0; k < V; ++k) tv[k] = v[k];
+            *reinterpret_cast<VT *>(py) = t;
+        } else {
+#pragma unroll
+            for (int k = 0; k < V; ++k)
+                if (c0 + k < nrhs) py[k] = v[k];
+        }
+    };
+    // a row across segments: every lane of the group writes its columns of
+    // the slot; lane 0 of the group takes the arrival; the last part's group
+    // adds the slots in segment order and stores y
+    auto arrive = [&](int span, const T *v, int slot) {
+        T *part = static_cast<T *>(rs.part);
+#pragma unroll
+        for (int k = 0; k < V; ++k)
+            if (c0 + k < nrhs) part[(int64_t)slot * kRsMaxRhs + c0 + k] = v[k];
+        __threadfence();
+        __syncwarp(gmask);
+        int last = 0;
+        const int4 sp = __ldg(&rs.spans[span]);
+        if (q == 0) {
+            cuda::atomic_ref<int32_t, cuda::thread_scope_device> ctr(rs.counters[span]);
+            last = ctr.fetch_add(1, cuda::memory_order_acq_rel) + 1 == sp.y - sp.x + 1;
+            if (last) ctr.store(0, cuda::memory_order_relaxed);
+        }
+        last = __shfl_sync(gmask, last, p * G);
+        if (last) {
+            __threadfence();
+            T tot[V];
+#pragma unroll
+            for (int k = 0; k < V; ++k)
+                tot[k] = c0 + k < nrhs ? __ldcg(&part[(int64_t)(2 * sp.x + 1) * kRsMaxRhs + c0 + k])
+                                       : T(0);
+            for (int w = sp.x + 1; w <= sp.y; ++w)
+#pragma unroll
+                for (int k = 0; k < V; ++k)
+                    if (c0 + k < nrhs) tot[k] += __ldcg(&part[(int64_t)(2 * w) * kRsMaxRhs + c0 + k]);
+            store_y(rid(sp.z), tot);
+        }
+    };
+    while (true) {
+        const int4 meta = __ldg(&rs.meta[s]);
+        const int32_t first = meta.x;
+        int32_t ord0 = meta.x;
+        T carry[V];
+#pragma unroll
+        for (int k = 0; k < V; ++k) carry[k] = T(0);
+        const int cbeg = s * M, cend = min(nch, cbeg + M);
+        for (int c = cbeg; c < cend; ++c) {
+            const uint4 *gw = reinterpret_cast<const uint4 *>(rs.chunks + (int64_t)c * CB);
+            const uint8_t *gv = rs.chunks + (int64_t)c * CB + 4 * 128;
+            // row starts of the group's entries: each lane counts one
+            // 4-entry step, the group adds them
+            int cnt;
+            {
+                const uint4 t = __ldg(gw + G * p + q);
+                cnt = (int)((t.x >> 31) + (t.y >> 31) + (t.z >> 31) + (t.w >> 31));
+#pragma unroll
+                for (int d = 1; d < G; d <<= 1) cnt += __shfl_xor_sync(kFull, cnt, d);
+            }
+            int inc = cnt;  // inclusive scan over the groups
+#pragma unroll
+            for (int d = 1; d < P; d <<= 1) {
+                const int t = __shfl_up_sync(kFull, inc, d * G);
+                if (p >= d) inc += t;
+            }
+            const int32_t ordS = ord0 + inc - cnt;  // the row this group starts in
+            int32_t ord = ordS;
+            T run[V], head[V];
+#pragma unroll
+            for (int k = 0; k < V; ++k) run[k] = head[k] = T(0);
+            bool seen = false;
+#pragma unroll 1
+            for (int i = 0; i < G; ++i) {
+                const int ls = G * p + i;  // the one-vector lane whose 4 entries these are
+                const uint4 t = __ldg(gw + ls);
+                const uint32_t w[4] = {t.x, t.y, t.z, t.w};
+                T v[4];
+                if (UNIT) {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) v[j] = T(1);
+                } else if (NV == 4) {
+                    unpack(ld_stream(reinterpret_cast<const VT *>(gv) + ls, pol), v);
+                } else {
+                    unpack(ld_stream(reinterpret_cast<const VT *>(gv) + ls, pol), v);
+                    unpack(ld_stream(reinterpret_cast<const VT *>(gv) + 32 + ls, pol), v + 2);
+                }
+                T xv[4][V];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) load_x(w[j] & kRsColMask, xv[j]);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const bool f = (w[j] >> 31) != 0;
+                    if (f && seen) store_y(rid(ord), run);  // a row whole inside the group
+#pragma unroll
+                    for (int k = 0; k < V; ++k) {
+                        head[k] = (f && !seen) ? run[k] : head[k];
+                        run[k] = fma(v[j], xv[j][k], f ? T(0) : run[k]);
+                    }
+                    seen = seen || f;
+                    ord += f ? 1 : 0;
+                }
+            }
+            // rows across groups: inclusive scan over the groups, reset at
+            // groups holding a row start; group 0 continues the previous chunk
+            T sc[V];
+#pragma unroll
+            for (int k = 0; k < V; ++k) sc[k] = (p == 0 && !seen) ? run[k] + carry[k] : run[k];
+            bool r = seen;
+#pragma unroll
+            for (int d = 1; d < P; d <<= 1) {
+                const bool ru = __shfl_up_sync(kFull, (int)r, d * G) != 0;
+#pragma unroll
+                for (int k = 0; k < V; ++k) {
+                    const T su = __shfl_up_sync(kFull, sc[k], d * G);
+                    if (p >= d && !r) sc[k] += su;
+                }
+                if (p >= d) r = r || ru;
+            }
+            T cin[V];
+#pragma unroll
+            for (int k = 0; k < V; ++k) {
+                const T t = __shfl_up_sync(kFull, sc[k], G);
+                cin[k] = p == 0 ? carry[k] : t;
+            }
+            if (seen) {  // the row this group started in ends here
+                T val[V];
+#pragma unroll
+                for (int k = 0; k < V; ++k) val[k] = cin[k] + head[k];
+                if (ordS == first && meta.z >= 0)
+                    arrive(meta.z, val, 2 * s);
+                else if (!(ordS == first && meta.y) && ordS < nord)
+                    store_y(rid(ordS), val);
+            }
+#pragma unroll
+            for (int k = 0; k < V; ++k) carry[k] = __shfl_sync(kFull, sc[k], (P - 1) * G + q);
+            ord0 = __shfl_sync(kFull, ord, (P - 1) * G);
+        }
+        // the segment's last row: a span's part, or whole here (group 0)
+        if (p == 0) {
+            if (ord0 == first && meta.z >= 0)
+                arrive(meta.z, carry, 2 * s);
+            else if (meta.w >= 0)
+                arrive(meta.w, carry, 2 * s + 1);
+            else if (ord0 < nord && !(ord0 == first && meta.y))
+                store_y(rid(ord0), carry);
+        }
+        s += kRsWarps;
+        if (s >= sb1) break;
+    }
+}
+
 // Stream values refreshed from the tile payload: chunks[value of entry
 // vpos[v]] = payload value v.
 template <typename T>
@@ -292,6 +499,55 @@ cudaError_t launch_rowseg(const DevLayout &d, const void *x, void *y, cudaStream
     if (e != cudaSuccess) return e;
     note_launch();
     return cudaGetLastError();
+}
+
+template <typename T, int G, bool UNIT>
+cudaError_t launch_mrhs_g(const DevLayout &d, const T *x, T *y, int r, int64_t ldx, int64_t ldy,
+                          int xvec, int yvec, cudaStream_t stream) {
+    const void *fn = reinterpret_cast<const void *>(cb_rowseg_mrhs_kernel<T, G, UNIT>);
+    dev_resident_l1(fn, kRsWarps * 32, 0);  // sets the carveout: all L1
+    cb_rowseg_mrhs_kernel<T, G, UNIT><<<(unsigned)d.rs.G, kRsWarps * 32, 0, stream>>>(
+        d.rs, x, y, r, ldx, ldy, xvec, yvec);
+    note_launch();
+    return cudaGetLastError();
+}
+
+template <typename T, bool UNIT>
+cudaError_t launch_mrhs_t(const DevLayout &d, const T *x, T *y, int nrhs, int64_t ldx,
+                          int64_t ldy, cudaStream_t stream) {
+    constexpr int V = 16 / sizeof(T);
+    // slabs of at most kRsMaxRhs right-hand sides, one launch each
+    for (int c = 0; c < nrhs; c += kRsMaxRhs) {
+        const int r = std::min(kRsMaxRhs, nrhs - c);
+        const int xvec = ldx % V == 0 && reinterpret_cast<uintptr_t>(x + c) % 16 == 0;
+        const int yvec = ldy % V == 0 && reinterpret_cast<uintptr_t>(y + c) % 16 == 0;
+        int g = 1;
+        while (g * V < r) g *= 2;
+        cudaError_t e;
+        switch (g) {
+            case 1: e = launch_mrhs_g<T, 1, UNIT>(d, x + c, y + c, r, ldx, ldy, xvec, yvec, stream); break;
+            case 2: e = launch_mrhs_g<T, 2, UNIT>(d, x + c, y + c, r, ldx, ldy, xvec, yvec, stream); break;
+            case 4: e = launch_mrhs_g<T, 4, UNIT>(d, x + c, y + c, r, ldx, ldy, xvec, yvec, stream); break;
+            default: e = launch_mrhs_g<T, (16 / sizeof(T) == 2 ? 8 : 4), UNIT>(
+                         d, x + c, y + c, r, ldx, ldy, xvec, yvec, stream);
+        }
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_rowseg_mrhs(const DevLayout &d, const void *x, void *y, int nrhs,
+                               int64_t ldx, int64_t ldy, cudaStream_t stream) {
+    if (!d.rs.chunks || d.rs.nseg <= 0 || d.rs.G <= 0 || nrhs < 1) return cudaErrorInvalidValue;
+    if (d.f32)
+        return d.rs.unit ? launch_mrhs_t<float, true>(d, static_cast<const float *>(x),
+                                                      static_cast<float *>(y), nrhs, ldx, ldy, stream)
+                         : launch_mrhs_t<float, false>(d, static_cast<const float *>(x),
+                                                       static_cast<float *>(y), nrhs, ldx, ldy, stream);
+    return d.rs.unit ? launch_mrhs_t<double, true>(d, static_cast<const double *>(x),
+                                                   static_cast<double *>(y), nrhs, ldx, ldy, stream)
+                     : launch_mrhs_t<double, false>(d, static_cast<const double *>(x),
+                                                    static_cast<double *>(y), nrhs, ldx, ldy, stream);
 }
 
 cudaError_t launch_rowseg_values(const DevLayout &d, int64_t nvals, const uint64_t *val_off,

@@ -127,3 +127,44 @@ def test_rowseg_set_values_and_transpose(cuda, f32):
     y2 = plan.spmv(xd)
     torch.cuda.synchronize()
     _check(y2.cpu().numpy()[None, :], yref, ab, f32, f"autotuned kernel {k}")
+
+
+@pytest.mark.parametrize("name", ["random", "huge-row-empty-rows", "entries-5121", "power-law",
+                                  "unit"])
+@pytest.mark.parametrize("f32", [False, True])
+@pytest.mark.parametrize("nrhs", [2, 3, 5, 8, 13, 16, 20])
+def test_rowseg_several_rhs(cuda, name, f32, nrhs):
+    """Several right-hand sides over the stream (lanes per entry chosen from
+    nrhs; more than 16 in slabs of 16), against the oracle; with leading
+    dimensions wider than nrhs (no vector loads) through the C ABI."""
+    import ctypes
+    import torch
+    import cbspmv
+    import cbdump as cd
+    from cbspmv import gen
+    coo = dict(CASES)[name]
+    plan = cbspmv.Plan(coo, value_type=int(f32))
+    X = gen.uniform_x(coo.n, 7, nrhs=nrhs)  # (nrhs, n)
+    if f32:
+        X = X.astype(np.float32).astype(np.float64)
+    dt = torch.float32 if f32 else torch.float64
+    Xd = torch.from_numpy(np.ascontiguousarray(X.T)).to(cuda, dt)
+    Y = plan.spmv(Xd)
+    assert plan.info()["rowseg_bytes"] > 0
+    torch.cuda.synchronize()
+    yref, ab = cd.oracle_spmm_ld(coo, X)
+    _check(Y.cpu().numpy().T, yref, ab, f32, f"{name} nrhs {nrhs}")
+    # padded leading dimensions
+    ldx, ldy = nrhs + 3, nrhs + 5
+    Xp = torch.zeros(coo.n, ldx, dtype=dt, device=cuda)
+    Xp[:, :nrhs] = Xd
+    Yp = torch.full((coo.m, ldy), float("nan"), dtype=dt, device=cuda)
+    P = ctypes.c_void_p
+    rc = cbspmv.lib().cbspmv_spmv(plan._h, P(Xp.data_ptr()), P(Yp.data_ptr()), nrhs, ldx, ldy,
+                                  P(torch.cuda.current_stream().cuda_stream))
+    assert rc == 0, cbspmv.last_error()
+    torch.cuda.synchronize()
+    Yh = Yp.cpu().numpy()
+    _check(Yh[:, :nrhs].T, yref, ab, f32, f"{name} nrhs {nrhs} padded")
+    assert np.all(np.isnan(Yh[:, nrhs:]))  # columns past nrhs untouched
+    plan.check()
