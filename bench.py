@@ -342,8 +342,10 @@ def bsr_comparator(coo, xh, dev, sizes=(2, 4, 8, 16)):
                                        bd, dC, P(rowp.data_ptr()), ctypes.byref(nnzb)), "nnz")
             torch.cuda.synchronize()
             nbytes = nnzb.value * bd * bd * 8
-            if nbytes > (48 << 30):
-                per[bd] = {"skipped": f"{nbytes / 2**30:.0f} GiB of blocks"}
+            if nnzb.value * bd * bd >= 2**31 - 1 or nbytes > (48 << 30):
+                # the legacy BSR routines index values with 32-bit ints
+                per[bd] = {"skipped": f"{nnzb.value} blocks: {nnzb.value * bd * bd} values, "
+                                      "beyond the library's 32-bit value index"}
                 continue
             colb = torch.empty(max(nnzb.value, 1), dtype=torch.int32, device=dev)
             valb = torch.empty(max(nnzb.value * bd * bd, 1), dtype=torch.float64, device=dev)
