@@ -284,9 +284,9 @@ cbspmv_status upload_partition(DevSide &s, int kernel, cudaStream_t st) {
     return CBSPMV_OK;
 }
 
-// The row-segment stream (kernel 5, and the automatic choice for one
-// right-hand side) of a layout whose stored entries are all in COO blocks,
-// segmented for this device's resident warps.
+// The row-segment stream (kernel 5; the automatic choice for several
+// right-hand sides, and for one when every block is a COO block), segmented
+// for this device's resident warps.
 cbspmv_status upload_rowseg(DevSide &s, int kernel, cudaStream_t st) {
     if ((kernel != 0 && kernel != 5) || !cb::rowseg_applies(s.lay)) return CBSPMV_OK;
     const int64_t warps = cb::rowseg_warps(s.lay.f32);
@@ -326,6 +326,7 @@ cbspmv_status upload_rowseg(DevSide &s, int kernel, cudaStream_t st) {
     d.wbase = static_cast<const int32_t *>(s.rs[8]);
     d.n = R.n;
     d.unit = R.unit;
+    d.auto1 = cb::rowseg_all_coo(s.lay) ? 1 : 0;
     s.rs_bytes = (int64_t)(R.chunks.size() + 4 * (R.meta.size() + R.spans.size() +
                                                   R.rowmap.size() + R.empty.size()));
     return CBSPMV_OK;

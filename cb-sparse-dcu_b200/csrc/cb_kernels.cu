@@ -793,9 +793,11 @@ cudaError_t launch_tiles(const DevLayout &d, const void *x, void *y, int nrhs,
         return launch_pattern_v<T>(d, x, y, stream);
     // the row-segment stream: when chosen, and the automatic choice for
     // all-COO layouts except the reference's small-direct case
-    if (d.rs.chunks && (d.kernel == 5 || (d.kernel == 0 && !d.small_direct && !use_pattern(d))))
-        return nrhs == 1 && ldx == 1 && ldy == 1 ? launch_rowseg(d, x, y, stream)
-                                                 : launch_rowseg_mrhs(d, x, y, nrhs, ldx, ldy, stream);
+    const bool one = nrhs == 1 && ldx == 1 && ldy == 1;
+    if (d.rs.chunks && (d.kernel == 5 || (d.kernel == 0 && !d.small_direct &&
+                                          !use_pattern(d) && (!one || d.rs.auto1))))
+        return one ? launch_rowseg(d, x, y, stream)
+                   : launch_rowseg_mrhs(d, x, y, nrhs, ldx, ldy, stream);
     if (nrhs == 1 && ldx == 1 && ldy == 1 && use_stream(d))
         return launch_stream<T, BS>(d, x, y, stream);
     if (nrhs > 1 || d.kernel == 3 || d.kernel == 4)

@@ -25,6 +25,7 @@ struct RowSegDev {
     const int32_t *wbase = nullptr;   // per CTA: first column of its x window
     int64_t n = 0;                    // columns (length of x)
     int unit = 0;                     // words only: every stored value is 1
+    int auto1 = 0;                    // the automatic choice for one right-hand side
 };
 
 // Device-resident pieces of one DeviceLayout (cb_layout.hpp).

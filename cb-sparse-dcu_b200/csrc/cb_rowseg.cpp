@@ -13,7 +13,10 @@ int64_t a16_64(int64_t x) { return (x + 15) & ~int64_t(15); }
 }  // namespace
 
 bool rowseg_applies(const DeviceLayout &L) {
-    if (L.nvals <= 0 || L.n > kRsMaxCols || L.m >= (int64_t(1) << 31)) return false;
+    return L.nvals > 0 && L.n <= kRsMaxCols && L.m < (int64_t(1) << 31);
+}
+
+bool rowseg_all_coo(const DeviceLayout &L) {
     for (const BlockDesc &b : L.blocks)
         if (meta_type(b.meta) != 0) return false;  // a CSR or DENSE block
     return true;
@@ -30,26 +33,67 @@ std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
     R.unit = unit;
     R.m = m;
     R.n = L.n;
-    // the entries of the tiles' COO sections (every block is a COO block):
-    // row, column and the payload offset of the value
-    int64_t nv = 0;
-    for (const TileDesc &t : L.tiles) nv += t.coo_entries;
-    if (nv != L.nvals) return "row-segment stream: COO entries and stored values differ";
-    std::vector<int32_t> erow((size_t)nv), ecol((size_t)nv);
-    std::vector<int64_t> eoff((size_t)nv);
-    {
-        int64_t k = 0;
-        for (const TileDesc &t : L.tiles) {
-            const int64_t E = t.coo_entries, base = (int64_t)t.payload16 * 16;
-            const uint32_t *idx = reinterpret_cast<const uint32_t *>(L.payload.data() + base);
-            const int64_t vals = base + a16_64(4 * E);  // (none when unit)
-            for (int64_t q = 0; q < E; ++q, ++k) {
-                erow[(size_t)k] = (int32_t)((int64_t)t.block_row * L.bs + (idx[q] >> kColBits));
-                ecol[(size_t)k] = (int32_t)(idx[q] & ((1u << kColBits) - 1));
-                eoff[(size_t)k] = vals + q * vsz;
+    // every stored entry of the tiles, with the payload offset of its value:
+    // the COO sections, then CSR blocks (row pointers, block-local columns
+    // resolved through the gather list) and DENSE blocks (columns below the
+    // block's valid count; unit-valued layouts: the bits set in the mask)
+    std::vector<int32_t> erow, ecol;
+    std::vector<int64_t> eoff;
+    erow.reserve((size_t)L.nvals);
+    ecol.reserve((size_t)L.nvals);
+    eoff.reserve((size_t)L.nvals);
+    const int bs = L.bs;
+    const int64_t isz = bs == 16 ? 1 : 2;
+    for (const TileDesc &t : L.tiles) {
+        const int64_t E = t.coo_entries, base = (int64_t)t.payload16 * 16;
+        const uint32_t *idx = reinterpret_cast<const uint32_t *>(L.payload.data() + base);
+        const int64_t vals = base + a16_64(4 * E);  // (none when unit)
+        for (int64_t q = 0; q < E; ++q) {
+            erow.push_back((int32_t)((int64_t)t.block_row * bs + (idx[q] >> kColBits)));
+            ecol.push_back((int32_t)(idx[q] & ((1u << kColBits) - 1)));
+            eoff.push_back(vals + q * vsz);
+        }
+        const uint32_t nb = t.counts & 0xffu, ncoo = (t.counts >> 8) & 0xffu;
+        for (uint32_t j = ncoo; j < nb; ++j) {
+            const BlockDesc &bd = L.blocks[(size_t)t.block_begin + j];
+            const int64_t pb = base + bd.off;
+            const uint32_t k = meta_nnz(bd.meta), valid = (bd.meta >> 14) & 63u;
+            auto col_of = [&](int64_t c) -> int32_t {
+                return L.gather ? L.block_cols[(size_t)bd.xbase + (size_t)c]
+                                : (int32_t)(bd.xbase + c);
+            };
+            if (meta_type(bd.meta) == 1) {  // CSR
+                const uint8_t *p8 = L.payload.data() + pb;
+                auto at = [&](int64_t i) -> int64_t {
+                    return isz == 1 ? p8[i] : reinterpret_cast<const uint16_t *>(p8)[i];
+                };
+                const int64_t cv = pb + a16_64((bs + 1 + (int64_t)k) * isz);
+                for (int64_t r = 0; r < bs; ++r) {
+                    const int64_t row = (int64_t)t.block_row * bs + r;
+                    for (int64_t q = at(r); q < at(r + 1); ++q) {
+                        if (row >= m) continue;
+                        erow.push_back((int32_t)row);
+                        ecol.push_back(col_of(at(bs + 1 + q)));
+                        eoff.push_back(cv + q * vsz);
+                    }
+                }
+            } else {  // DENSE, row-major bs x bs
+                for (int64_t r = 0; r < bs; ++r) {
+                    const int64_t row = (int64_t)t.block_row * bs + r;
+                    if (row >= m) continue;
+                    for (int64_t c = 0; c < (int64_t)valid; ++c) {
+                        const int64_t i = r * bs + c;
+                        if (unit && !((L.payload[(size_t)(pb + i / 8)] >> (i % 8)) & 1)) continue;
+                        erow.push_back((int32_t)row);
+                        ecol.push_back(col_of(c));
+                        eoff.push_back(pb + i * vsz);
+                    }
+                }
             }
         }
     }
+    const int64_t nv = (int64_t)erow.size();
+    if (nv == 0) return "row-segment stream: no entries";
     // entries by (row, column): counting sort on rows, then columns
     std::vector<int64_t> rp((size_t)m + 1, 0);
     for (int64_t v = 0; v < nv; ++v) ++rp[(size_t)erow[v] + 1];
@@ -81,6 +125,7 @@ std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
     R.chunks.assign((size_t)(nch * CB), 0);
     // words, values and per-entry ordinals; padding: value 0 on column 0,
     // the first padding entry starting the extra ordinal nord
+    std::vector<int32_t> epos((size_t)nv);  // each entry's place in the stream
     std::vector<int32_t> ordv((size_t)(nch * C));
     std::vector<uint8_t> start((size_t)(nch * C), 0);
     int64_t ord = 0;
@@ -95,7 +140,7 @@ std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
             if (!unit)
                 std::memcpy(R.chunks.data() + rs_value_offset(e, f32),
                             L.payload.data() + eoff[v], (size_t)vsz);
-            eoff[v] = -1 - e;  // from here on: the entry's place in the stream
+            epos[(size_t)v] = (int32_t)e;
         } else {
             const bool st = e == nv;
             ord = st ? nord : ord;
@@ -175,26 +220,17 @@ std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
     // per stored value (device order) its stream entry, for value updates:
     // stored value v sits at payload offset val_off[v] (absent from plans
     // loaded from SpMV-only files, which take no new values)
-    if (!unit && (int64_t)L.val_off.size() == nv) {
+    if (!unit && (int64_t)L.val_off.size() == L.nvals) {
         std::vector<std::pair<int64_t, int32_t>> by_off((size_t)nv);
-        {
-            int64_t k = 0;
-            for (const TileDesc &t : L.tiles) {
-                const int64_t E = t.coo_entries, base = (int64_t)t.payload16 * 16;
-                for (int64_t q = 0; q < E; ++q, ++k)
-                    by_off[(size_t)k] = {base + a16_64(4 * E) + q * vsz,
-                                         (int32_t)(-1 - eoff[(size_t)k])};
-            }
-        }
+        for (int64_t k = 0; k < nv; ++k) by_off[(size_t)k] = {eoff[(size_t)k], epos[(size_t)k]};
         std::sort(by_off.begin(), by_off.end());
-        R.vpos.resize((size_t)nv);
-        for (int64_t v = 0; v < nv; ++v) {
+        R.vpos.resize((size_t)L.nvals);
+        for (int64_t v = 0; v < L.nvals; ++v) {
             const int64_t off = (int64_t)L.val_off[v];
             auto it = std::lower_bound(by_off.begin(), by_off.end(),
                                        std::make_pair(off, INT32_MIN));
-            if (it == by_off.end() || it->first != off)
-                return "row-segment stream: a stored value outside the COO sections";
-            R.vpos[(size_t)v] = it->second;
+            // a DENSE slot outside the valid columns or rows has no entry
+            R.vpos[(size_t)v] = it != by_off.end() && it->first == off ? it->second : -1;
         }
     }
     R.alg_bytes = L.alg_bytes;

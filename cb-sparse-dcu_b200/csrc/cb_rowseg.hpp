@@ -1,6 +1,7 @@
-// Row-segment stream: the one-right-hand-side layout of matrices whose
-// stored entries are all in COO blocks (power-law and other scattered
-// matrices, where the blocks hold a few entries each).
+// Row-segment stream: a second device layout of a plan's stored entries,
+// sorted by row (power-law and other scattered matrices, where the blocks
+// hold a few entries each, run fastest on it; CSR and DENSE blocks are
+// expanded into entries).
 //
 // The stored entries, sorted by (row, column), are cut into CHUNKS of
 // 32 x kRsK entries: lane l of a warp takes the kRsK consecutive entries
@@ -86,9 +87,13 @@ struct RowSegHost {
     int64_t alg_bytes = 0;
 };
 
-// Whether the layout takes the row-segment stream: every block a COO block,
-// columns below 2^30, rows below 2^31.
+// Whether the layout takes the row-segment stream: stored entries, columns
+// below 2^30, rows below 2^31 (CSR and DENSE blocks are expanded into
+// entries).  rowseg_all_coo: every block is a COO block (the automatic choice
+// for one right-hand side then takes the stream; otherwise the tile kernels,
+// which read CSR/DENSE blocks with fewer index bytes).
 bool rowseg_applies(const DeviceLayout &L);
+bool rowseg_all_coo(const DeviceLayout &L);
 
 // Builds the stream from the tiles' COO sections (row, column and value of
 // every entry) for `warps` resident warps (G = warps / kRsWarps CTAs); vpos only when the layout has its

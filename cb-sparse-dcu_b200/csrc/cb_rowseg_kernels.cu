@@ -448,6 +448,7 @@ __global__ void cb_rowseg_values_kernel(const RowSegDev rs, const uint8_t *__res
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nvals;
          v += (int64_t)gridDim.x * blockDim.x) {
         const int64_t e = __ldg(&rs.vpos[v]);
+        if (e < 0) continue;  // a DENSE slot outside the valid rows and columns
         const int64_t c = e / C, i = e % C, l = i / kRsK, j = i % kRsK;
         const int64_t pos = (j / NV) * 32 * NV + l * NV + j % NV;
         *reinterpret_cast<T *>(chunks + c * CB + 4 * C + pos * (int64_t)sizeof(T)) =

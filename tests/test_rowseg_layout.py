@@ -76,17 +76,44 @@ def test_rowseg_layout_decodes_to_oracle(name, coo, f32, warps):
     assert np.array_equal(got.astype(np.float64), dv)
 
 
-def test_rowseg_not_built_for_csr_layouts():
-    """A layout with CSR/DENSE blocks keeps the tile kernels (no stream)."""
-    import cbspmv
+def _csr_dense_cases():
     from cbspmv import gen
-    from layout_decode import rowseg_arrays
     rng = np.random.default_rng(3)
-    coo = gen.random_small(rng, 100, 100, 9000)  # dense blocks
-    plan = cbspmv.Plan(coo)
+    return [("dense", gen.random_small(rng, 100, 100, 9000)),
+            ("dense-unit", gen.random_small(rng, 100, 100, 9000, unit=True)),
+            ("banded", gen.banded(rng, 3000, 40)),
+            ("stencil", gen.stencil_27pt(6)),
+            ("laplacian", gen.laplacian_2d(40))]
+
+
+@pytest.mark.parametrize("name,coo", _csr_dense_cases(), ids=[c[0] for c in _csr_dense_cases()])
+@pytest.mark.parametrize("f32", [False, True])
+@pytest.mark.parametrize("bs", [16, 32])
+def test_rowseg_layout_with_csr_dense_blocks(name, coo, f32, bs):
+    """Layouts with CSR and DENSE blocks: their entries are expanded into the
+    stream (DENSE blocks within their valid columns and rows; unit-valued
+    masks by their set bits), which decodes to the oracle's y; every stored
+    value inside those bounds has its stream position."""
+    import cbspmv
+    import cbdump as cd
+    from cbspmv import gen
+    from layout_decode import rowseg_arrays, rowseg_spmv
+    plan = cbspmv.Plan(coo, value_type=int(f32), block_size=bs)
     info = plan.info()
-    assert info["csr_blocks"] + info["dense_blocks"] > 0
-    assert rowseg_arrays(plan, 64) is None
+    rs = rowseg_arrays(plan, 64)
+    assert rs is not None
+    x = gen.uniform_x(coo.n, 4)
+    if f32:
+        x = x.astype(np.float32).astype(np.float64)
+    y = rowseg_spmv(rs, x, coo.m, f32)
+    assert np.all(np.isfinite(y))
+    yref, ab = cd.oracle_spmm_ld(coo, x[None, :])
+    err = np.abs(y.astype(np.float64)[None, :] - yref)
+    assert np.all(err <= TOL[f32] * ab + 1e-300), name
+    if not info["unit_values"]:
+        vp = rs["vpos"]
+        placed = vp[vp >= 0]
+        assert np.array_equal(np.sort(placed), np.arange(placed.size))
 
 
 @pytest.mark.parametrize("spmv_only", [False, True])
