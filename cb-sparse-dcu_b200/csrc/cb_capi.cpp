@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <future>
@@ -72,6 +73,8 @@ struct DevSide {
     // partial slots, rowmap, empty rows, value positions, window bases
     void *rs[9] = {};
     int64_t rs_bytes = 0;
+    std::vector<int32_t> rs_cinfo;  // per chunk summaries (batches cut their own segments)
+    std::vector<int32_t> rs_empty;  // rows without entries
 
     void release() {
         void *ps[] = {tiles, blocks, payload, block_cols, partials, counters,
@@ -84,6 +87,8 @@ struct DevSide {
             q = nullptr;
         }
         rs_bytes = 0;
+        rs_cinfo.clear();
+        rs_empty.clear();
         for (int32_t *&q : pat) q = nullptr;
         tiles = blocks = partials = nullptr;
         payload = nullptr;
@@ -329,6 +334,8 @@ cbspmv_status upload_rowseg(DevSide &s, int kernel, cudaStream_t st) {
     d.auto1 = cb::rowseg_all_coo(s.lay) ? 1 : 0;
     s.rs_bytes = (int64_t)(R.chunks.size() + 4 * (R.meta.size() + R.spans.size() +
                                                   R.rowmap.size() + R.empty.size()));
+    s.rs_cinfo = std::move(R.cinfo);
+    s.rs_empty = std::move(R.empty);
     return CBSPMV_OK;
 }
 
@@ -1286,6 +1293,18 @@ struct cbspmv_batch {
     cudaStream_t cap[8] = {};
     cudaEvent_t ev[9] = {};
     cudaGraphExec_t exec[2] = {};
+    // over the row-segment streams (every plan has one, nrhs <= 16): the
+    // matrices' table, segments {matrix, first chunk, end chunk, -} with their
+    // meta, each warp's first segment, empty rows {matrix, row}, the batch's
+    // spans, counters and partial slots
+    bool rs_mode = false;
+    std::vector<cb::RsBatchMat> rmats;
+    cb::RsBatchMat *d_rmats = nullptr;
+    int4 *d_rsegs = nullptr, *d_rmeta = nullptr, *d_rspans = nullptr;
+    int32_t *d_wseg = nullptr, *d_rcnt = nullptr;
+    int2 *d_rempty = nullptr;
+    void *d_rpart = nullptr;
+    int64_t rwarps = 0, nrempty = 0;
     ~cbspmv_batch() {
         for (cudaGraphExec_t &g : exec)
             if (g) cudaGraphExecDestroy(g);
@@ -1294,7 +1313,9 @@ struct cbspmv_batch {
         for (cudaStream_t &c : cap)
             if (c) cudaStreamDestroy(c);
         for (void *p : {(void *)d_toff, (void *)d_ustart, (void *)d_uorder, (void *)d_sched,
-                        (void *)d_views})
+                        (void *)d_views, (void *)d_rmats, (void *)d_rsegs, (void *)d_rmeta,
+                        (void *)d_rspans, (void *)d_wseg, (void *)d_rcnt, (void *)d_rempty,
+                        d_rpart})
             if (p) cudaFree(p);
         if (herr) cudaFreeHost(herr);
     }
@@ -1338,8 +1359,108 @@ cbspmv_status batch_each(cbspmv_batch *b, cudaStream_t st) {
     return CBSPMV_OK;
 }
 
+template <typename V>
+cudaError_t upload_raw(const std::vector<V> &h, V **d) {
+    const size_t n = std::max<size_t>(1, h.size());
+    cudaError_t e = cudaMalloc((void **)d, n * sizeof(V));
+    if (e == cudaSuccess) e = cudaMemset(*d, 0, n * sizeof(V));
+    if (e == cudaSuccess && !h.empty())
+        e = cudaMemcpy(*d, h.data(), h.size() * sizeof(V), cudaMemcpyHostToDevice);
+    return e;
+}
+
+// The batch over the row-segment streams, when every plan has one and takes
+// at most 16 right-hand sides: the matrices' chunks, ordered by lanes per
+// entry (most first: warps of one SM then mostly run one code path), are cut
+// into one cost-balanced range per resident warp (a chunk costs its lanes per
+// entry); each (warp, matrix) overlap is a segment with its own meta and the
+// batch's own spans, so one launch runs every matrix with static ranges.
+cbspmv_status batch_rowseg_setup(cbspmv_batch *b, const int *nrhs) {
+    const int count = (int)b->plans.size();
+    for (int k = 0; k < count; ++k) {
+        const DevSide &s = b->plans[k]->A;
+        if (!s.d.rs.chunks || s.rs_cinfo.empty() || nrhs[k] > cb::kRsSlotValues)
+            return CBSPMV_OK;
+    }
+    const int64_t W = cb::rowseg_batch_warps(b->f32);
+    if (W <= 0) return CBSPMV_OK;
+    std::vector<int> g(count), order(count);
+    double total = 0;
+    for (int k = 0; k < count; ++k) {
+        g[k] = cb::rs_lanes_per_entry(b->f32, nrhs[k]);
+        total += (double)b->plans[k]->A.d.rs.nch * g[k];
+    }
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return g[a] > g[c]; });
+    std::vector<int32_t> segs, meta, spans, segw;
+    std::vector<int2> empty;
+    int64_t w = 0;
+    double pos = 0;
+    for (int k : order) {
+        const DevSide &s = b->plans[k]->A;
+        const int64_t nch = s.d.rs.nch, seg0 = (int64_t)segw.size();
+        std::vector<int64_t> cuts(1, 0);
+        int64_t c = 0;
+        while (c < nch) {
+            const double bound = total * (double)(w + 1) / (double)W;
+            int64_t n = (int64_t)std::floor((bound - pos) / g[k] + 1e-9);
+            n = std::min<int64_t>(n, nch - c);
+            if (n <= 0 && w + 1 < W) {
+                ++w;
+                continue;
+            }
+            if (n <= 0) n = nch - c;  // the last warp takes the rest
+            segw.push_back((int32_t)w);
+            segs.insert(segs.end(), {k, (int32_t)c, (int32_t)(c + n), 0});
+            c += n;
+            cuts.push_back(c);
+            pos += (double)n * g[k];
+        }
+        cb::rowseg_cut(s.rs_cinfo, cuts, seg0, k, meta, spans);
+        for (int32_t r : s.rs_empty) empty.push_back(make_int2(k, r));
+    }
+    std::vector<int32_t> wseg((size_t)W + 1);
+    for (int64_t q = 0; q <= W; ++q)
+        wseg[(size_t)q] = (int32_t)(std::lower_bound(segw.begin(), segw.end(), (int32_t)q) -
+                                    segw.begin());
+    const size_t nseg = segw.size(), nspan = spans.size() / 4;
+    const size_t vsz = b->f32 ? 4 : 8;
+    cudaError_t e = upload_raw(segs, (int32_t **)&b->d_rsegs);
+    if (e == cudaSuccess) e = upload_raw(meta, (int32_t **)&b->d_rmeta);
+    if (e == cudaSuccess) e = upload_raw(spans, (int32_t **)&b->d_rspans);
+    if (e == cudaSuccess) e = upload_raw(wseg, &b->d_wseg);
+    if (e == cudaSuccess) e = upload_raw(std::vector<int32_t>(std::max<size_t>(1, nspan), 0),
+                                         &b->d_rcnt);
+    if (e == cudaSuccess) e = upload_raw(empty, &b->d_rempty);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&b->d_rpart, std::max<size_t>(1, 2 * nseg) * cb::kRsSlotValues * vsz);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&b->d_rmats, count * sizeof(cb::RsBatchMat));
+    if (e != cudaSuccess) return cuda_fail(e, "allocate batch tables");
+    b->rmats.assign(count, cb::RsBatchMat());
+    for (int k = 0; k < count; ++k) {
+        const cb::RowSegDev &r = b->plans[k]->A.d.rs;
+        cb::RsBatchMat &m = b->rmats[k];
+        m.chunks = r.chunks;
+        m.rowmap = r.rowmap;
+        m.nrhs = nrhs[k];
+        m.nord = r.nord;
+        m.g = g[k];
+        m.unit = r.unit;
+    }
+    b->rwarps = W;
+    b->nrempty = (int64_t)empty.size();
+    b->rs_mode = true;
+    return CBSPMV_OK;
+}
+
 // One persistent launch over every matrix of the batch.
 cbspmv_status batch_one(cbspmv_batch *b, cudaStream_t st) {
+    if (b->rs_mode) {
+        const cudaError_t e = cb::launch_rowseg_batch(
+            b->f32, b->d_rmats, b->d_rsegs, b->d_rmeta, b->d_wseg, b->rwarps, b->d_rempty,
+            b->nrempty, b->d_rspans, b->d_rcnt, b->d_rpart, st);
+        return e == cudaSuccess ? CBSPMV_OK : cuda_fail(e, "batch launch");
+    }
     const cudaError_t e = cb::launch_batch(b->bs, b->f32, b->d_views, (int)b->plans.size(),
                                            b->d_toff, b->d_ustart, b->d_uorder, b->nunits,
                                            b->tile_cap, b->d_sched, b->derr, st);
@@ -1467,6 +1588,10 @@ cbspmv_status cbspmv_batch_create(cbspmv_plan *const *plans, int count, const in
         delete b;
         return cuda_fail(e, "allocate batch tables");
     }
+    if (cbspmv_status rc = batch_rowseg_setup(b, nrhs)) {
+        delete b;
+        return rc;
+    }
     *out = b;
     return CBSPMV_OK;
 }
@@ -1487,6 +1612,21 @@ cbspmv_status cbspmv_batch_bind(cbspmv_batch *b, const void *const *x, void *con
     CB_CUDA(cudaMemcpyAsync(b->d_views, b->views.data(), b->views.size() * sizeof(cb::MatView),
                             cudaMemcpyHostToDevice, st),
             "upload batch table");
+    if (b->rs_mode) {
+        for (size_t k = 0; k < b->plans.size(); ++k) {
+            cb::RsBatchMat &m = b->rmats[k];
+            const int V = b->f32 ? 4 : 2;
+            m.x = x[k];
+            m.y = y[k];
+            m.ldx = m.ldy = m.nrhs;
+            m.xvec = m.nrhs % V == 0 && reinterpret_cast<uintptr_t>(x[k]) % 16 == 0;
+            m.yvec = m.nrhs % V == 0 && reinterpret_cast<uintptr_t>(y[k]) % 16 == 0;
+        }
+        CB_CUDA(cudaMemcpyAsync(b->d_rmats, b->rmats.data(),
+                                b->rmats.size() * sizeof(cb::RsBatchMat), cudaMemcpyHostToDevice,
+                                st),
+                "upload batch table");
+    }
     CB_CUDA(cudaStreamSynchronize(st), "upload batch table");
     if (b->exec[1]) {  // captured with the old pointers
         cudaGraphExecDestroy(b->exec[1]);

@@ -163,6 +163,32 @@ cudaError_t launch_rowseg_mrhs(const DevLayout &d, const void *x, void *y, int n
 cudaError_t launch_rowseg_values(const DevLayout &d, int64_t nvals, const uint64_t *val_off,
                                  cudaStream_t stream);
 
+// Batches over the row-segment streams: one matrix of the device table.
+struct RsBatchMat {
+    const uint8_t *chunks = nullptr;
+    const int32_t *rowmap = nullptr;  // NULL: ordinals are rows
+    const void *x = nullptr;
+    void *y = nullptr;
+    int64_t ldx = 0, ldy = 0;
+    int32_t nrhs = 0, nord = 0;
+    int32_t xvec = 0, yvec = 0;       // 16-byte x loads / y stores allowed
+    int32_t g = 1, unit = 0;          // lanes per entry; words only
+};
+// Lanes per entry for nrhs right-hand sides (1, 2, 4; 8 for FP64 above 8).
+int rs_lanes_per_entry(int f32, int nrhs);
+// Warps of one batch launch on the current device (one CTA of kRsBatchWarps
+// warps per SM).
+int64_t rowseg_batch_warps(int f32);
+// One launch: warp w runs segments segs[wseg[w] .. wseg[w+1]) ({matrix,
+// first chunk, end chunk, -}) with meta[] ({ordinal before, starts a row,
+// head span, tail span}); empty rows {matrix, row} are zeroed first; spans
+// {first segment, last segment, ordinal, -}, counters (zero) and partial
+// slots (kRsSlotValues values, two per segment) belong to the batch.
+cudaError_t launch_rowseg_batch(int f32, const RsBatchMat *mats, const int4 *segs,
+                                const int4 *meta, const int32_t *wseg, int64_t nwarps,
+                                const int2 *empty, int64_t nempty, const int4 *spans,
+                                int32_t *counters, void *part, cudaStream_t stream);
+
 // y = A x; x: n rows, y: m rows, row-major with leading dims for nrhs > 1.
 cudaError_t launch_spmv(const DevLayout &d, const void *x, void *y, int nrhs,
                         int64_t ldx, int64_t ldy, cudaStream_t stream);

@@ -22,6 +22,34 @@ bool rowseg_all_coo(const DeviceLayout &L) {
     return true;
 }
 
+void rowseg_cut(const std::vector<int32_t> &cinfo, const std::vector<int64_t> &cuts,
+                int64_t seg0, int32_t tag, std::vector<int32_t> &meta,
+                std::vector<int32_t> &spans) {
+    const int64_t nseg = (int64_t)cuts.size() - 1;
+    int32_t open = -1;
+    for (int64_t s = 0; s < nseg; ++s) {
+        const int64_t c0 = cuts[(size_t)s], c1 = cuts[(size_t)s + 1];
+        const int32_t *f = &cinfo[(size_t)(4 * c0)];
+        int32_t mt[4] = {f[0], f[1], -1, -1};
+        int64_t nfl = 0;
+        for (int64_t c = c0; c < c1; ++c) nfl += cinfo[(size_t)(4 * c + 2)];
+        if (s > 0 && !f[1] && open >= 0) {  // the first row goes on from segment s - 1
+            mt[2] = open;
+            spans[(size_t)(4 * open + 1)] = (int32_t)(seg0 + s);
+        }
+        const bool cont = s + 1 < nseg && !cinfo[(size_t)(4 * cuts[(size_t)s + 1] + 1)];
+        if (!cont) {
+            open = -1;
+        } else if (nfl > 0 || mt[2] < 0) {  // the last row starts here: a new span
+            open = (int32_t)(spans.size() / 4);
+            spans.insert(spans.end(), {(int32_t)(seg0 + s), (int32_t)(seg0 + s),
+                                       cinfo[(size_t)(4 * (c1 - 1) + 3)], tag});
+            mt[3] = open;
+        }
+        meta.insert(meta.end(), mt, mt + 4);
+    }
+}
+
 std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
     if (!rowseg_applies(L)) return "the layout does not take the row-segment stream";
     const int64_t m = L.m, C = rs_chunk_entries();
@@ -152,34 +180,26 @@ std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
         const int64_t c = e / C, i = e % C;
         std::memcpy(R.chunks.data() + c * CB + 4 * i, &word, 4);
     }
-    // segments of M chunks, about one per warp
+    // chunk summaries, then segments of M chunks, about one per warp
+    R.cinfo.assign((size_t)(4 * nch), 0);
+    for (int64_t c = 0; c < nch; ++c) {
+        int32_t *ci = &R.cinfo[(size_t)(4 * c)];
+        const int64_t e0 = c * C;
+        ci[0] = ordv[(size_t)e0] - start[(size_t)e0];
+        ci[1] = start[(size_t)e0];
+        for (int64_t e = e0; e < e0 + C; ++e) ci[2] += start[(size_t)e];
+        ci[3] = ordv[(size_t)(e0 + C - 1)];
+    }
     const int64_t M = std::max<int64_t>(1, (nch + std::max<int64_t>(warps, 1) - 1) /
                                                std::max<int64_t>(warps, 1));
     const int64_t nseg = (nch + M - 1) / M;
     R.M = (int32_t)M;
     R.nseg = (int32_t)nseg;
-    R.meta.assign((size_t)(4 * nseg), -1);
-    int32_t open = -1;
-    for (int64_t s = 0; s < nseg; ++s) {
-        const int64_t e0 = s * M * C, e1 = std::min(nch, (s + 1) * M) * C - 1;
-        int32_t *mt = &R.meta[(size_t)(4 * s)];
-        mt[0] = ordv[(size_t)e0] - start[(size_t)e0];
-        mt[1] = start[(size_t)e0];
-        int64_t nfl = 0;
-        for (int64_t e = e0; e <= e1; ++e) nfl += start[(size_t)e];
-        if (s > 0 && !start[(size_t)e0]) {  // the first row goes on from segment s - 1
-            if (open < 0) return "row-segment spans out of order";
-            mt[2] = open;
-            R.spans[(size_t)(4 * open + 1)] = (int32_t)s;
-        }
-        const bool cont = s + 1 < nseg && !start[(size_t)((s + 1) * M * C)];
-        if (!cont) {
-            open = -1;
-        } else if (nfl > 0 || mt[2] < 0) {  // the last row starts here: a new span
-            open = (int32_t)(R.spans.size() / 4);
-            R.spans.insert(R.spans.end(), {(int32_t)s, (int32_t)s, ordv[(size_t)e1], 0});
-            mt[3] = open;
-        }
+    {
+        std::vector<int64_t> cuts;
+        for (int64_t s0 = 0; s0 < nseg; ++s0) cuts.push_back(s0 * M);
+        cuts.push_back(nch);
+        rowseg_cut(R.cinfo, cuts, 0, 0, R.meta, R.spans);
     }
     // the CTAs' windows of x: per CTA, the W consecutive columns holding the
     // most of its entries (a sliding window over its sorted columns)

@@ -46,6 +46,7 @@ namespace cb {
 
 constexpr int kRsK = 4;            // entries per lane per chunk
 constexpr int kRsWarps = 32;       // warps per CTA (one CTA per SM)
+constexpr int kRsBatchWarps = 24;  // the batch kernel's (more registers per thread)
 constexpr uint32_t kRsStart = 1u << 31;   // word: the entry starts a row
 constexpr uint32_t kRsWin = 1u << 30;    // word: x[column] is in the CTA's window
 constexpr uint32_t kRsColMask = (1u << 30) - 1;
@@ -77,6 +78,10 @@ struct RowSegHost {
     int32_t G = 0;          // CTAs of every launch
     int32_t W = 0;          // window length in values
     std::vector<int32_t> wbase;    // per CTA: first column of its window
+    // per chunk: ordinal running before its first entry, its first entry
+    // starts a row, row starts in it, ordinal of its last entry (what any
+    // other segmentation needs: a batch cuts its own)
+    std::vector<int32_t> cinfo;
     std::vector<uint8_t> chunks;
     std::vector<int32_t> meta;     // per segment: ord0, starts_row, head span, tail span
     std::vector<int32_t> spans;    // per span: first segment, last segment, ordinal, 0
@@ -94,6 +99,16 @@ struct RowSegHost {
 // which read CSR/DENSE blocks with fewer index bytes).
 bool rowseg_applies(const DeviceLayout &L);
 bool rowseg_all_coo(const DeviceLayout &L);
+
+// Segment meta and spans of the segmentation `cuts` (chunk boundaries,
+// increasing, cuts.front() == 0, cuts.back() == nch) of one stream from its
+// chunk summaries: per segment {ordinal before, starts a row, head span, tail
+// span} appended to meta (span ids offset by the spans already there), per
+// span {first segment, last segment, ordinal, tag} appended to spans
+// (segment ids offset by seg0).
+void rowseg_cut(const std::vector<int32_t> &cinfo, const std::vector<int64_t> &cuts,
+                int64_t seg0, int32_t tag, std::vector<int32_t> &meta,
+                std::vector<int32_t> &spans);
 
 // Builds the stream from the tiles' COO sections (row, column and value of
 // every entry) for `warps` resident warps (G = warps / kRsWarps CTAs); vpos only when the layout has its

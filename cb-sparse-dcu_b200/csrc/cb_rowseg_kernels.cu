@@ -243,33 +243,45 @@ __global__ void __launch_bounds__(kRsWarps * 32, 1)
 // vectors).
 constexpr int kRsMaxRhs = kRsSlotValues;  // right-hand sides per launch (slots hold this many)
 
+// One matrix as the several-right-hand-side segment code reads it.
+template <typename T>
+struct RsMat {
+    const uint8_t *chunks;
+    const int32_t *rowmap;  // NULL: ordinals are rows
+    const T *x;
+    T *y;
+    int64_t ldx, ldy;
+    int32_t nrhs, nord;
+    int32_t xvec, yvec;     // 16-byte loads of x rows / stores of y rows allowed
+};
+
+// The spans of one segmentation: per span {first segment, last segment,
+// ordinal, -}, an arrival counter each (zero between launches), kRsMaxRhs
+// values per slot and two slots per segment.
+template <typename T>
+struct RsSpans {
+    const int4 *spans;
+    int32_t *counters;
+    T *part;
+};
+
+// Chunks [cb, ce) of matrix A as segment s, meta = {ordinal running before
+// chunk cb, chunk cb starts a row, head span, tail span}.  Called by a whole
+// warp.
 template <typename T, int G, bool UNIT>
-__global__ void __launch_bounds__(kRsWarps * 32, 1)
-    cb_rowseg_mrhs_kernel(const RowSegDev rs, const T *__restrict__ x, T *__restrict__ y,
-                          int nrhs, int64_t ldx, int64_t ldy, int xvec, int yvec) {
+__device__ __forceinline__ void rs_mrhs_segment(const RsMat<T> &A, int cb, int ce, int4 meta,
+                                                int s, const RsSpans<T> &S, int lane,
+                                                uint64_t pol) {
     using VT = typename RsVec<T>::V;
     constexpr int V = RsVec<T>::n, P = 32 / G, NV = RsVec<T>::n;
     constexpr int64_t CB = 128 * (4 + (UNIT ? 0 : (int64_t)sizeof(T)));
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int p = lane / G, q = lane % G, c0 = q * V;
     const unsigned gmask = (G == 32 ? kFull : ((1u << G) - 1u)) << (p * G);
-    {  // rows without entries
-        const int64_t total = (int64_t)rs.nempty * nrhs;
-        for (int64_t i = ((int64_t)blockIdx.x * kRsWarps + wib) * 32 + lane; i < total;
-             i += (int64_t)gridDim.x * kRsWarps * 32)
-            y[(int64_t)__ldg(&rs.empty[i / nrhs]) * ldy + i % nrhs] = T(0);
-    }
-    const int NB = gridDim.x, b = blockIdx.x;
-    const int sb0 = (int)((int64_t)b * rs.nseg / NB);
-    const int sb1 = (int)((int64_t)(b + 1) * rs.nseg / NB);
-    int s = sb0 + wib;
-    if (s >= sb1) return;
-    const int M = rs.M, nch = rs.nch, nord = rs.nord;
-    const uint64_t pol = dev::policy_evict_first();
-    auto rid = [&](int32_t o) -> int64_t { return rs.rowmap ? __ldg(&rs.rowmap[o]) : o; };
+    const int nrhs = A.nrhs, nord = A.nord;
+    auto rid = [&](int32_t o) -> int64_t { return A.rowmap ? __ldg(&A.rowmap[o]) : o; };
     auto load_x = [&](uint32_t col, T *o) {
-        const T *px = x + (int64_t)col * ldx + c0;
-        if (xvec) {
+        const T *px = A.x + (int64_t)col * A.ldx + c0;
+        if (A.xvec) {
             if (c0 < nrhs) unpack(__ldg(reinterpret_cast<const VT *>(px)), o);
             else
 #pragma unroll
@@ -280,8 +292,8 @@ __global__ void __launch_bounds__(kRsWarps * 32, 1)
         }
     };
     auto store_y = [&](int64_t row, const T *v) {
-        T *py = y + row * ldy + c0;
-        if (yvec && c0 + V <= nrhs) {
+        T *py = A.y + row * A.ldy + c0;
+        if (A.yvec && c0 + V <= nrhs) {
             VT t;
             T *tv = reinterpret_cast<T *>(&t);
 #pragma unroll
@@ -297,16 +309,15 @@ __global__ void __launch_bounds__(kRsWarps * 32, 1)
     // the slot; lane 0 of the group takes the arrival; the last part's group
     // adds the slots in segment order and stores y
     auto arrive = [&](int span, const T *v, int slot) {
-        T *part = static_cast<T *>(rs.part);
 #pragma unroll
         for (int k = 0; k < V; ++k)
-            if (c0 + k < nrhs) part[(int64_t)slot * kRsMaxRhs + c0 + k] = v[k];
+            if (c0 + k < nrhs) S.part[(int64_t)slot * kRsMaxRhs + c0 + k] = v[k];
         __threadfence();
         __syncwarp(gmask);
         int last = 0;
-        const int4 sp = __ldg(&rs.spans[span]);
+        const int4 sp = __ldg(&S.spans[span]);
         if (q == 0) {
-            cuda::atomic_ref<int32_t, cuda::thread_scope_device> ctr(rs.counters[span]);
+            cuda::atomic_ref<int32_t, cuda::thread_scope_device> ctr(S.counters[span]);
             last = ctr.fetch_add(1, cuda::memory_order_acq_rel) + 1 == sp.y - sp.x + 1;
             if (last) ctr.store(0, cuda::memory_order_relaxed);
         }
@@ -316,124 +327,185 @@ __global__ void __launch_bounds__(kRsWarps * 32, 1)
             T tot[V];
 #pragma unroll
             for (int k = 0; k < V; ++k)
-                tot[k] = c0 + k < nrhs ? __ldcg(&part[(int64_t)(2 * sp.x + 1) * kRsMaxRhs + c0 + k])
-                                       : T(0);
+                tot[k] = c0 + k < nrhs
+                             ? __ldcg(&S.part[(int64_t)(2 * sp.x + 1) * kRsMaxRhs + c0 + k])
+                             : T(0);
             for (int w = sp.x + 1; w <= sp.y; ++w)
 #pragma unroll
                 for (int k = 0; k < V; ++k)
-                    if (c0 + k < nrhs) tot[k] += __ldcg(&part[(int64_t)(2 * w) * kRsMaxRhs + c0 + k]);
+                    if (c0 + k < nrhs)
+                        tot[k] += __ldcg(&S.part[(int64_t)(2 * w) * kRsMaxRhs + c0 + k]);
             store_y(rid(sp.z), tot);
         }
     };
-    while (true) {
-        const int4 meta = __ldg(&rs.meta[s]);
-        const int32_t first = meta.x;
-        int32_t ord0 = meta.x;
-        T carry[V];
+    const int32_t first = meta.x;
+    int32_t ord0 = meta.x;
+    T carry[V];
 #pragma unroll
-        for (int k = 0; k < V; ++k) carry[k] = T(0);
-        const int cbeg = s * M, cend = min(nch, cbeg + M);
-        for (int c = cbeg; c < cend; ++c) {
-            const uint4 *gw = reinterpret_cast<const uint4 *>(rs.chunks + (int64_t)c * CB);
-            const uint8_t *gv = rs.chunks + (int64_t)c * CB + 4 * 128;
-            // row starts of the group's entries: each lane counts one
-            // 4-entry step, the group adds them
-            int cnt;
-            {
-                const uint4 t = __ldg(gw + G * p + q);
-                cnt = (int)((t.x >> 31) + (t.y >> 31) + (t.z >> 31) + (t.w >> 31));
+    for (int k = 0; k < V; ++k) carry[k] = T(0);
+    for (int c = cb; c < ce; ++c) {
+        const uint4 *gw = reinterpret_cast<const uint4 *>(A.chunks + (int64_t)c * CB);
+        const uint8_t *gv = A.chunks + (int64_t)c * CB + 4 * 128;
+        // row starts of the group's entries: each lane counts one 4-entry
+        // step, the group adds them
+        int cnt;
+        {
+            const uint4 t = __ldg(gw + G * p + q);
+            cnt = (int)((t.x >> 31) + (t.y >> 31) + (t.z >> 31) + (t.w >> 31));
 #pragma unroll
-                for (int d = 1; d < G; d <<= 1) cnt += __shfl_xor_sync(kFull, cnt, d);
-            }
-            int inc = cnt;  // inclusive scan over the groups
+            for (int d = 1; d < G; d <<= 1) cnt += __shfl_xor_sync(kFull, cnt, d);
+        }
+        int inc = cnt;  // inclusive scan over the groups
 #pragma unroll
-            for (int d = 1; d < P; d <<= 1) {
-                const int t = __shfl_up_sync(kFull, inc, d * G);
-                if (p >= d) inc += t;
-            }
-            const int32_t ordS = ord0 + inc - cnt;  // the row this group starts in
-            int32_t ord = ordS;
-            T run[V], head[V];
+        for (int d = 1; d < P; d <<= 1) {
+            const int t = __shfl_up_sync(kFull, inc, d * G);
+            if (p >= d) inc += t;
+        }
+        const int32_t ordS = ord0 + inc - cnt;  // the row this group starts in
+        int32_t ord = ordS;
+        T run[V], head[V];
 #pragma unroll
-            for (int k = 0; k < V; ++k) run[k] = head[k] = T(0);
-            bool seen = false;
+        for (int k = 0; k < V; ++k) run[k] = head[k] = T(0);
+        bool seen = false;
 #pragma unroll 1
-            for (int i = 0; i < G; ++i) {
-                const int ls = G * p + i;  // the one-vector lane whose 4 entries these are
-                const uint4 t = __ldg(gw + ls);
-                const uint32_t w[4] = {t.x, t.y, t.z, t.w};
-                T v[4];
-                if (UNIT) {
+        for (int i = 0; i < G; ++i) {
+            const int ls = G * p + i;  // the one-vector lane whose 4 entries these are
+            const uint4 t = __ldg(gw + ls);
+            const uint32_t w[4] = {t.x, t.y, t.z, t.w};
+            T v[4];
+            if (UNIT) {
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) v[j] = T(1);
-                } else if (NV == 4) {
-                    unpack(ld_stream(reinterpret_cast<const VT *>(gv) + ls, pol), v);
-                } else {
-                    unpack(ld_stream(reinterpret_cast<const VT *>(gv) + ls, pol), v);
-                    unpack(ld_stream(reinterpret_cast<const VT *>(gv) + 32 + ls, pol), v + 2);
-                }
-                T xv[4][V];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) load_x(w[j] & kRsColMask, xv[j]);
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const bool f = (w[j] >> 31) != 0;
-                    if (f && seen) store_y(rid(ord), run);  // a row whole inside the group
-#pragma unroll
-                    for (int k = 0; k < V; ++k) {
-                        head[k] = (f && !seen) ? run[k] : head[k];
-                        run[k] = fma(v[j], xv[j][k], f ? T(0) : run[k]);
-                    }
-                    seen = seen || f;
-                    ord += f ? 1 : 0;
-                }
+                for (int j = 0; j < 4; ++j) v[j] = T(1);
+            } else if (NV == 4) {
+                unpack(ld_stream(reinterpret_cast<const VT *>(gv) + ls, pol), v);
+            } else {
+                unpack(ld_stream(reinterpret_cast<const VT *>(gv) + ls, pol), v);
+                unpack(ld_stream(reinterpret_cast<const VT *>(gv) + 32 + ls, pol), v + 2);
             }
-            // rows across groups: inclusive scan over the groups, reset at
-            // groups holding a row start; group 0 continues the previous chunk
-            T sc[V];
+            T xv[4][V];
 #pragma unroll
-            for (int k = 0; k < V; ++k) sc[k] = (p == 0 && !seen) ? run[k] + carry[k] : run[k];
-            bool r = seen;
+            for (int j = 0; j < 4; ++j) load_x(w[j] & kRsColMask, xv[j]);
 #pragma unroll
-            for (int d = 1; d < P; d <<= 1) {
-                const bool ru = __shfl_up_sync(kFull, (int)r, d * G) != 0;
+            for (int j = 0; j < 4; ++j) {
+                const bool f = (w[j] >> 31) != 0;
+                if (f && seen) store_y(rid(ord), run);  // a row whole inside the group
 #pragma unroll
                 for (int k = 0; k < V; ++k) {
-                    const T su = __shfl_up_sync(kFull, sc[k], d * G);
-                    if (p >= d && !r) sc[k] += su;
+                    head[k] = (f && !seen) ? run[k] : head[k];
+                    run[k] = fma(v[j], xv[j][k], f ? T(0) : run[k]);
                 }
-                if (p >= d) r = r || ru;
+                seen = seen || f;
+                ord += f ? 1 : 0;
             }
-            T cin[V];
+        }
+        // rows across groups: inclusive scan over the groups, reset at groups
+        // holding a row start; group 0 continues the previous chunk
+        T sc[V];
+#pragma unroll
+        for (int k = 0; k < V; ++k) sc[k] = (p == 0 && !seen) ? run[k] + carry[k] : run[k];
+        bool r = seen;
+#pragma unroll
+        for (int d = 1; d < P; d <<= 1) {
+            const bool ru = __shfl_up_sync(kFull, (int)r, d * G) != 0;
 #pragma unroll
             for (int k = 0; k < V; ++k) {
-                const T t = __shfl_up_sync(kFull, sc[k], G);
-                cin[k] = p == 0 ? carry[k] : t;
+                const T su = __shfl_up_sync(kFull, sc[k], d * G);
+                if (p >= d && !r) sc[k] += su;
             }
-            if (seen) {  // the row this group started in ends here
-                T val[V];
-#pragma unroll
-                for (int k = 0; k < V; ++k) val[k] = cin[k] + head[k];
-                if (ordS == first && meta.z >= 0)
-                    arrive(meta.z, val, 2 * s);
-                else if (!(ordS == first && meta.y) && ordS < nord)
-                    store_y(rid(ordS), val);
-            }
-#pragma unroll
-            for (int k = 0; k < V; ++k) carry[k] = __shfl_sync(kFull, sc[k], (P - 1) * G + q);
-            ord0 = __shfl_sync(kFull, ord, (P - 1) * G);
+            if (p >= d) r = r || ru;
         }
-        // the segment's last row: a span's part, or whole here (group 0)
-        if (p == 0) {
-            if (ord0 == first && meta.z >= 0)
-                arrive(meta.z, carry, 2 * s);
-            else if (meta.w >= 0)
-                arrive(meta.w, carry, 2 * s + 1);
-            else if (ord0 < nord && !(ord0 == first && meta.y))
-                store_y(rid(ord0), carry);
+        T cin[V];
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+            const T t = __shfl_up_sync(kFull, sc[k], G);
+            cin[k] = p == 0 ? carry[k] : t;
         }
-        s += kRsWarps;
-        if (s >= sb1) break;
+        if (seen) {  // the row this group started in ends here
+            T val[V];
+#pragma unroll
+            for (int k = 0; k < V; ++k) val[k] = cin[k] + head[k];
+            if (ordS == first && meta.z >= 0)
+                arrive(meta.z, val, 2 * s);
+            else if (!(ordS == first && meta.y) && ordS < nord)
+                store_y(rid(ordS), val);
+        }
+#pragma unroll
+        for (int k = 0; k < V; ++k) carry[k] = __shfl_sync(kFull, sc[k], (P - 1) * G + q);
+        ord0 = __shfl_sync(kFull, ord, (P - 1) * G);
+    }
+    // the segment's last row: a span's part, or whole here (group 0)
+    if (p == 0) {
+        if (ord0 == first && meta.z >= 0)
+            arrive(meta.z, carry, 2 * s);
+        else if (meta.w >= 0)
+            arrive(meta.w, carry, 2 * s + 1);
+        else if (ord0 < nord && !(ord0 == first && meta.y))
+            store_y(rid(ord0), carry);
+    }
+    __syncwarp();
+}
+
+template <typename T, int G, bool UNIT>
+__global__ void __launch_bounds__(kRsWarps * 32, 1)
+    cb_rowseg_mrhs_kernel(const RowSegDev rs, const T *__restrict__ x, T *__restrict__ y,
+                          int nrhs, int64_t ldx, int64_t ldy, int xvec, int yvec) {
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    {  // rows without entries
+        const int64_t total = (int64_t)rs.nempty * nrhs;
+        for (int64_t i = ((int64_t)blockIdx.x * kRsWarps + wib) * 32 + lane; i < total;
+             i += (int64_t)gridDim.x * kRsWarps * 32)
+            y[(int64_t)__ldg(&rs.empty[i / nrhs]) * ldy + i % nrhs] = T(0);
+    }
+    const int NB = gridDim.x, b = blockIdx.x;
+    const int sb0 = (int)((int64_t)b * rs.nseg / NB);
+    const int sb1 = (int)((int64_t)(b + 1) * rs.nseg / NB);
+    const RsMat<T> A{rs.chunks, rs.rowmap, x, y, ldx, ldy, nrhs, rs.nord, xvec, yvec};
+    const RsSpans<T> S{rs.spans, rs.counters, static_cast<T *>(rs.part)};
+    const uint64_t pol = dev::policy_evict_first();
+    for (int s = sb0 + wib; s < sb1; s += kRsWarps)
+        rs_mrhs_segment<T, G, UNIT>(A, s * rs.M, min(rs.nch, s * rs.M + rs.M),
+                                    __ldg(&rs.meta[s]), s, S, lane, pol);
+}
+
+// A batch over the streams (kRsBatchWarps warps per CTA: the kernel holds
+// every lanes-per-entry variant, so it is given more registers per thread):
+// warp w runs the segments segs[wseg[w] ..
+// wseg[w+1]) (each {matrix, first chunk, end chunk, -}, with meta[] and the
+// batch's own spans), choosing the lanes per entry from the matrix's entry.
+template <typename T>
+__global__ void __launch_bounds__(kRsBatchWarps * 32, 1)
+    cb_rowseg_batch_kernel(const RsBatchMat *__restrict__ mats, const int4 *__restrict__ segs,
+                           const int4 *__restrict__ meta, const int32_t *__restrict__ wseg,
+                           const int2 *__restrict__ empty, int64_t nempty, const int4 *spans,
+                           int32_t *counters, T *part) {
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    for (int64_t i = ((int64_t)blockIdx.x * kRsBatchWarps + wib) * 32 + lane; i < nempty;
+         i += (int64_t)gridDim.x * kRsBatchWarps * 32) {  // rows without entries
+        const int2 e = __ldg(&empty[i]);
+        const RsBatchMat &m = mats[e.x];
+        for (int k = 0; k < m.nrhs; ++k) static_cast<T *>(m.y)[(int64_t)e.y * m.ldy + k] = T(0);
+    }
+    const int w = blockIdx.x * kRsBatchWarps + wib;
+    const RsSpans<T> S{spans, counters, part};
+    const uint64_t pol = dev::policy_evict_first();
+    for (int si = __ldg(&wseg[w]); si < __ldg(&wseg[w + 1]); ++si) {
+        const int4 sg = __ldg(&segs[si]);
+        const RsBatchMat &m = mats[sg.x];
+        const RsMat<T> A{m.chunks, m.rowmap, static_cast<const T *>(m.x), static_cast<T *>(m.y),
+                         m.ldx, m.ldy, m.nrhs, m.nord, m.xvec, m.yvec};
+        const int4 mt = __ldg(&meta[si]);
+        constexpr int GMAX = sizeof(T) == 4 ? 4 : 8;
+        switch (m.g * 2 + (m.unit ? 1 : 0)) {
+            case 2: rs_mrhs_segment<T, 1, false>(A, sg.y, sg.z, mt, si, S, lane, pol); break;
+            case 3: rs_mrhs_segment<T, 1, true>(A, sg.y, sg.z, mt, si, S, lane, pol); break;
+            case 4: rs_mrhs_segment<T, 2, false>(A, sg.y, sg.z, mt, si, S, lane, pol); break;
+            case 5: rs_mrhs_segment<T, 2, true>(A, sg.y, sg.z, mt, si, S, lane, pol); break;
+            case 8: rs_mrhs_segment<T, 4, false>(A, sg.y, sg.z, mt, si, S, lane, pol); break;
+            case 9: rs_mrhs_segment<T, 4, true>(A, sg.y, sg.z, mt, si, S, lane, pol); break;
+            case 16: rs_mrhs_segment<T, GMAX, false>(A, sg.y, sg.z, mt, si, S, lane, pol); break;
+            case 17: rs_mrhs_segment<T, GMAX, true>(A, sg.y, sg.z, mt, si, S, lane, pol); break;
+            default: break;
+        }
     }
 }
 
@@ -522,8 +594,7 @@ cudaError_t launch_mrhs_t(const DevLayout &d, const T *x, T *y, int nrhs, int64_
         const int r = std::min(kRsMaxRhs, nrhs - c);
         const int xvec = ldx % V == 0 && reinterpret_cast<uintptr_t>(x + c) % 16 == 0;
         const int yvec = ldy % V == 0 && reinterpret_cast<uintptr_t>(y + c) % 16 == 0;
-        int g = 1;
-        while (g * V < r) g *= 2;
+        const int g = rs_lanes_per_entry(sizeof(T) == 4, r);
         cudaError_t e;
         switch (g) {
             case 1: e = launch_mrhs_g<T, 1, UNIT>(d, x + c, y + c, r, ldx, ldy, xvec, yvec, stream); break;
@@ -549,6 +620,35 @@ cudaError_t launch_rowseg_mrhs(const DevLayout &d, const void *x, void *y, int n
                                                    static_cast<double *>(y), nrhs, ldx, ldy, stream)
                      : launch_mrhs_t<double, false>(d, static_cast<const double *>(x),
                                                     static_cast<double *>(y), nrhs, ldx, ldy, stream);
+}
+
+int rs_lanes_per_entry(int f32, int nrhs) {
+    const int V = f32 ? 4 : 2, gmax = f32 ? 4 : 8;
+    int g = 1;
+    while (g * V < std::min(nrhs, kRsMaxRhs) && g < gmax) g *= 2;
+    return g;
+}
+
+int64_t rowseg_batch_warps(int f32) {
+    const void *fn = f32 ? reinterpret_cast<const void *>(cb_rowseg_batch_kernel<float>)
+                         : reinterpret_cast<const void *>(cb_rowseg_batch_kernel<double>);
+    return (int64_t)dev_sms() * dev_resident_l1(fn, kRsBatchWarps * 32, 0) * kRsBatchWarps;
+}
+
+cudaError_t launch_rowseg_batch(int f32, const RsBatchMat *mats, const int4 *segs,
+                                const int4 *meta, const int32_t *wseg, int64_t nwarps,
+                                const int2 *empty, int64_t nempty, const int4 *spans,
+                                int32_t *counters, void *part, cudaStream_t stream) {
+    if (nwarps <= 0 || nwarps % kRsBatchWarps) return cudaErrorInvalidValue;
+    const unsigned grid = (unsigned)(nwarps / kRsBatchWarps);
+    if (f32)
+        cb_rowseg_batch_kernel<float><<<grid, kRsBatchWarps * 32, 0, stream>>>(
+            mats, segs, meta, wseg, empty, nempty, spans, counters, static_cast<float *>(part));
+    else
+        cb_rowseg_batch_kernel<double><<<grid, kRsBatchWarps * 32, 0, stream>>>(
+            mats, segs, meta, wseg, empty, nempty, spans, counters, static_cast<double *>(part));
+    note_launch();
+    return cudaGetLastError();
 }
 
 cudaError_t launch_rowseg_values(const DevLayout &d, int64_t nvals, const uint64_t *val_off,
