@@ -85,7 +85,10 @@ std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
         for (uint32_t j = ncoo; j < nb; ++j) {
             const BlockDesc &bd = L.blocks[(size_t)t.block_begin + j];
             const int64_t pb = base + bd.off;
-            const uint32_t k = meta_nnz(bd.meta), valid = (bd.meta >> 14) & 63u;
+            // (the valid-column field can carry a bit of an oversized raw
+            // entry count of a DENSE block built from duplicates: clamp)
+            const uint32_t k = meta_nnz(bd.meta);
+            const uint32_t valid = std::min<uint32_t>((bd.meta >> 14) & 63u, (uint32_t)bs);
             auto col_of = [&](int64_t c) -> int32_t {
                 return L.gather ? L.block_cols[(size_t)bd.xbase + (size_t)c]
                                 : (int32_t)(bd.xbase + c);
@@ -122,6 +125,10 @@ std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
     }
     const int64_t nv = (int64_t)erow.size();
     if (nv == 0) return "row-segment stream: no entries";
+    for (int64_t k2 = 0; k2 < nv; ++k2)  // every gather stays inside x, every row inside y
+        if (ecol[(size_t)k2] < 0 || ecol[(size_t)k2] >= L.n || erow[(size_t)k2] < 0 ||
+            erow[(size_t)k2] >= m)
+            return "row-segment stream: an entry outside the matrix";
     // entries by (row, column): counting sort on rows, then columns
     std::vector<int64_t> rp((size_t)m + 1, 0);
     for (int64_t v = 0; v < nv; ++v) ++rp[(size_t)erow[v] + 1];

@@ -134,3 +134,37 @@ def test_rowseg_same_stream_after_plan_file(tmp_path, spmv_only):
     for k in ("sizes", "chunks", "meta", "spans", "rowmap", "empty", "wbase"):
         assert np.array_equal(a[k], b[k]), k
     assert b["vpos"].size == (0 if spmv_only else coo.nnz)
+
+
+def _suite_cases():
+    import test_gpu_spmv as tg
+    import test_gpu_batch as tb
+    seen, out = set(), []
+    for name, coo in list(tg.CASES) + list(getattr(tb, "CASES", [])):
+        if name not in seen:
+            seen.add(name)
+            out.append((name, coo))
+    return out
+
+
+@pytest.mark.parametrize("name,coo", _suite_cases(), ids=[c[0] for c in _suite_cases()])
+@pytest.mark.parametrize("bs", [16, 32])
+def test_rowseg_layout_on_the_gpu_suite_matrices(name, coo, bs):
+    """Every matrix the GPU parity tests run, through the stream as the
+    device builds it for a full B200 (4736 warps): decodes to the oracle, and
+    every column lies inside x (the host build refuses anything else)."""
+    import cbspmv
+    import cbdump as cd
+    from cbspmv import gen
+    from layout_decode import rowseg_arrays, rowseg_spmv
+    plan = cbspmv.Plan(coo, block_size=bs, tile_entries=64)
+    rs = rowseg_arrays(plan, 4736)
+    if coo.nnz == 0:
+        assert rs is None
+        return
+    words = rs["chunks"].reshape(int(rs["sizes"][0]), -1)[:, :512].view(np.uint32)
+    assert int((words & ((1 << 30) - 1)).max()) < coo.n
+    x = gen.uniform_x(coo.n, 6)
+    y = rowseg_spmv(rs, x, coo.m, False)
+    yref, ab = cd.oracle_spmm_ld(coo, x[None, :])
+    assert np.all(np.abs(y[None, :] - yref) <= TOL[False] * ab + 1e-300)
