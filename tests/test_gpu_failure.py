@@ -98,14 +98,16 @@ def test_giveup_host_call_reports(cuda):
 
 
 def test_batch_giveup_is_reported_and_reset(cuda):
-    """The same for the one-launch batch: cbspmv_batch_check reports the
-    give-up, the batch's scratch is reset, and the next launches are exact."""
+    """The same for the one-launch batch of the staged kernel (plans pinned
+    to kernel 3 carry no row-segment stream, whose batch kernel has no waits):
+    cbspmv_batch_check reports the give-up, the batch's scratch is reset, and
+    the next launches are exact."""
     import torch
     import cbspmv
     import cbdump as cd
     from cbspmv import gen
     items = gen.batch_uneven(count=12, seed=6, nmin=500, nmax=20000)
-    plans = [cbspmv.Plan(it.coo, tile_entries=64) for it in items]
+    plans = [cbspmv.Plan(it.coo, tile_entries=64, kernel=3) for it in items]
     Xs = [np.ascontiguousarray(gen.uniform_x(it.coo.n, 50 + i, nrhs=max(it.nrhs, 2))[:it.nrhs].T)
           for i, it in enumerate(items)]
     xs = [torch.from_numpy(X).to(cuda) for X in Xs]
