@@ -1294,14 +1294,15 @@ struct cbspmv_batch {
     cudaEvent_t ev[9] = {};
     cudaGraphExec_t exec[2] = {};
     // over the row-segment streams (every plan has one, nrhs <= 16): the
-    // matrices' table, segments {matrix, first chunk, end chunk, -} with their
-    // meta, each warp's first segment, empty rows {matrix, row}, the batch's
-    // spans, counters and partial slots
+    // matrices' table, segments {matrix, first chunk, end chunk, -} in queue
+    // order with their meta, scheduler words, empty rows {matrix, row}, the
+    // batch's spans, counters and partial slots
     bool rs_mode = false;
     std::vector<cb::RsBatchMat> rmats;
     cb::RsBatchMat *d_rmats = nullptr;
     int4 *d_rsegs = nullptr, *d_rmeta = nullptr, *d_rspans = nullptr;
-    int32_t *d_wseg = nullptr, *d_rcnt = nullptr;
+    int32_t *d_rcnt = nullptr, nrseg = 0;
+    uint32_t *d_rsched = nullptr;   // 2 scheduler words (next segment, warps out)
     int2 *d_rempty = nullptr;
     void *d_rpart = nullptr;
     int64_t rwarps = 0, nrempty = 0;
@@ -1314,7 +1315,7 @@ struct cbspmv_batch {
             if (c) cudaStreamDestroy(c);
         for (void *p : {(void *)d_toff, (void *)d_ustart, (void *)d_uorder, (void *)d_sched,
                         (void *)d_views, (void *)d_rmats, (void *)d_rsegs, (void *)d_rmeta,
-                        (void *)d_rspans, (void *)d_wseg, (void *)d_rcnt, (void *)d_rempty,
+                        (void *)d_rspans, (void *)d_rsched, (void *)d_rcnt, (void *)d_rempty,
                         d_rpart})
             if (p) cudaFree(p);
         if (herr) cudaFreeHost(herr);
@@ -1370,11 +1371,12 @@ cudaError_t upload_raw(const std::vector<V> &h, V **d) {
 }
 
 // The batch over the row-segment streams, when every plan has one and takes
-// at most 16 right-hand sides: the matrices' chunks, ordered by lanes per
-// entry (most first: warps of one SM then mostly run one code path), are cut
-// into one cost-balanced range per resident warp (a chunk costs its lanes per
-// entry); each (warp, matrix) overlap is a segment with its own meta and the
-// batch's own spans, so one launch runs every matrix with static ranges.
+// at most 16 right-hand sides: each matrix's chunks cut into segments of
+// about one eighth of a resident warp's share of the work (a chunk costs its
+// lanes per entry), queued by lanes per entry (most first: warps of one SM
+// then mostly run one code path) and taken by the warps from a counter, so
+// one launch runs every matrix and balances itself; each segment has its own
+// meta and the batch its own spans.
 cbspmv_status batch_rowseg_setup(cbspmv_batch *b, const int *nrhs) {
     const int count = (int)b->plans.size();
     for (int k = 0; k < count; ++k) {
@@ -1392,43 +1394,28 @@ cbspmv_status batch_rowseg_setup(cbspmv_batch *b, const int *nrhs) {
     }
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return g[a] > g[c]; });
-    std::vector<int32_t> segs, meta, spans, segw;
+    const double share = std::max(1.0, total / ((double)W * 8));
+    std::vector<int32_t> segs, meta, spans;
     std::vector<int2> empty;
-    int64_t w = 0;
-    double pos = 0;
     for (int k : order) {
         const DevSide &s = b->plans[k]->A;
-        const int64_t nch = s.d.rs.nch, seg0 = (int64_t)segw.size();
+        const int64_t nch = s.d.rs.nch, seg0 = (int64_t)(segs.size() / 4);
+        const int64_t per = std::max<int64_t>(1, (int64_t)std::llround(share / g[k]));
         std::vector<int64_t> cuts(1, 0);
-        int64_t c = 0;
-        while (c < nch) {
-            const double bound = total * (double)(w + 1) / (double)W;
-            int64_t n = (int64_t)std::floor((bound - pos) / g[k] + 1e-9);
-            n = std::min<int64_t>(n, nch - c);
-            if (n <= 0 && w + 1 < W) {
-                ++w;
-                continue;
-            }
-            if (n <= 0) n = nch - c;  // the last warp takes the rest
-            segw.push_back((int32_t)w);
-            segs.insert(segs.end(), {k, (int32_t)c, (int32_t)(c + n), 0});
-            c += n;
-            cuts.push_back(c);
-            pos += (double)n * g[k];
+        for (int64_t c = 0; c < nch; c += per) {
+            const int64_t e = std::min(nch, c + per);
+            segs.insert(segs.end(), {k, (int32_t)c, (int32_t)e, 0});
+            cuts.push_back(e);
         }
         cb::rowseg_cut(s.rs_cinfo, cuts, seg0, k, meta, spans);
         for (int32_t r : s.rs_empty) empty.push_back(make_int2(k, r));
     }
-    std::vector<int32_t> wseg((size_t)W + 1);
-    for (int64_t q = 0; q <= W; ++q)
-        wseg[(size_t)q] = (int32_t)(std::lower_bound(segw.begin(), segw.end(), (int32_t)q) -
-                                    segw.begin());
-    const size_t nseg = segw.size(), nspan = spans.size() / 4;
+    const size_t nseg = segs.size() / 4, nspan = spans.size() / 4;
     const size_t vsz = b->f32 ? 4 : 8;
     cudaError_t e = upload_raw(segs, (int32_t **)&b->d_rsegs);
     if (e == cudaSuccess) e = upload_raw(meta, (int32_t **)&b->d_rmeta);
     if (e == cudaSuccess) e = upload_raw(spans, (int32_t **)&b->d_rspans);
-    if (e == cudaSuccess) e = upload_raw(wseg, &b->d_wseg);
+    if (e == cudaSuccess) e = upload_raw(std::vector<uint32_t>(2, 0u), &b->d_rsched);
     if (e == cudaSuccess) e = upload_raw(std::vector<int32_t>(std::max<size_t>(1, nspan), 0),
                                          &b->d_rcnt);
     if (e == cudaSuccess) e = upload_raw(empty, &b->d_rempty);
@@ -1448,6 +1435,7 @@ cbspmv_status batch_rowseg_setup(cbspmv_batch *b, const int *nrhs) {
         m.unit = r.unit;
     }
     b->rwarps = W;
+    b->nrseg = (int32_t)nseg;
     b->nrempty = (int64_t)empty.size();
     b->rs_mode = true;
     return CBSPMV_OK;
@@ -1457,8 +1445,8 @@ cbspmv_status batch_rowseg_setup(cbspmv_batch *b, const int *nrhs) {
 cbspmv_status batch_one(cbspmv_batch *b, cudaStream_t st) {
     if (b->rs_mode) {
         const cudaError_t e = cb::launch_rowseg_batch(
-            b->f32, b->d_rmats, b->d_rsegs, b->d_rmeta, b->d_wseg, b->rwarps, b->d_rempty,
-            b->nrempty, b->d_rspans, b->d_rcnt, b->d_rpart, st);
+            b->f32, b->d_rmats, b->d_rsegs, b->d_rmeta, b->nrseg, b->d_rsched, b->rwarps,
+            b->d_rempty, b->nrempty, b->d_rspans, b->d_rcnt, b->d_rpart, st);
         return e == cudaSuccess ? CBSPMV_OK : cuda_fail(e, "batch launch");
     }
     const cudaError_t e = cb::launch_batch(b->bs, b->f32, b->d_views, (int)b->plans.size(),

@@ -179,13 +179,15 @@ int rs_lanes_per_entry(int f32, int nrhs);
 // Warps of one batch launch on the current device (one CTA of kRsBatchWarps
 // warps per SM).
 int64_t rowseg_batch_warps(int f32);
-// One launch: warp w runs segments segs[wseg[w] .. wseg[w+1]) ({matrix,
-// first chunk, end chunk, -}) with meta[] ({ordinal before, starts a row,
-// head span, tail span}); empty rows {matrix, row} are zeroed first; spans
-// {first segment, last segment, ordinal, -}, counters (zero) and partial
-// slots (kRsSlotValues values, two per segment) belong to the batch.
+// One launch: warps take segments segs[0 .. nseg) ({matrix, first chunk,
+// end chunk, -}, in queue order) from the scheduler word sched[0] (sched[0..1]
+// zero before the first launch; the kernel leaves them zero), with meta[]
+// ({ordinal before, starts a row, head span, tail span}); empty rows {matrix,
+// row} are zeroed first; spans {first segment, last segment, ordinal, -},
+// counters (zero) and partial slots (kRsSlotValues values, two per segment)
+// belong to the batch.
 cudaError_t launch_rowseg_batch(int f32, const RsBatchMat *mats, const int4 *segs,
-                                const int4 *meta, const int32_t *wseg, int64_t nwarps,
+                                const int4 *meta, int32_t nseg, uint32_t *sched, int64_t nwarps,
                                 const int2 *empty, int64_t nempty, const int4 *spans,
                                 int32_t *counters, void *part, cudaStream_t stream);
 

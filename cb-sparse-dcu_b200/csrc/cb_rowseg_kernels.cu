@@ -469,13 +469,14 @@ __global__ void __launch_bounds__(kRsWarps * 32, 1)
 
 // A batch over the streams (kRsBatchWarps warps per CTA: the kernel holds
 // every lanes-per-entry variant, so it is given more registers per thread):
-// warp w runs the segments segs[wseg[w] ..
-// wseg[w+1]) (each {matrix, first chunk, end chunk, -}, with meta[] and the
-// batch's own spans), choosing the lanes per entry from the matrix's entry.
+// warps take segments segs[0 .. nseg) ({matrix, first chunk, end chunk, -},
+// with meta[] and the batch's own spans; queued by lanes per entry) from
+// sched[0], choosing the segment code from the matrix's entry; the last warp
+// out (sched[1]) resets both words for the next launch.
 template <typename T>
 __global__ void __launch_bounds__(kRsBatchWarps * 32, 1)
     cb_rowseg_batch_kernel(const RsBatchMat *__restrict__ mats, const int4 *__restrict__ segs,
-                           const int4 *__restrict__ meta, const int32_t *__restrict__ wseg,
+                           const int4 *__restrict__ meta, int32_t nseg, uint32_t *sched,
                            const int2 *__restrict__ empty, int64_t nempty, const int4 *spans,
                            int32_t *counters, T *part) {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -485,10 +486,13 @@ __global__ void __launch_bounds__(kRsBatchWarps * 32, 1)
         const RsBatchMat &m = mats[e.x];
         for (int k = 0; k < m.nrhs; ++k) static_cast<T *>(m.y)[(int64_t)e.y * m.ldy + k] = T(0);
     }
-    const int w = blockIdx.x * kRsBatchWarps + wib;
     const RsSpans<T> S{spans, counters, part};
     const uint64_t pol = dev::policy_evict_first();
-    for (int si = __ldg(&wseg[w]); si < __ldg(&wseg[w + 1]); ++si) {
+    while (true) {
+        int si = 0;
+        if (lane == 0) si = (int)atomicAdd(&sched[0], 1u);
+        si = __shfl_sync(kFull, si, 0);
+        if (si >= nseg) break;
         const int4 sg = __ldg(&segs[si]);
         const RsBatchMat &m = mats[sg.x];
         const RsMat<T> A{m.chunks, m.rowmap, static_cast<const T *>(m.x), static_cast<T *>(m.y),
@@ -505,6 +509,14 @@ __global__ void __launch_bounds__(kRsBatchWarps * 32, 1)
             case 16: rs_mrhs_segment<T, GMAX, false>(A, sg.y, sg.z, mt, si, S, lane, pol); break;
             case 17: rs_mrhs_segment<T, GMAX, true>(A, sg.y, sg.z, mt, si, S, lane, pol); break;
             default: break;
+        }
+    }
+    // the last warp out resets the scheduler words for the next launch
+    if (lane == 0) {
+        __threadfence();
+        if (atomicAdd(&sched[1], 1u) == gridDim.x * kRsBatchWarps - 1) {
+            atomicExch(&sched[0], 0u);
+            atomicExch(&sched[1], 0u);
         }
     }
 }
@@ -636,17 +648,19 @@ int64_t rowseg_batch_warps(int f32) {
 }
 
 cudaError_t launch_rowseg_batch(int f32, const RsBatchMat *mats, const int4 *segs,
-                                const int4 *meta, const int32_t *wseg, int64_t nwarps,
+                                const int4 *meta, int32_t nseg, uint32_t *sched, int64_t nwarps,
                                 const int2 *empty, int64_t nempty, const int4 *spans,
                                 int32_t *counters, void *part, cudaStream_t stream) {
     if (nwarps <= 0 || nwarps % kRsBatchWarps) return cudaErrorInvalidValue;
     const unsigned grid = (unsigned)(nwarps / kRsBatchWarps);
     if (f32)
         cb_rowseg_batch_kernel<float><<<grid, kRsBatchWarps * 32, 0, stream>>>(
-            mats, segs, meta, wseg, empty, nempty, spans, counters, static_cast<float *>(part));
+            mats, segs, meta, nseg, sched, empty, nempty, spans, counters,
+            static_cast<float *>(part));
     else
         cb_rowseg_batch_kernel<double><<<grid, kRsBatchWarps * 32, 0, stream>>>(
-            mats, segs, meta, wseg, empty, nempty, spans, counters, static_cast<double *>(part));
+            mats, segs, meta, nseg, sched, empty, nempty, spans, counters,
+            static_cast<double *>(part));
     note_launch();
     return cudaGetLastError();
 }
