@@ -432,8 +432,9 @@ class Plan:
 
     def adjoint_fused(self, g, x, gx=None, gvals_t=None, stream=None):
         """(A^T g, value gradient) in one kernel launch on the transposed
-        layout; the value gradient is indexed by A^T payload position (see
-        ``grad_positions_t``).  Returns (gx, gvals_t)."""
+        layout (its row-segment stream when it has one, else its tiles); the
+        value gradient is in that layout's order (see ``grad_positions_t``).
+        Returns (gx, gvals_t)."""
         import torch
         self.upload(stream)
         self._check_dev(g, x)
@@ -451,7 +452,8 @@ class Plan:
 
     def grad_positions_t(self) -> np.ndarray:
         """For each input nonzero, its position in ``adjoint_fused``'s value
-        gradient."""
+        gradient (the order depends on the uploaded layout: uploads first)."""
+        self.upload()
         pos = np.zeros(self.nnz, np.int64)
         _check(_lib.cbspmv_grad_positions_t(self._h, _np_ptr(pos)))
         return pos

@@ -75,6 +75,7 @@ struct DevSide {
     int64_t rs_bytes = 0;
     std::vector<int32_t> rs_cinfo;  // per chunk summaries (batches cut their own segments)
     std::vector<int32_t> rs_empty;  // rows without entries
+    std::vector<int32_t> rs_vpos;   // per stored value: its stream entry (-1: none)
 
     void release() {
         void *ps[] = {tiles, blocks, payload, block_cols, partials, counters,
@@ -89,6 +90,7 @@ struct DevSide {
         rs_bytes = 0;
         rs_cinfo.clear();
         rs_empty.clear();
+        rs_vpos.clear();
         for (int32_t *&q : pat) q = nullptr;
         tiles = blocks = partials = nullptr;
         payload = nullptr;
@@ -336,6 +338,7 @@ cbspmv_status upload_rowseg(DevSide &s, int kernel, cudaStream_t st) {
                                                   R.rowmap.size() + R.empty.size()));
     s.rs_cinfo = std::move(R.cinfo);
     s.rs_empty = std::move(R.empty);
+    s.rs_vpos = std::move(R.vpos);
     return CBSPMV_OK;
 }
 
@@ -1031,6 +1034,18 @@ cbspmv_status cbspmv_adjoint(cbspmv_plan *p, const void *g, const void *x, void 
     return rc;
 }
 
+namespace {
+// The fused adjoint runs on the transposed plan's row-segment stream (its
+// value gradient then in stream order) once the plan is uploaded with one
+// that holds values and their positions; otherwise on the transposed tiles
+// (gradient in payload order).
+bool fused_on_stream(const cbspmv_plan *p) {
+    const DevSide &s = p->AT;
+    return p->uploaded && s.d.rs.chunks && !s.d.rs.unit &&
+           (int64_t)s.rs_vpos.size() == s.lay.nvals && s.lay.nvals > 0;
+}
+}  // namespace
+
 cbspmv_status cbspmv_adjoint_fused(cbspmv_plan *p, const void *g, const void *x, void *gx,
                                    void *gvals_t, int nrhs, int64_t ldg, int64_t ldx,
                                    int64_t ldgx, void *stream) {
@@ -1055,6 +1070,11 @@ cbspmv_status cbspmv_adjoint_fused(cbspmv_plan *p, const void *g, const void *x,
     if (dev != p->device) return fail(CBSPMV_ERR_STATE, "plan was uploaded to another device");
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (cbspmv_status rc = take_device_error(p, 1, st)) return rc;
+    if (fused_on_stream(p)) {
+        CB_CUDA(cb::launch_rowseg_adjoint(s.d, g, gx, nrhs, ldg, ldgx, x, ldx, gvals_t, st),
+                "fused adjoint launch");
+        return CBSPMV_OK;
+    }
     if (cbspmv_status rc = ensure_partials(s, nrhs, vsize(p))) return rc;
     CB_CUDA(cb::launch_spmm(s.d, g, gx, nrhs, ldg, ldgx, st, gvals_t, x, ldx),
             "fused adjoint launch");
@@ -1063,6 +1083,7 @@ cbspmv_status cbspmv_adjoint_fused(cbspmv_plan *p, const void *g, const void *x,
 
 int64_t cbspmv_grad_size_t(const cbspmv_plan *p) {
     if (!p || !p->has_t) return -1;
+    if (fused_on_stream(p)) return (int64_t)p->AT.d.rs.nch * cb::rs_chunk_entries();
     return (int64_t)(p->AT.lay.payload.size() / vsize(p));
 }
 
@@ -1071,6 +1092,10 @@ cbspmv_status cbspmv_grad_positions_t(const cbspmv_plan *p, int64_t *pos) {
     if (!p->has_t) return fail(CBSPMV_ERR_STATE, "plan built without want_transpose");
     if (cbspmv_status rc = refuse_spmv_only(p)) return rc;
     const cb::DeviceLayout &L = p->AT.lay;
+    if (fused_on_stream(p)) {
+        for (int64_t i = 0; i < p->host.nnz; ++i) pos[i] = p->AT.rs_vpos[L.input_slot[i]];
+        return CBSPMV_OK;
+    }
     const int64_t vsz = (int64_t)vsize(p);
     for (int64_t i = 0; i < p->host.nnz; ++i) pos[i] = (int64_t)L.val_off[L.input_slot[i]] / vsz;
     return CBSPMV_OK;

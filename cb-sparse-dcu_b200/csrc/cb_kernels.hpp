@@ -163,6 +163,14 @@ cudaError_t launch_rowseg_mrhs(const DevLayout &d, const void *x, void *y, int n
 cudaError_t launch_rowseg_values(const DevLayout &d, int64_t nvals, const uint64_t *val_off,
                                  cudaStream_t stream);
 
+// The fused adjoint over a transposed plan's stream d.rs (values stored):
+// gx = A^T g (n x nrhs, the stream's rows) and, per stream entry e of row j
+// gathering row i of g, gv[e] = sum over the right-hand sides of
+// g[i, :] . x[j, :] (gv holds nch * 128 values; padding entries get 0).
+cudaError_t launch_rowseg_adjoint(const DevLayout &d, const void *g, void *gx, int nrhs,
+                                  int64_t ldg, int64_t ldgx, const void *x, int64_t ldx,
+                                  void *gv, cudaStream_t stream);
+
 // Batches over the row-segment streams: one matrix of the device table.
 struct RsBatchMat {
     const uint8_t *chunks = nullptr;

@@ -47,6 +47,7 @@ namespace cb {
 constexpr int kRsK = 4;            // entries per lane per chunk
 constexpr int kRsWarps = 32;       // warps per CTA (one CTA per SM)
 constexpr int kRsBatchWarps = 24;  // the batch kernel's (more registers per thread)
+constexpr int kRsGvWarps = 16;     // the fused adjoint's (its gradient's registers)
 constexpr uint32_t kRsStart = 1u << 31;   // word: the entry starts a row
 constexpr uint32_t kRsWin = 1u << 30;    // word: x[column] is in the CTA's window
 constexpr uint32_t kRsColMask = (1u << 30) - 1;

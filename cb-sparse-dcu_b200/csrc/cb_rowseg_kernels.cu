@@ -265,13 +265,25 @@ struct RsSpans {
     T *part;
 };
 
+// The value gradient of a transposed stream (the fused adjoint): per stream
+// entry e of row j (a column of A) gathering row i of G, gv[e] = sum over the
+// right-hand sides of G[i, :] . xo[j, :] (written, or added when accum).
+template <typename T>
+struct RsGV {
+    const T *xo;
+    int64_t ldo;
+    int32_t xovec;  // 16-byte loads of xo rows allowed
+    int32_t accum;
+    T *gv;
+};
+
 // Chunks [cb, ce) of matrix A as segment s, meta = {ordinal running before
 // chunk cb, chunk cb starts a row, head span, tail span}.  Called by a whole
-// warp.
-template <typename T, int G, bool UNIT>
+// warp.  GV: also the value gradient of every entry (gvp).
+template <typename T, int G, bool UNIT, bool GV = false>
 __device__ __forceinline__ void rs_mrhs_segment(const RsMat<T> &A, int cb, int ce, int4 meta,
                                                 int s, const RsSpans<T> &S, int lane,
-                                                uint64_t pol) {
+                                                uint64_t pol, const RsGV<T> *gvp = nullptr) {
     using VT = typename RsVec<T>::V;
     constexpr int V = RsVec<T>::n, P = 32 / G, NV = RsVec<T>::n;
     constexpr int64_t CB = 128 * (4 + (UNIT ? 0 : (int64_t)sizeof(T)));
@@ -385,9 +397,37 @@ __device__ __forceinline__ void rs_mrhs_segment(const RsMat<T> &A, int cb, int c
             T xv[4][V];
 #pragma unroll
             for (int j = 0; j < 4; ++j) load_x(w[j] & kRsColMask, xv[j]);
+            T xo[GV ? 4 : 1][V];
+            if (GV) {  // the entries' own rows of xo (the padding row: zeros)
+                int32_t o = ord;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    o += (int32_t)(w[j] >> 31);
+                    const T *po = gvp->xo + (o < nord ? rid(o) : 0) * gvp->ldo + c0;
+                    if (o < nord && c0 < nrhs && gvp->xovec) {
+                        unpack(__ldg(reinterpret_cast<const VT *>(po)), xo[GV ? j : 0]);
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < V; ++k)
+                            xo[GV ? j : 0][k] = o < nord && c0 + k < nrhs ? __ldg(po + k) : T(0);
+                    }
+                }
+            }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const bool f = (w[j] >> 31) != 0;
+                if (GV) {  // value gradient of this entry: the group's dot product
+                    T dot = T(0);
+#pragma unroll
+                    for (int k = 0; k < V; ++k)
+                        if (c0 + k < nrhs) dot = fma(xv[j][k], xo[GV ? j : 0][k], dot);
+#pragma unroll
+                    for (int d = 1; d < G; d <<= 1) dot += __shfl_xor_sync(kFull, dot, d);
+                    if (q == 0) {
+                        T *pg = gvp->gv + (int64_t)c * 128 + 4 * ls + j;
+                        *pg = gvp->accum ? *pg + dot : dot;
+                    }
+                }
                 if (f && seen) store_y(rid(ord), run);  // a row whole inside the group
 #pragma unroll
                 for (int k = 0; k < V; ++k) {
@@ -465,6 +505,32 @@ __global__ void __launch_bounds__(kRsWarps * 32, 1)
     for (int s = sb0 + wib; s < sb1; s += kRsWarps)
         rs_mrhs_segment<T, G, UNIT>(A, s * rs.M, min(rs.nch, s * rs.M + rs.M),
                                     __ldg(&rs.meta[s]), s, S, lane, pol);
+}
+
+// The fused adjoint on a transposed stream: A^T G into y and the value
+// gradient of every entry (kRsGvWarps warps per CTA: the gradient's registers fit without
+// spills; each CTA's warps stride over its share of the segments).
+template <typename T, int G>
+__global__ void __launch_bounds__(kRsGvWarps * 32, 1)
+    cb_rowseg_gv_kernel(const RowSegDev rs, const T *__restrict__ x, T *__restrict__ y,
+                        int nrhs, int64_t ldx, int64_t ldy, int xvec, int yvec,
+                        const RsGV<T> gvp) {
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    {  // rows without entries
+        const int64_t total = (int64_t)rs.nempty * nrhs;
+        for (int64_t i = ((int64_t)blockIdx.x * kRsGvWarps + wib) * 32 + lane; i < total;
+             i += (int64_t)gridDim.x * kRsGvWarps * 32)
+            y[(int64_t)__ldg(&rs.empty[i / nrhs]) * ldy + i % nrhs] = T(0);
+    }
+    const int NB = gridDim.x, b = blockIdx.x;
+    const int sb0 = (int)((int64_t)b * rs.nseg / NB);
+    const int sb1 = (int)((int64_t)(b + 1) * rs.nseg / NB);
+    const RsMat<T> A{rs.chunks, rs.rowmap, x, y, ldx, ldy, nrhs, rs.nord, xvec, yvec};
+    const RsSpans<T> S{rs.spans, rs.counters, static_cast<T *>(rs.part)};
+    const uint64_t pol = dev::policy_evict_first();
+    for (int s = sb0 + wib; s < sb1; s += kRsGvWarps)
+        rs_mrhs_segment<T, G, false, true>(A, s * rs.M, min(rs.nch, s * rs.M + rs.M),
+                                           __ldg(&rs.meta[s]), s, S, lane, pol, &gvp);
 }
 
 // A batch over the streams (kRsBatchWarps warps per CTA: the kernel holds
@@ -632,6 +698,57 @@ cudaError_t launch_rowseg_mrhs(const DevLayout &d, const void *x, void *y, int n
                                                    static_cast<double *>(y), nrhs, ldx, ldy, stream)
                      : launch_mrhs_t<double, false>(d, static_cast<const double *>(x),
                                                     static_cast<double *>(y), nrhs, ldx, ldy, stream);
+}
+
+template <typename T, int G>
+cudaError_t launch_gv_g(const DevLayout &d, const T *g, T *gx, int r, int64_t ldg,
+                        int64_t ldgx, int xvec, int yvec, const RsGV<T> &gvp,
+                        cudaStream_t stream) {
+    const void *fn = reinterpret_cast<const void *>(cb_rowseg_gv_kernel<T, G>);
+    dev_resident_l1(fn, kRsGvWarps * 32, 0);  // sets the carveout: all L1
+    cb_rowseg_gv_kernel<T, G><<<(unsigned)d.rs.G, kRsGvWarps * 32, 0, stream>>>(
+        d.rs, g, gx, r, ldg, ldgx, xvec, yvec, gvp);
+    note_launch();
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_gv_t(const DevLayout &d, const T *g, T *gx, int nrhs, int64_t ldg,
+                        int64_t ldgx, const T *x, int64_t ldx, T *gv, cudaStream_t stream) {
+    constexpr int V = 16 / sizeof(T);
+    for (int c = 0; c < nrhs; c += kRsMaxRhs) {  // slabs of 16: the gradient adds up
+        const int r = std::min(kRsMaxRhs, nrhs - c);
+        const int xvec = ldg % V == 0 && reinterpret_cast<uintptr_t>(g + c) % 16 == 0;
+        const int yvec = ldgx % V == 0 && reinterpret_cast<uintptr_t>(gx + c) % 16 == 0;
+        const RsGV<T> gvp{x + c, ldx,
+                          (int32_t)(ldx % V == 0 && reinterpret_cast<uintptr_t>(x + c) % 16 == 0),
+                          (int32_t)(c > 0), gv};
+        const int gl = rs_lanes_per_entry(sizeof(T) == 4, r);
+        cudaError_t e;
+        switch (gl) {
+            case 1: e = launch_gv_g<T, 1>(d, g + c, gx + c, r, ldg, ldgx, xvec, yvec, gvp, stream); break;
+            case 2: e = launch_gv_g<T, 2>(d, g + c, gx + c, r, ldg, ldgx, xvec, yvec, gvp, stream); break;
+            case 4: e = launch_gv_g<T, 4>(d, g + c, gx + c, r, ldg, ldgx, xvec, yvec, gvp, stream); break;
+            default: e = launch_gv_g<T, (16 / sizeof(T) == 2 ? 8 : 4)>(
+                         d, g + c, gx + c, r, ldg, ldgx, xvec, yvec, gvp, stream);
+        }
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_rowseg_adjoint(const DevLayout &d, const void *g, void *gx, int nrhs,
+                                  int64_t ldg, int64_t ldgx, const void *x, int64_t ldx,
+                                  void *gv, cudaStream_t stream) {
+    if (!d.rs.chunks || d.rs.unit || d.rs.nseg <= 0 || d.rs.G <= 0 || nrhs < 1)
+        return cudaErrorInvalidValue;
+    if (d.f32)
+        return launch_gv_t<float>(d, static_cast<const float *>(g), static_cast<float *>(gx),
+                                  nrhs, ldg, ldgx, static_cast<const float *>(x), ldx,
+                                  static_cast<float *>(gv), stream);
+    return launch_gv_t<double>(d, static_cast<const double *>(g), static_cast<double *>(gx),
+                               nrhs, ldg, ldgx, static_cast<const double *>(x), ldx,
+                               static_cast<double *>(gv), stream);
 }
 
 int rs_lanes_per_entry(int f32, int nrhs) {

@@ -184,9 +184,12 @@ def test_finite_differences_n4096(cuda):
 @pytest.mark.parametrize("f32", [False, True])
 @pytest.mark.parametrize("nrhs", [1, 3, 8, 16, 21])
 @pytest.mark.parametrize("name", ["pl", "mixed"])
-def test_fused_adjoint(cuda, bs, f32, nrhs, name):
+@pytest.mark.parametrize("kernel", [0, 3])
+def test_fused_adjoint(cuda, bs, f32, nrhs, name, kernel):
     """cbspmv_adjoint_fused: A^T g and the value gradient in one launch on the
-    transposed layout, against the FP64 oracle (COO, CSR and DENSE blocks)."""
+    transposed layout -- its row-segment stream (kernel 0) or its tiles
+    (kernel 3, no stream) -- against the FP64 oracle (COO, CSR and DENSE
+    blocks; more than 16 right-hand sides in slabs whose gradients add)."""
     import torch
     import cbdump as cd
     from cbspmv import gen
@@ -194,7 +197,7 @@ def test_fused_adjoint(cuda, bs, f32, nrhs, name):
         coo = gen.power_law(4096, kmax=4096, band=256, seed=3, mean=24)
     else:  # stencil rows: CSR blocks, and dense couplings
         coo = gen.stencil_27pt(6)
-    plan = _plan(coo, f32, block_size=bs, tile_entries=128)
+    plan = _plan(coo, f32, block_size=bs, tile_entries=128, kernel=kernel)
     dt = torch.float32 if f32 else torch.float64
     tol = 1e-5 if f32 else 1e-12
     G = gen.uniform_x(coo.m, 41, nrhs=max(nrhs, 2))[:nrhs]
