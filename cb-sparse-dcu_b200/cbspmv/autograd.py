@@ -6,11 +6,12 @@ caller's COO order) and X is (n,) or (n, k).  Backward:
 * dL/dX    = A^T dL/dY, on the plan's transposed CB layout (build the plan
   with ``want_transpose=1``);
 * dL/dvals = for each input nonzero k, dL/dY[row_k, :] . X[col_k, :],
-  computed per stored value in the same launch as A^T dL/dY
-  (``adjoint_fused``) and gathered back to input order through
-  ``grad_positions_t`` -- every input is summed into exactly one stored
-  value, so that value's gradient is the input's gradient.  (Without the
-  transposed layout: ``grad_vals`` per slot of A and ``input_slots``.)
+  computed per stored value of A (``adjoint``: the value-gradient kernel on
+  a second stream beside A^T dL/dY, the faster of the library's two adjoint
+  forms on the stream layouts) and gathered back to input order through
+  ``input_slots`` -- every input is summed into exactly one stored value, so
+  that value's gradient is the input's gradient.  ``adjoint_fused`` (one
+  launch, gradient gathered through ``grad_positions_t``) computes the same.
 
 Build the plan with ``keep_values=1`` when its initial values may all be 1:
 a unit-valued plan stores no values and cannot take new ones.
@@ -37,17 +38,8 @@ class CBSpMVFunction(torch.autograd.Function):
         want_gx, want_v = ctx.needs_input_grad[1], ctx.needs_input_grad[0]
         if not (want_gx or want_v):
             return None, None, None
-        if want_v and plan.has_transpose:
-            # one launch on the transposed layout: A^T g and the value gradient
-            # (by A^T payload position) from the same gathered rows of g
-            gx, gpay = plan.adjoint_fused(gy, x.contiguous())
-            pos = getattr(plan, "_gpos_dev", None)
-            if pos is None or pos.device != gy.device:
-                pos = torch.from_numpy(plan.grad_positions_t()).to(gy.device)
-                plan._gpos_dev = pos
-            return gpay[pos], (gx if want_gx else None), None
-        # otherwise both in one call: the value gradient overlaps A^T g on a
-        # second stream
+        # both in one call: the value gradient overlaps A^T g on a second
+        # stream
         gx, gslots = plan.adjoint(gy, x.contiguous(), want_gx=want_gx, want_gvals=want_v)
         gvals = None
         if want_v:

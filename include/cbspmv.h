@@ -192,7 +192,11 @@ cbspmv_status cbspmv_spmv(cbspmv_plan *plan, const void *x, void *y, int nrhs,
  * address; make that first call before any stream capture.  All calls share
  * the array and it keeps the last call's contents (the counters are cleared
  * at the start of every call), so calls that overlap on the GPU -- on
- * different streams, or from different plans -- race. */
+ * different streams, or from different plans -- race.  The looked-up address
+ * is kept for the process: do not use this call after a device reset
+ * (cudaDeviceReset) in the same process.  Plans whose kernel is the
+ * row-segment stream need no scratch from the array (their span counters
+ * and slots are the plan's own, allocated at upload). */
 cbspmv_status cbspmv_spmv_noalloc(cbspmv_plan *plan, const void *x, void *y,
                                   int nrhs, int64_t ldx, int64_t ldy,
                                   void *stream);
