@@ -76,6 +76,9 @@ struct DevSide {
     std::vector<int32_t> rs_cinfo;  // per chunk summaries (batches cut their own segments)
     std::vector<int32_t> rs_empty;  // rows without entries
     std::vector<int32_t> rs_vpos;   // per stored value: its stream entry (-1: none)
+    // balanced schedule (row_owned = 0 plans): rows, cols, vals, gstart, eoff
+    void *bal[5] = {};
+    int64_t bal_bytes = 0;
 
     void release() {
         void *ps[] = {tiles, blocks, payload, block_cols, partials, counters,
@@ -88,6 +91,11 @@ struct DevSide {
             q = nullptr;
         }
         rs_bytes = 0;
+        for (void *&q : bal) {
+            if (q) cudaFree(q);
+            q = nullptr;
+        }
+        bal_bytes = 0;
         rs_cinfo.clear();
         rs_empty.clear();
         rs_vpos.clear();
@@ -342,6 +350,32 @@ cbspmv_status upload_rowseg(DevSide &s, int kernel, cudaStream_t st) {
     return CBSPMV_OK;
 }
 
+// The balanced schedule's stream (kernel 6, and the automatic choice for one
+// right-hand side) of a plan built with row_owned = 0 and stored values.
+cbspmv_status upload_balanced(DevSide &s, const cb::HostCB &g, int kernel, cudaStream_t st) {
+    if ((kernel != 0 && kernel != 6) || g.o.row_owned || s.lay.unit || s.lay.nvals <= 0 ||
+        g.gb_row.empty())
+        return CBSPMV_OK;
+    cb::BalancedHost B;
+    const std::string msg = cb::build_balanced(s.lay, g, B);
+    if (!msg.empty()) return fail(CBSPMV_ERR_UNSUPPORTED, msg);
+    CB_CUDA(upload_vec(B.rows, (uint32_t **)&s.bal[0], st), "upload balanced stream");
+    CB_CUDA(upload_vec(B.cols, (uint32_t **)&s.bal[1], st), "upload balanced stream");
+    CB_CUDA(upload_vec(B.vals, (uint8_t **)&s.bal[2], st), "upload balanced stream");
+    CB_CUDA(upload_vec(B.gstart, (int64_t **)&s.bal[3], st), "upload balanced stream");
+    CB_CUDA(upload_vec(B.eoff, (int64_t **)&s.bal[4], st), "upload balanced stream");
+    cb::BalancedDev &d = s.d.bal;
+    d.rows = static_cast<const uint4 *>(s.bal[0]);
+    d.cols = static_cast<const uint4 *>(s.bal[1]);
+    d.vals = s.bal[2];
+    d.gstart = static_cast<const int64_t *>(s.bal[3]);
+    d.eoff = static_cast<const int64_t *>(s.bal[4]);
+    d.ngroups = (int64_t)B.gstart.size() - 1;
+    d.nquads = B.nquads;
+    s.bal_bytes = (int64_t)(B.rows.size() * 8 + B.vals.size() + B.gstart.size() * 8);
+    return CBSPMV_OK;
+}
+
 // The row patterns of a unit-valued plan (the reference's pattern_* arrays,
 // coo2block.h:566-602) for the pattern-reuse schedule; its automatic choice
 // follows the reference's rule: fewer patterns than half the rows
@@ -461,8 +495,8 @@ cbspmv_status cbspmv_coo2block_gather(const cbspmv_coo *coo,
     if (opts) o = *opts;
     if (o.value_type != CBSPMV_F64 && o.value_type != CBSPMV_F32)
         return fail(CBSPMV_ERR_INVALID, "value_type must be CBSPMV_F64 or CBSPMV_F32");
-    if (o.kernel < 0 || o.kernel > 5)
-        return fail(CBSPMV_ERR_INVALID, "kernel must be 0 (auto), 1, 2, 3, 4 or 5");
+    if (o.kernel < 0 || o.kernel > 6)
+        return fail(CBSPMV_ERR_INVALID, "kernel must be 0 (auto) or 1 to 6");
     cbspmv_plan *p = new (std::nothrow) cbspmv_plan;
     if (!p) return fail(CBSPMV_ERR_ALLOC, "out of host memory");
     p->opts = o;
@@ -618,7 +652,7 @@ cbspmv_status cbspmv_plan_load(const char *path, cbspmv_plan **out) {
     p->has_t = img.has_t != 0;
     if ((o.block_size != 16 && o.block_size != 32) ||
         (o.value_type != CBSPMV_F64 && o.value_type != CBSPMV_F32) || o.kernel < 0 ||
-        o.kernel > 5 || p->A.lay.bs != o.block_size) {
+        o.kernel > 6 || p->A.lay.bs != o.block_size) {
         delete p;
         return fail(CBSPMV_ERR_INVALID, std::string(path) + " holds inconsistent options");
     }
@@ -640,6 +674,7 @@ cbspmv_status cbspmv_upload(cbspmv_plan *p, void *stream) {
     if (!rc) rc = upload_partition(p->A, p->opts.kernel, st);
     if (!rc) rc = upload_patterns(p->A, p->host, st);
     if (!rc) rc = upload_rowseg(p->A, p->opts.kernel, st);
+    if (!rc && !p->spmv_only) rc = upload_balanced(p->A, p->host, p->opts.kernel, st);
     if (!rc && p->has_t) rc = upload_side(p->AT, st);
     if (!rc && p->has_t) rc = upload_partition(p->AT, p->opts.kernel, st);
     if (!rc && p->has_t) rc = upload_rowseg(p->AT, p->opts.kernel, st);
@@ -732,6 +767,7 @@ cbspmv_status cbspmv_autotune_ex(cbspmv_plan *p, int nrhs, void *stream, int *ke
         cands.push_back({3, 0});
         if (s.d.npat) cands.push_back({4, 0});
         if (s.d.rs.chunks) cands.push_back({5, 0});
+        if (s.d.bal.rows) cands.push_back({6, 0});
     } else {
         for (int rl : {0, 1, 2, 4}) cands.push_back({3, rl});
         if (s.d.rs.chunks) cands.push_back({5, 0});
@@ -1121,6 +1157,7 @@ cbspmv_status cbspmv_set_values(cbspmv_plan *p, const void *input_values,
                 "set_values launch");
         CB_CUDA(cb::launch_rowseg_values(s->d, s->lay.nvals, s->val_off, st),
                 "set_values launch");
+        CB_CUDA(cb::launch_balanced_values(s->d, st), "set_values launch");
     }
     return CBSPMV_OK;
 }
@@ -1180,7 +1217,7 @@ cbspmv_status cbspmv_info_get(const cbspmv_plan *p, cbspmv_info *info) {
     I.device_bytes = (int64_t)(p->A.lay.tiles.size() * sizeof(cb::TileDesc) +
                                p->A.lay.blocks.size() * sizeof(cb::BlockDesc) +
                                p->A.lay.payload.size() + p->A.lay.block_cols.size() * 4) +
-                     p->A.rs_bytes;
+                     p->A.rs_bytes + p->A.bal_bytes;
     I.algorithmic_bytes = p->A.lay.alg_bytes;
     I.rowseg_bytes = p->A.rs_bytes;
     I.scratch_bytes = (int64_t)(p->A.lay.slots * p->A.lay.bs * vsize(p) +
@@ -1250,9 +1287,29 @@ bool exportable(const cbspmv_plan *p, const std::string &k) {
     return ok;
 }
 
+namespace {
+// The balanced schedule's stream of A (plans built with row_owned = 0):
+// bal_rows, bal_cols (uint32, 4 per quad), bal_vals (the value type) and
+// bal_gstart (int64, per group its first quad, then the quad count).
+int64_t export_balanced(const cbspmv_plan *p, const std::string &k, void *out) {
+    cb::BalancedHost B;
+    if (!cb::build_balanced(p->A.lay, p->host, B).empty()) return -1;
+    auto raw = [&](const void *src, size_t bytes, size_t unit) -> int64_t {
+        if (out && bytes) std::memcpy(out, src, bytes);
+        return (int64_t)(bytes / unit);
+    };
+    if (k == "bal_rows") return raw(B.rows.data(), B.rows.size() * 4, 4);
+    if (k == "bal_cols") return raw(B.cols.data(), B.cols.size() * 4, 4);
+    if (k == "bal_vals") return raw(B.vals.data(), B.vals.size(), B.f32 ? 4 : 8);
+    if (k == "bal_gstart") return raw(B.gstart.data(), B.gstart.size() * 8, 8);
+    return -1;
+}
+}  // namespace
+
 int64_t cbspmv_export(const cbspmv_plan *p, const char *name, void *out) {
     if (!p || !name) return -1;
     const std::string k(name);
+    if (k.rfind("bal_", 0) == 0) return p->spmv_only ? -1 : export_balanced(p, k, out);
     if (!exportable(p, k)) return -1;
     if (k.rfind("dev_", 0) == 0 || k.rfind("rs_", 0) == 0)
         return export_device(p->A.lay, k, out);

@@ -794,6 +794,10 @@ cudaError_t launch_tiles(const DevLayout &d, const void *x, void *y, int nrhs,
     // the row-segment stream: when chosen, and the automatic choice for
     // all-COO layouts except the reference's small-direct case
     const bool one = nrhs == 1 && ldx == 1 && ldy == 1;
+    // the balanced schedule: plans built with row_owned = 0 (the reference's
+    // non-row-owned mode), one right-hand side
+    if (one && d.bal.rows && (d.kernel == 6 || d.kernel == 0))
+        return launch_balanced(d, x, y, stream);
     if (d.rs.chunks && (d.kernel == 5 || (d.kernel == 0 && !d.small_direct &&
                                           !use_pattern(d) && (!one || d.rs.auto1))))
         return one ? launch_rowseg(d, x, y, stream)

@@ -28,6 +28,16 @@ struct RowSegDev {
     int auto1 = 0;                    // the automatic choice for one right-hand side
 };
 
+// The balanced schedule's stream on the device (cb_rowseg.hpp,
+// BalancedHost); rows is NULL when the plan has none.
+struct BalancedDev {
+    const uint4 *rows = nullptr, *cols = nullptr;  // 4 entries per quad
+    const void *vals = nullptr;                    // 4 values per quad
+    const int64_t *gstart = nullptr;               // ngroups + 1 quad indices
+    const int64_t *eoff = nullptr;                 // per entry: payload offset (-1: skip)
+    int64_t ngroups = 0, nquads = 0;
+};
+
 // Device-resident pieces of one DeviceLayout (cb_layout.hpp).
 struct DevLayout {
     const void *tiles = nullptr;      // TileDesc[ntiles]
@@ -57,8 +67,10 @@ struct DevLayout {
     int small_direct = 0;
     int64_t max_entries = 0;          // largest COO section of a tile
     int kernel = 0;                   // 0 auto, 1 streaming (TMA), 2 direct, 3 several
-                                      // right-hand sides, 4 pattern reuse, 5 row segments
+                                      // right-hand sides, 4 pattern reuse, 5 row segments,
+                                      // 6 balanced
     RowSegDev rs;                     // row-segment stream (kernel 5)
+    BalancedDev bal;                  // balanced schedule (kernel 6; row_owned = 0)
     double coo_share = 1.0;
     const uint32_t *wpart = nullptr;  // streaming: per-warp tile ranges
     int64_t nwarps = 0;               // streaming: warps of the launch
@@ -170,6 +182,11 @@ cudaError_t launch_rowseg_values(const DevLayout &d, int64_t nvals, const uint64
 cudaError_t launch_rowseg_adjoint(const DevLayout &d, const void *g, void *gx, int nrhs,
                                   int64_t ldg, int64_t ldgx, const void *x, int64_t ldx,
                                   void *gv, cudaStream_t stream);
+
+// y = A x by the balanced schedule over d.bal (zeroes y, then one launch
+// adding with atomics); its values refreshed from the tile payload.
+cudaError_t launch_balanced(const DevLayout &d, const void *x, void *y, cudaStream_t stream);
+cudaError_t launch_balanced_values(const DevLayout &d, cudaStream_t stream);
 
 // Batches over the row-segment streams: one matrix of the device table.
 struct RsBatchMat {

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <climits>
 #include <cstring>
+#include <unordered_map>
 #include <utility>
 
 namespace cb {
@@ -50,23 +51,15 @@ void rowseg_cut(const std::vector<int32_t> &cinfo, const std::vector<int64_t> &c
     }
 }
 
-std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
-    if (!rowseg_applies(L)) return "the layout does not take the row-segment stream";
-    const int64_t m = L.m, C = rs_chunk_entries();
-    const int f32 = L.f32;
+// Every stored entry of the tiles with the payload offset of its value: the
+// COO sections, then CSR blocks (row pointers, block-local columns resolved
+// through the gather list) and DENSE blocks (columns below the block's valid
+// count; unit-valued layouts: the bits set in the mask).
+void tile_entries(const DeviceLayout &L, std::vector<int32_t> &erow, std::vector<int32_t> &ecol,
+                  std::vector<int64_t> &eoff) {
+    const int64_t m = L.m;
     const int unit = L.unit;
-    const int64_t vsz = f32 ? 4 : 8, CB = rs_chunk_bytes(f32, unit);
-    R = RowSegHost();
-    R.f32 = f32;
-    R.unit = unit;
-    R.m = m;
-    R.n = L.n;
-    // every stored entry of the tiles, with the payload offset of its value:
-    // the COO sections, then CSR blocks (row pointers, block-local columns
-    // resolved through the gather list) and DENSE blocks (columns below the
-    // block's valid count; unit-valued layouts: the bits set in the mask)
-    std::vector<int32_t> erow, ecol;
-    std::vector<int64_t> eoff;
+    const int64_t vsz = L.f32 ? 4 : 8;
     erow.reserve((size_t)L.nvals);
     ecol.reserve((size_t)L.nvals);
     eoff.reserve((size_t)L.nvals);
@@ -123,6 +116,22 @@ std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
             }
         }
     }
+}
+
+std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
+    if (!rowseg_applies(L)) return "the layout does not take the row-segment stream";
+    const int64_t m = L.m, C = rs_chunk_entries();
+    const int f32 = L.f32;
+    const int unit = L.unit;
+    const int64_t vsz = f32 ? 4 : 8, CB = rs_chunk_bytes(f32, unit);
+    R = RowSegHost();
+    R.f32 = f32;
+    R.unit = unit;
+    R.m = m;
+    R.n = L.n;
+    std::vector<int32_t> erow, ecol;
+    std::vector<int64_t> eoff;
+    tile_entries(L, erow, ecol, eoff);
     const int64_t nv = (int64_t)erow.size();
     if (nv == 0) return "row-segment stream: no entries";
     for (int64_t k2 = 0; k2 < nv; ++k2)  // every gather stays inside x, every row inside y
@@ -261,6 +270,91 @@ std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R) {
         }
     }
     R.alg_bytes = L.alg_bytes;
+    return "";
+}
+
+}  // namespace cb
+
+namespace cb {
+
+std::string build_balanced(const DeviceLayout &L, const HostCB &g, BalancedHost &B) {
+    if (g.o.row_owned || L.unit) return "the plan is row-owned or stores no values";
+    if (L.n > kRsMaxCols || L.m >= (int64_t(1) << 31)) return "matrix too large";
+    const int bs = L.bs, W = g.o.waves;
+    const int64_t vsz = L.f32 ? 4 : 8;
+    B = BalancedHost();
+    B.f32 = L.f32;
+    std::vector<int32_t> erow, ecol;
+    std::vector<int64_t> eoff;
+    tile_entries(L, erow, ecol, eoff);
+    const int64_t ne = (int64_t)erow.size();
+    for (int64_t k = 0; k < ne; ++k)
+        if (ecol[(size_t)k] < 0 || ecol[(size_t)k] >= L.n || erow[(size_t)k] < 0 ||
+            erow[(size_t)k] >= L.m)
+            return "balanced stream: an entry outside the matrix";
+    // each entry's block (block row, block column in the gathered space) and
+    // that block's place in the balanced order
+    std::unordered_map<uint64_t, int32_t> gpos;  // (block row, column) -> gathered position
+    if (g.gather_flag)
+        for (int64_t R = 0; R < g.gb_m; ++R)
+            for (int32_t p = g.block_cols_offset[(size_t)R]; p < g.block_cols_offset[(size_t)R + 1];
+                 ++p)
+                gpos[(uint64_t)R << 32 | (uint32_t)g.block_cols[(size_t)p]] =
+                    p - g.block_cols_offset[(size_t)R];
+    std::unordered_map<uint64_t, int64_t> bpos;  // (block row, block column) -> balanced index
+    const int64_t nb = (int64_t)g.gb_row.size();
+    for (int64_t i = 0; i < nb; ++i)
+        if (g.gb_row[(size_t)i] >= 0)
+            bpos[(uint64_t)g.gb_row[(size_t)i] << 32 | (uint32_t)g.gb_col[(size_t)i]] = i;
+    std::vector<int64_t> blk((size_t)ne);
+    for (int64_t k = 0; k < ne; ++k) {
+        const int64_t R = erow[(size_t)k] / bs;
+        int64_t C;
+        if (g.gather_flag) {
+            auto it = gpos.find((uint64_t)R << 32 | (uint32_t)ecol[(size_t)k]);
+            if (it == gpos.end()) return "balanced stream: a column outside its gather list";
+            C = it->second / bs;
+        } else {
+            C = ecol[(size_t)k] / bs;
+        }
+        auto it = bpos.find((uint64_t)R << 32 | (uint32_t)C);
+        if (it == bpos.end()) return "balanced stream: an entry outside every block";
+        blk[(size_t)k] = it->second;
+    }
+    // entries by (balanced block, row, column)
+    std::vector<int64_t> order((size_t)ne);
+    for (int64_t k = 0; k < ne; ++k) order[(size_t)k] = k;
+    std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) {
+        if (blk[(size_t)a] != blk[(size_t)b]) return blk[(size_t)a] < blk[(size_t)b];
+        if (erow[(size_t)a] != erow[(size_t)b]) return erow[(size_t)a] < erow[(size_t)b];
+        return ecol[(size_t)a] < ecol[(size_t)b];
+    });
+    // groups of W consecutive balanced blocks (the reference's CTAs), each
+    // padded to whole quads with skip entries
+    const int64_t ngroups = (nb + W - 1) / W;
+    B.gstart.assign((size_t)ngroups + 1, 0);
+    int64_t k = 0, quads = 0;
+    for (int64_t gi = 0; gi < ngroups; ++gi) {
+        B.gstart[(size_t)gi] = quads;
+        const int64_t k0 = k;
+        while (k < ne && blk[(size_t)order[(size_t)k]] / W == gi) ++k;
+        const int64_t cnt = k - k0, nq = (cnt + 3) / 4;
+        for (int64_t e = 0; e < nq * 4; ++e) {
+            const bool real = e < cnt;
+            const int64_t v = real ? order[(size_t)(k0 + e)] : -1;
+            B.rows.push_back(real ? (uint32_t)erow[(size_t)v] : kBalSkip);
+            B.cols.push_back(real ? (uint32_t)ecol[(size_t)v] : 0u);
+            B.eoff.push_back(real ? eoff[(size_t)v] : -1);
+        }
+        quads += nq;
+    }
+    B.gstart[(size_t)ngroups] = quads;
+    B.nquads = quads;
+    B.vals.assign((size_t)(quads * 4 * vsz), 0);
+    for (int64_t e = 0; e < quads * 4; ++e)
+        if (B.eoff[(size_t)e] >= 0)
+            std::memcpy(B.vals.data() + e * vsz, L.payload.data() + B.eoff[(size_t)e],
+                        (size_t)vsz);
     return "";
 }
 

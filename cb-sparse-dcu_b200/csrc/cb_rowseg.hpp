@@ -117,4 +117,26 @@ void rowseg_cut(const std::vector<int32_t> &cinfo, const std::vector<int64_t> &c
 // the same stream, so the same sums.  Returns "" or an error.
 std::string build_rowseg(const DeviceLayout &L, int64_t warps, RowSegHost &R);
 
+// The balanced (non-row-owned) schedule of a plan built with row_owned = 0:
+// the stored entries in the plan's block order -- the reference's balanced
+// order (the builder's permutation, coo2block.h:382-498) when it balanced
+// (nnz >= 10000), else the build order -- sorted by row within a block, grouped
+// as the reference groups blocks (waves_per_block blocks per group, its CTA)
+// and padded to quads of 4 entries with skip entries (row kBalSkip).  A warp
+// takes whole groups and adds each run of one row into y with an atomic
+// (the reference's accumulate_output without CB_ROW_OWNED,
+// cb-spmv-dcu.hpp:149-157), so the sums' order is not fixed.
+constexpr uint32_t kBalSkip = 0xffffffffu;
+struct BalancedHost {
+    int f32 = 0;
+    int64_t nquads = 0;
+    std::vector<uint32_t> rows, cols;  // 4 per quad
+    std::vector<uint8_t> vals;         // 4 values per quad
+    std::vector<int64_t> eoff;         // per entry: its value's payload offset (-1: skip)
+    std::vector<int64_t> gstart;       // per group: first quad, then the quad count
+};
+// "" or an error (no permutation, unit values: the plan keeps the row-owned
+// kernels).
+std::string build_balanced(const DeviceLayout &L, const HostCB &g, BalancedHost &B);
+
 }  // namespace cb

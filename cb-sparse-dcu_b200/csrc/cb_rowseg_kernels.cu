@@ -606,6 +606,66 @@ __global__ void cb_rowseg_values_kernel(const RowSegDev rs, const uint8_t *__res
     }
 }
 
+
+// The balanced schedule (plans built with row_owned = 0): warps take whole
+// groups (the reference's CTAs of waves_per_block blocks, balanced by its
+// permutation), each lane a quad of 4 entries at a time; a run of one row
+// inside the quad is summed in registers and added into y with an atomic
+// (the reference's accumulate_output without CB_ROW_OWNED,
+// cb-spmv-dcu.hpp:149-157).  y is zeroed before the launch.
+constexpr int kBalWarps = 8;
+template <typename T>
+__global__ void __launch_bounds__(kBalWarps * 32)
+    cb_balanced_kernel(const BalancedDev b, const T *__restrict__ x, T *__restrict__ y) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = (int64_t)gridDim.x * kBalWarps;
+    for (int64_t g = (int64_t)blockIdx.x * kBalWarps + (threadIdx.x >> 5); g < b.ngroups;
+         g += nw) {
+        const int64_t q1 = __ldg(&b.gstart[g + 1]);
+        for (int64_t q = __ldg(&b.gstart[g]) + lane; q < q1; q += 32) {
+            const uint4 r4 = __ldg(&b.rows[q]), c4 = __ldg(&b.cols[q]);
+            const uint32_t r[4] = {r4.x, r4.y, r4.z, r4.w}, c[4] = {c4.x, c4.y, c4.z, c4.w};
+            T v[4];
+            if (sizeof(T) == 4) {
+                unpack(__ldg(reinterpret_cast<const float4 *>(b.vals) + q),
+                       reinterpret_cast<float *>(v));
+            } else {
+                unpack(__ldg(reinterpret_cast<const double2 *>(b.vals) + 2 * q),
+                       reinterpret_cast<double *>(v));
+                unpack(__ldg(reinterpret_cast<const double2 *>(b.vals) + 2 * q + 1),
+                       reinterpret_cast<double *>(v) + 2);
+            }
+            T xv[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) xv[j] = r[j] != kBalSkip ? __ldg(x + c[j]) : T(0);
+            uint32_t rr = r[0];
+            T run = v[0] * xv[0];
+#pragma unroll
+            for (int j = 1; j < 4; ++j) {
+                if (r[j] == rr) {
+                    run = fma(v[j], xv[j], run);
+                } else {
+                    if (rr != kBalSkip) atomicAdd(&y[rr], run);
+                    rr = r[j];
+                    run = v[j] * xv[j];
+                }
+            }
+            if (rr != kBalSkip) atomicAdd(&y[rr], run);
+        }
+    }
+}
+
+// Balanced stream values refreshed from the tile payload (skip entries 0).
+template <typename T>
+__global__ void cb_balanced_values_kernel(const BalancedDev b, const uint8_t *__restrict__ payload) {
+    T *vals = static_cast<T *>(const_cast<void *>(b.vals));
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < 4 * b.nquads;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t off = __ldg(&b.eoff[e]);
+        vals[e] = off >= 0 ? *reinterpret_cast<const T *>(payload + off) : T(0);
+    }
+}
+
 }  // namespace
 
 template <typename T, bool UNIT>
@@ -749,6 +809,38 @@ cudaError_t launch_rowseg_adjoint(const DevLayout &d, const void *g, void *gx, i
     return launch_gv_t<double>(d, static_cast<const double *>(g), static_cast<double *>(gx),
                                nrhs, ldg, ldgx, static_cast<const double *>(x), ldx,
                                static_cast<double *>(gv), stream);
+}
+
+cudaError_t launch_balanced(const DevLayout &d, const void *x, void *y, cudaStream_t stream) {
+    if (!d.bal.rows) return cudaErrorInvalidValue;
+    const size_t vsz = d.f32 ? 4 : 8;
+    cudaError_t e = cudaMemsetAsync(y, 0, (size_t)d.m * vsz, stream);
+    if (e != cudaSuccess) return e;
+    const void *fn = d.f32 ? reinterpret_cast<const void *>(cb_balanced_kernel<float>)
+                           : reinterpret_cast<const void *>(cb_balanced_kernel<double>);
+    const int64_t grid = std::max<int64_t>(
+        1, std::min<int64_t>((d.bal.ngroups + kBalWarps - 1) / kBalWarps,
+                             (int64_t)dev_sms() * dev_resident(fn, kBalWarps * 32, 0)));
+    if (d.f32)
+        cb_balanced_kernel<float><<<(unsigned)grid, kBalWarps * 32, 0, stream>>>(
+            d.bal, static_cast<const float *>(x), static_cast<float *>(y));
+    else
+        cb_balanced_kernel<double><<<(unsigned)grid, kBalWarps * 32, 0, stream>>>(
+            d.bal, static_cast<const double *>(x), static_cast<double *>(y));
+    note_launch();
+    return cudaGetLastError();
+}
+
+cudaError_t launch_balanced_values(const DevLayout &d, cudaStream_t stream) {
+    if (!d.bal.rows || !d.bal.eoff || d.bal.nquads <= 0) return cudaSuccess;
+    const unsigned grid =
+        (unsigned)std::min<int64_t>((4 * d.bal.nquads + 255) / 256, (int64_t)dev_sms() * 16);
+    if (d.f32)
+        cb_balanced_values_kernel<float><<<grid, 256, 0, stream>>>(d.bal, d.payload);
+    else
+        cb_balanced_values_kernel<double><<<grid, 256, 0, stream>>>(d.bal, d.payload);
+    note_launch();
+    return cudaGetLastError();
 }
 
 int rs_lanes_per_entry(int f32, int nrhs) {

@@ -73,7 +73,13 @@ typedef struct cbspmv_opts {
                              at upload, and the automatic choice, when every
                              block is a COO block and values are stored;
                              keeps a second copy of the values on the
-                             device); see cbspmv_autotune */
+                             device), 6 balanced (plans built with row_owned
+                             = 0 and stored values: the entries in the
+                             plan's block order, grouped as the reference's
+                             CTAs, added into y with atomics as its
+                             non-row-owned mode does; the automatic choice
+                             for one right-hand side on such plans); see
+                             cbspmv_autotune */
     int keep_values;      /* 0 (default): when every stored value is 1, store
                              no values and DENSE blocks as bitmasks, as the
                              reference does (UNIT_VALUES,
@@ -287,7 +293,9 @@ cbspmv_status cbspmv_info_get(const cbspmv_plan *plan, cbspmv_info *info);
  * nord, G, W), rs_chunks (bytes), rs_meta, rs_spans, rs_rowmap, rs_empty,
  * rs_vpos and rs_wbase (int32), each
  * followed by ":W", the row-segment stream as built for W resident warps
- * (-1 when the layout does not take it). */
+ * (-1 when the layout does not take it); bal_rows, bal_cols (uint32), bal_vals
+ * (the value type) and bal_gstart (int64), the balanced schedule's stream
+ * of a plan built with row_owned = 0 (-1 otherwise). */
 int64_t cbspmv_export(const cbspmv_plan *plan, const char *name, void *out);
 
 /* The same for the CB structure of A^T (plans built with want_transpose). */
