@@ -270,6 +270,11 @@ def secondary_configs(dev, peak: float, want=("lap", "pl32", "st", "diff", "bat"
         single("PL fp64 unit values (value-free payload)",
                gen.Coo(pl.m, pl.n, pl.row, pl.col, np.ones(pl.nnz)), False)
         del pl
+    if "unit" in want:  # the balanced schedule (the reference's load-balance ablation)
+        try:
+            balanced_config(dev, peak, out)
+        except Exception as exc:  # informative only: never breaks the bench line
+            out["PL fp64 balanced (row_owned = 0)"] = {"unavailable": str(exc)[:200]}
     if "st" in want:
         st = gen.stencil_27pt()
         single("ST fp64 (64^3 x 3 dof 27-point)", st, False, reps=20, bsr=True)
@@ -280,6 +285,37 @@ def secondary_configs(dev, peak: float, want=("lap", "pl32", "st", "diff", "bat"
     if "bat" in want:
         bat_config(dev, peak, bat_count, out)
     return out
+
+
+def balanced_config(dev, peak, out):
+    """PL FP64 built with row_owned = 0: the balanced schedule (kernel 6:
+    the entries in the reference's balanced block order, added into y with
+    atomics, as its non-row-owned mode) beside the same plan's row-owned
+    kernel (kernel 5), each checked against the oracle."""
+    import numpy as np
+    import torch
+    import cbspmv
+    from cbspmv import gen
+    cd = _oracle()
+    coo = gen.power_law()
+    xh = gen.uniform_x(coo.n, 0)
+    x = torch.from_numpy(xh).to(dev)
+    yref, ab = cd.oracle_spmm_ld(coo, xh[None, :])
+    r = {"nnz": coo.nnz, "l2": "inputs larger than L2", "parity": {}}
+    for kernel, name in ((6, "balanced"), (5, "row_owned_stream")):
+        plan = cbspmv.Plan(coo, row_owned=0, kernel=kernel)
+        y = torch.empty(coo.m, dtype=torch.float64, device=dev)
+        alg = plan.info()["algorithmic_bytes"]
+        ms = _timed(lambda: plan.spmv(x, y), 100, 5)
+        plan.check()
+        r[name + "_ms"] = round(ms, 4)
+        r[name + "_gbs"] = round(alg / ms / 1e6, 1)
+        r[name + "_frac"] = round(alg / ms / 1e6 / peak, 4)
+        r["parity"][name] = _parity(y.cpu().numpy()[None, :], yref, ab, False)
+        r["load_stddev_before_after"] = [round(plan.info()["load_stddev_before"], 2),
+                                         round(plan.info()["load_stddev_after"], 2)]
+        del plan
+    out["PL fp64 balanced (row_owned = 0)"] = r
 
 
 def _cusparse():

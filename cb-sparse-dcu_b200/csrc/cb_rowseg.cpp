@@ -4,7 +4,6 @@
 #include <algorithm>
 #include <climits>
 #include <cstring>
-#include <unordered_map>
 #include <utility>
 
 namespace cb {
@@ -293,34 +292,47 @@ std::string build_balanced(const DeviceLayout &L, const HostCB &g, BalancedHost 
             erow[(size_t)k] >= L.m)
             return "balanced stream: an entry outside the matrix";
     // each entry's block (block row, block column in the gathered space) and
-    // that block's place in the balanced order
-    std::unordered_map<uint64_t, int32_t> gpos;  // (block row, column) -> gathered position
-    if (g.gather_flag)
-        for (int64_t R = 0; R < g.gb_m; ++R)
-            for (int32_t p = g.block_cols_offset[(size_t)R]; p < g.block_cols_offset[(size_t)R + 1];
-                 ++p)
-                gpos[(uint64_t)R << 32 | (uint32_t)g.block_cols[(size_t)p]] =
-                    p - g.block_cols_offset[(size_t)R];
-    std::unordered_map<uint64_t, int64_t> bpos;  // (block row, block column) -> balanced index
+    // that block's place in the block order: sorted tables searched by
+    // binary search (the gather lists can be as long as the entries)
+    std::vector<std::pair<int32_t, int32_t>> gcol;  // per block row: (column, position), by column
+    if (g.gather_flag) {
+        gcol.resize(g.block_cols.size());
+        for (int64_t R = 0; R < g.gb_m; ++R) {
+            const int32_t o0 = g.block_cols_offset[(size_t)R], o1 = g.block_cols_offset[(size_t)R + 1];
+            for (int32_t q = o0; q < o1; ++q) gcol[(size_t)q] = {g.block_cols[(size_t)q], q - o0};
+            std::sort(gcol.begin() + o0, gcol.begin() + o1);
+        }
+    }
+    std::vector<std::pair<uint64_t, int64_t>> bkey;  // ((block row, block column), index), sorted
     const int64_t nb = (int64_t)g.gb_row.size();
     for (int64_t i = 0; i < nb; ++i)
         if (g.gb_row[(size_t)i] >= 0)
-            bpos[(uint64_t)g.gb_row[(size_t)i] << 32 | (uint32_t)g.gb_col[(size_t)i]] = i;
+            bkey.push_back({(uint64_t)g.gb_row[(size_t)i] << 32 | (uint32_t)g.gb_col[(size_t)i], i});
+    std::sort(bkey.begin(), bkey.end());
     std::vector<int64_t> blk((size_t)ne);
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
     for (int64_t k = 0; k < ne; ++k) {
         const int64_t R = erow[(size_t)k] / bs;
-        int64_t C;
+        int64_t C = -1;
         if (g.gather_flag) {
-            auto it = gpos.find((uint64_t)R << 32 | (uint32_t)ecol[(size_t)k]);
-            if (it == gpos.end()) return "balanced stream: a column outside its gather list";
-            C = it->second / bs;
+            const auto b0 = gcol.begin() + g.block_cols_offset[(size_t)R];
+            const auto b1 = gcol.begin() + g.block_cols_offset[(size_t)R + 1];
+            const auto it = std::lower_bound(b0, b1, std::make_pair(ecol[(size_t)k], INT32_MIN));
+            if (it != b1 && it->first == ecol[(size_t)k]) C = it->second / bs;
         } else {
             C = ecol[(size_t)k] / bs;
         }
-        auto it = bpos.find((uint64_t)R << 32 | (uint32_t)C);
-        if (it == bpos.end()) return "balanced stream: an entry outside every block";
-        blk[(size_t)k] = it->second;
+        const uint64_t key = (uint64_t)R << 32 | (uint32_t)C;
+        const auto it = std::lower_bound(bkey.begin(), bkey.end(), std::make_pair(key, INT64_MIN));
+        if (C < 0 || it == bkey.end() || it->first != key) {
+            bad |= 1;
+            blk[(size_t)k] = -1;
+        } else {
+            blk[(size_t)k] = it->second;
+        }
     }
+    if (bad) return "balanced stream: an entry outside every block";
     // entries by (balanced block, row, column)
     std::vector<int64_t> order((size_t)ne);
     for (int64_t k = 0; k < ne; ++k) order[(size_t)k] = k;
