@@ -21,9 +21,13 @@ roofline    the kernel of the one launch of a step (the row-segment stream
             from the committed ncu summary (profiles/).
 cpu_baseline  the reference's own CPU SpMV (utils.h:98-111, compiled from its
             headers into oracle/_ref) on a bounded sample, 1 thread as written.
-configs     the other workloads (LAP, PL FP32, ST FP64/FP32, DIFF forward and
-            adjoint with 8 right-hand sides, BAT 512-matrix batch), each timed
-            on the device with its roofline fraction (--configs none skips).
+configs     the other workloads (LAP, PL FP32, PL unit values, PL built with
+            row_owned = 0 (balanced schedule beside row-owned), ST FP64/FP32,
+            DIFF forward and adjoint with 8 right-hand sides, BAT 512-matrix
+            batch), each timed on the device with its roofline fraction and
+            checked against the oracle (--configs none skips).
+comparator  cuSPARSE CSR SpMV (and BSR, block sizes 2-16, the analogue of
+            the reference's hipSPARSE BSR baseline) on the same matrix.
 --impl reference   times that CPU SpMV as the reference arm (rank 0 only).
 
 Multi-GPU: every rank runs its own copy of the workload (replicas; SpMV of

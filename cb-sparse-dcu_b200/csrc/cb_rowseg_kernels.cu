@@ -1,9 +1,15 @@
-// Row-segment stream kernel (layout in cb_rowseg.hpp): y = A x for matrices
-// whose stored entries are all in COO blocks.
+// Row-segment stream kernels (layout in cb_rowseg.hpp) and the balanced
+// schedule:
+//   * cb_rowseg_kernel       y = A x, one right-hand side (below);
+//   * cb_rowseg_mrhs_kernel  Y = A X, G lanes per entry, several right-hand
+//                            sides (rs_mrhs_segment);
+//   * cb_rowseg_gv_kernel    the fused adjoint: A^T G and the value gradient;
+//   * cb_rowseg_batch_kernel every matrix of a batch in one launch;
+//   * cb_balanced_kernel     plans built with row_owned = 0: the reference's
+//                            block order, atomics into y;
+//   * value refreshes after cbspmv_set_values.
 //
-// One CTA of kRsWarps warps per SM; warp w of CTA b takes the segments
-// sb0 + w, sb0 + w + kRsWarps, ... of the CTA's share [sb0, sb1) of the
-// segments (about one per warp).  Per chunk a lane
+// One right-hand side: one CTA of 32 warps per SM.  Per chunk a lane
 //   * holds the NEXT chunk's words and values in registers, loaded with
 //     coalesced 16-byte loads that do not allocate in L1 (L1 is left to the
 //     x gathers) and are marked evict-first in L2 (x stays in L2),
@@ -18,9 +24,10 @@
 //     (reset at lanes holding a row start), carrying the chunk's last row into
 //     the next chunk.
 // The products of one row are added in entry order within a lane and in lane
-// order across lanes, fixed by the layout: results are bitwise reproducible.
-// The reference adds each entry into its row with an atomic
-// (cb-spmv-dcu.hpp:423-426); the sums here are the same rows' sums.
+// order across lanes, fixed by the layout: results are bitwise reproducible
+// (the balanced schedule's atomics excepted).  The reference adds each entry
+// into its row with an atomic (cb-spmv-dcu.hpp:423-426); the sums here are
+// the same rows' sums.
 #include <cuda/atomic>
 #include <cuda_runtime.h>
 
