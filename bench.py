@@ -274,7 +274,7 @@ def secondary_configs(dev, peak: float, want=("lap", "pl32", "st", "diff", "bat"
         single("PL fp64 unit values (value-free payload)",
                gen.Coo(pl.m, pl.n, pl.row, pl.col, np.ones(pl.nnz)), False)
         del pl
-    if "unit" in want:  # the balanced schedule (the reference's load-balance ablation)
+    if "bal" in want:  # the balanced schedule (the reference's load-balance ablation)
         try:
             balanced_config(dev, peak, out)
         except Exception as exc:  # informative only: never breaks the bench line
@@ -716,7 +716,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--configs", default="all",
                     help="other workloads to time (rank 0, N=1 only): all, none, or a "
-                         "comma list of lap,pl32,unit,st,diff,bat")
+                         "comma list of lap,pl32,unit,bal,st,diff,bat")
     ap.add_argument("--bat-count", type=int, default=512,
                     help="matrices in the BAT batch (512 is the workload; fewer for "
                          "profiling captures)")
@@ -849,7 +849,7 @@ def main():
     line = None
     configs = None
     if rank == 0 and world == 1 and args.configs != "none":
-        want = {"lap", "pl32", "unit", "st", "diff", "bat"} if args.configs == "all" \
+        want = {"lap", "pl32", "unit", "bal", "st", "diff", "bat"} if args.configs == "all" \
             else set(args.configs.split(","))
         configs = secondary_configs(dev, peak, want, args.bat_count)
     if rank == 0:
