@@ -332,10 +332,11 @@ cbspmv_status cbspmv_check(cbspmv_plan *plan, void *stream);
 void cbspmv_debug_wait_polls(int64_t polls);
 
 /* Times the kernels that can run this plan for nrhs right-hand sides (one
- * vector: streaming when the layout allows it, direct, staged, pattern reuse
- * and row segments when the plan has them; several: the staged kernel) on
- * scratch vectors, keeps the fastest for later calls and returns it in
- * *kernel (1 to 5) with its mean time in *ms (either may be
+ * vector: streaming when the layout allows it, direct, staged, and pattern
+ * reuse, row segments and the balanced schedule when the plan has them;
+ * several: the staged kernel and row segments) on scratch vectors, keeps
+ * the fastest for later calls and returns it in *kernel (1 to 6) with its
+ * mean time in *ms (either may be
  * NULL).  The plan must be uploaded; allocates and frees scratch device
  * memory and synchronizes `stream`.  No counterpart in the reference (its
  * kernel choice is compile-time, cb-spmv-dcu.hpp:1428-1450). */
