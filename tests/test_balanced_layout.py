@@ -91,3 +91,17 @@ def test_no_balanced_stream_without_the_permutation():
     from cbspmv import gen
     coo = gen.random_small(np.random.default_rng(1), 200, 200, 2000)
     assert _bal(cbspmv.Plan(coo), False) is None  # row_owned = 1
+
+
+def test_kernel_option_bounds():
+    """Kernel options 0-6 are accepted (6: the balanced schedule, taken only by
+    plans built with row_owned = 0); others are refused."""
+    import cbspmv
+    from cbspmv import gen
+    coo = gen.random_small(np.random.default_rng(2), 100, 100, 500)
+    for k in range(7):
+        cbspmv.Plan(coo, kernel=k)
+    for k in (-1, 7):
+        with pytest.raises(cbspmv.CBSpMVError) as e:
+            cbspmv.Plan(coo, kernel=k)
+        assert e.value.status == "INVALID"
